@@ -1,0 +1,367 @@
+/*
+ * oracle/prop_impl.h -- propagation, imaging and kz-split loops of the reference,
+ * restated for the CPU oracle.  TEST INFRASTRUCTURE.  Included twice by swd_oracle.c
+ * with T = float / SFX = f32 (the FP32 oracle and OpenMP CPU baseline) and
+ * T = double / SFX = f64 (the FP64 oracle).
+ *
+ * Expressions are written in the reference's order so the float build rounds like the
+ * reference kernels (the reference's nvcc build additionally contracts some mul+add
+ * pairs into FMAs; that difference is the expected ~1e-6 FP32 noise).
+ */
+#define ORC_CAT_(a, b) a##_##b
+#define ORC_CAT(a, b) ORC_CAT_(a, b)
+#define FN(name) ORC_CAT(name, SFX)
+
+typedef struct {
+    int ntx, ntz, Lc, pmlc, nt;
+    T dt;
+    float dx, dz;
+    T rc[16];
+    T *vp, *rho, *ax, *axh, *az, *azh, *bx, *bxh, *bz, *bzh;
+} FN(orc_mdl);
+
+static T *FN(cvt)(const float *src, size_t n)
+{
+    T *d = (T *)malloc(sizeof(T) * (n ? n : 1));
+    for (size_t i = 0; i < n; i++) d[i] = (T)src[i];
+    return d;
+}
+
+static void FN(mdl_init)(FN(orc_mdl) *M, const orc_model *m)
+{
+    size_t ntp = (size_t)m->ntx * m->ntz;
+    M->ntx = m->ntx; M->ntz = m->ntz; M->Lc = m->Lc; M->pmlc = m->pmlc; M->nt = m->nt;
+    M->dt = (T)m->dt; M->dx = m->dx; M->dz = m->dz;
+    for (int i = 0; i < m->Lc && i < 16; i++) M->rc[i] = (T)m->rc[i];
+    M->vp = FN(cvt)(m->vp, ntp); M->rho = FN(cvt)(m->rho, ntp);
+    M->ax = FN(cvt)(m->a_x, m->ntx); M->axh = FN(cvt)(m->a_x_half, m->ntx);
+    M->az = FN(cvt)(m->a_z, m->ntz); M->azh = FN(cvt)(m->a_z_half, m->ntz);
+    M->bx = FN(cvt)(m->b_x, m->ntx); M->bxh = FN(cvt)(m->b_x_half, m->ntx);
+    M->bz = FN(cvt)(m->b_z, m->ntz); M->bzh = FN(cvt)(m->b_z_half, m->ntz);
+}
+
+static void FN(mdl_free)(FN(orc_mdl) *M)
+{
+    free(M->vp); free(M->rho); free(M->ax); free(M->axh); free(M->az); free(M->azh);
+    free(M->bx); free(M->bxh); free(M->bz); free(M->bzh);
+}
+
+typedef struct { T *p, *vx, *vz, *ppx, *ppz, *pvx, *pvz; } FN(orc_fld);
+
+static void FN(fld_alloc)(FN(orc_fld) *f, size_t ntp)
+{
+    f->p = (T *)calloc(ntp, sizeof(T)); f->vx = (T *)calloc(ntp, sizeof(T));
+    f->vz = (T *)calloc(ntp, sizeof(T)); f->ppx = (T *)calloc(ntp, sizeof(T));
+    f->ppz = (T *)calloc(ntp, sizeof(T)); f->pvx = (T *)calloc(ntp, sizeof(T));
+    f->pvz = (T *)calloc(ntp, sizeof(T));
+}
+
+static void FN(fld_free)(FN(orc_fld) *f)
+{
+    free(f->p); free(f->vx); free(f->vz); free(f->ppx); free(f->ppz); free(f->pvx); free(f->pvz);
+}
+
+/* vx += dt/rho_x * (dp/dx + phi_p_x), with CPML memory.  acoustic_HLVSPRTMLc.cu:24-69
+ * (guard iz in [Lc, ntz-Lc], ix in [Lc-1, ntx-Lc-1]); the receiver back-propagation uses
+ * the same body with -dx and the wider guard of :623-667. */
+static void FN(upd_vx)(const FN(orc_mdl) *M, FN(orc_fld) *f, float dx, int iz0, int iz1, int ix0, int ix1)
+{
+    const int ntz = M->ntz, Lc = M->Lc;
+    const T odx = (T)(1.0 / (double)dx);
+    const T dt = M->dt;
+#pragma omp parallel for schedule(static)
+    for (int ix = ix0; ix <= ix1; ix++)
+        for (int iz = iz0; iz <= iz1; iz++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            T d = 0.0;
+            for (int ic = 0; ic < Lc; ic++) d += M->rc[ic] * (f->p[ip + (ic + 1) * ntz] - f->p[ip - ic * ntz]) * odx;
+            f->ppx[ip] = M->bxh[ix] * f->ppx[ip] + M->axh[ix] * d;
+            T orho = (T)(1 / (0.5 * (M->rho[ip] + M->rho[ip + 1 * ntz])));
+            f->vx[ip] = dt * orho * (d + f->ppx[ip]) + f->vx[ip];
+        }
+}
+
+/* vz analogue.  acoustic_HLVSPRTMLc.cu:72-118 (guard iz in [Lc-1, ntz-Lc-1], ix in
+ * [Lc, ntx-Lc]); receiver variant :670-715. */
+static void FN(upd_vz)(const FN(orc_mdl) *M, FN(orc_fld) *f, float dz, int iz0, int iz1, int ix0, int ix1)
+{
+    const int ntz = M->ntz, Lc = M->Lc;
+    const T odz = (T)(1.0 / (double)dz);
+    const T dt = M->dt;
+#pragma omp parallel for schedule(static)
+    for (int ix = ix0; ix <= ix1; ix++)
+        for (int iz = iz0; iz <= iz1; iz++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            T d = 0.0;
+            for (int ic = 0; ic < Lc; ic++) d += M->rc[ic] * (f->p[ip + (ic + 1)] - f->p[ip - ic]) * odz;
+            f->ppz[ip] = M->bzh[iz] * f->ppz[ip] + M->azh[iz] * d;
+            T orho = (T)(1 / (0.5 * (M->rho[ip] + M->rho[ip + 1])));
+            f->vz[ip] = dt * orho * (d + f->ppz[ip]) + f->vz[ip];
+        }
+}
+
+/* p += dt*rho*vp^2*(dvx/dx + phi_vx_x + dvz/dz + phi_vz_z).  acoustic_HLVSPRTMLc.cu:121-173
+ * (guard iz in [Lc, ntz-Lc], ix in [Lc, ntx-Lc]); receiver variant :717-762. */
+static void FN(upd_p)(const FN(orc_mdl) *M, FN(orc_fld) *f, float dx, float dz)
+{
+    const int ntz = M->ntz, ntx = M->ntx, Lc = M->Lc;
+    const T odx = (T)(1.0 / (double)dx), odz = (T)(1.0 / (double)dz);
+    const T dt = M->dt;
+#pragma omp parallel for schedule(static)
+    for (int ix = Lc; ix <= ntx - Lc; ix++)
+        for (int iz = Lc; iz <= ntz - Lc; iz++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            T dvx = 0.0, dvz = 0.0;
+            for (int ic = 0; ic < Lc; ic++) {
+                dvx += M->rc[ic] * (f->vx[ip + ic * ntz] - f->vx[ip - (ic + 1) * ntz]) * odx;
+                dvz += M->rc[ic] * (f->vz[ip + ic] - f->vz[ip - (ic + 1)]) * odz;
+            }
+            f->pvx[ip] = M->bx[ix] * f->pvx[ip] + M->ax[ix] * dvx;
+            f->pvz[ip] = M->bz[iz] * f->pvz[ip] + M->az[iz] * dvz;
+            f->p[ip] = dt * M->rho[ip] * M->vp[ip] * M->vp[ip] * (dvx + f->pvx[ip] + dvz + f->pvz[ip]) + f->p[ip];
+        }
+}
+
+/* boundary strips of p, saved (dir=0) or restored (dir=1).  Save:
+ * acoustic_HLVSPRTMLc.cu:199-219; restore: fdtd_2d_GPU_kernel_borders_backward :575-620.
+ * The per-step layout here is [top Lc x nx][bottom Lc x nx][left Lc x (nz-2Lc)][right]. */
+static void FN(strips_io)(const FN(orc_mdl) *M, T *p, T *s, int dir)
+{
+    const int ntz = M->ntz, ntx = M->ntx, Lc = M->Lc, pmlc = M->pmlc;
+    const int nx = ntx - 2 * pmlc, nz = ntz - 2 * pmlc, nzs = nz - 2 * Lc;
+    size_t k = 0;
+    for (int iz = pmlc; iz <= pmlc + Lc - 1; iz++)
+        for (int ix = pmlc; ix <= ntx - pmlc - 1; ix++, k++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            if (dir) p[ip] = s[k]; else s[k] = p[ip];
+        }
+    for (int iz = ntz - pmlc - Lc; iz <= ntz - pmlc - 1; iz++)
+        for (int ix = pmlc; ix <= ntx - pmlc - 1; ix++, k++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            if (dir) p[ip] = s[k]; else s[k] = p[ip];
+        }
+    for (int ix = pmlc; ix <= pmlc + Lc - 1; ix++)
+        for (int iz = pmlc + Lc; iz <= ntz - pmlc - Lc - 1; iz++, k++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            if (dir) p[ip] = s[k]; else s[k] = p[ip];
+        }
+    for (int ix = ntx - pmlc - Lc; ix <= ntx - pmlc - 1; ix++)
+        for (int iz = pmlc + Lc; iz <= ntz - pmlc - Lc - 1; iz++, k++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            if (dir) p[ip] = s[k]; else s[k] = p[ip];
+        }
+    (void)nx; (void)nzs;
+}
+
+void FN(orc_forward)(const orc_model *m, const orc_geom *g, const float *rick,
+                     const float *hrick, T *seis, T *strips, T *final_state,
+                     int ncol, const int *col_ix, T *cols)
+{
+    FN(orc_mdl) M;
+    FN(mdl_init)(&M, m);
+    const int ntx = M.ntx, ntz = M.ntz, Lc = M.Lc, nt = M.nt;
+    const size_t ntp = (size_t)ntx * ntz;
+    const int slen = orc_strip_len(m);
+    FN(orc_fld) f, h;
+    FN(fld_alloc)(&f, ntp);
+    if (hrick) FN(fld_alloc)(&h, ntp);
+    const size_t src = (size_t)g->s_ix * ntz + g->s_iz;
+    for (int it = 0; it < nt; it++) {
+        /* vx, vz, p, source, record -- the launch order of acoustic_HLVSPRTMLc.cu:320-354 */
+        FN(upd_vx)(&M, &f, m->dx, Lc, ntz - Lc, Lc - 1, ntx - Lc - 1);
+        FN(upd_vz)(&M, &f, m->dz, Lc - 1, ntz - Lc - 1, Lc, ntx - Lc);
+        FN(upd_p)(&M, &f, m->dx, m->dz);
+        f.p[src] += rick[it];
+        if (hrick) {   /* Hilbert twin, forward/...HLForLc.cu:724-760 */
+            FN(upd_vx)(&M, &h, m->dx, Lc, ntz - Lc, Lc - 1, ntx - Lc - 1);
+            FN(upd_vz)(&M, &h, m->dz, Lc - 1, ntz - Lc - 1, Lc, ntx - Lc);
+            FN(upd_p)(&M, &h, m->dx, m->dz);
+            h.p[src] += hrick[it];
+        }
+        if (seis)
+            for (int r = 0; r < g->nrec; r++)
+                seis[(size_t)r * nt + it] = f.p[(size_t)g->r_ix[r] * ntz + g->r_iz[r]];
+        if (strips) FN(strips_io)(&M, f.p, strips + (size_t)it * slen, 0);
+        if (cols)
+            for (int c = 0; c < ncol; c++) {
+                T *dst = cols + ((size_t)c * nt + it) * ntz * 2;
+                const size_t base = (size_t)col_ix[c] * ntz;
+                for (int iz = 0; iz < ntz; iz++) {
+                    dst[2 * iz] = f.p[base + iz];
+                    dst[2 * iz + 1] = hrick ? h.p[base + iz] : (T)0;
+                }
+            }
+    }
+    if (final_state) {
+        memcpy(final_state, f.vx, sizeof(T) * ntp);
+        memcpy(final_state + ntp, f.vz, sizeof(T) * ntp);
+        memcpy(final_state + 2 * ntp, f.p, sizeof(T) * ntp);
+    }
+    FN(fld_free)(&f);
+    if (hrick) FN(fld_free)(&h);
+    FN(mdl_free)(&M);
+}
+
+void FN(orc_kzsep)(int ntz, int nfftz, int nt, int ncol, const T *cols,
+                   const float *coef, int nrec, const int *rec_col, const int *r_iz,
+                   T *up, T *down)
+{
+    const int halfz = nfftz / 2;   /* ceilf(nfftz/2.0) for the power-of-two nfftz */
+#pragma omp parallel
+    {
+        double *F = (double *)malloc(sizeof(double) * 2 * nfftz);
+        double *U = (double *)malloc(sizeof(double) * 2 * nfftz);
+        double *D = (double *)malloc(sizeof(double) * 2 * nfftz);
+#pragma omp for schedule(static) collapse(2)
+        for (int c = 0; c < ncol; c++)
+            for (int it = 0; it < nt; it++) {
+                const T *src = cols + ((size_t)c * nt + it) * ntz * 2;
+                memset(F, 0, sizeof(double) * 2 * nfftz);
+                for (int iz = 0; iz < ntz; iz++) { F[2 * iz] = src[2 * iz]; F[2 * iz + 1] = src[2 * iz + 1]; }
+                orc_fft(nfftz, F, -1);
+                for (int k = 0; k < nfftz; k++) {
+                    double re = F[2 * k] * coef[k], im = F[2 * k + 1] * coef[k];
+                    if (k <= halfz) { U[2 * k] = re; U[2 * k + 1] = im; D[2 * k] = 0; D[2 * k + 1] = 0; }
+                    else { D[2 * k] = re; D[2 * k + 1] = im; U[2 * k] = 0; U[2 * k + 1] = 0; }
+                }
+                orc_fft(nfftz, U, +1);
+                orc_fft(nfftz, D, +1);
+                for (int r = 0; r < nrec; r++)
+                    if (rec_col[r] == c) {
+                        up[(size_t)r * nt + it] = (T)U[2 * r_iz[r]];
+                        down[(size_t)r * nt + it] = (T)D[2 * r_iz[r]];
+                    }
+            }
+        free(F); free(U); free(D);
+    }
+}
+
+void FN(orc_preprocess)(int nrec, int nt, float dtf, const float *d, T *rms)
+{
+    const T dt = (T)dtf;
+    T *frms = FN(cvt)(d, (size_t)nrec * nt);
+    for (int ix = 0; ix < nrec; ix++) {
+        T tmp = 0.0;
+        for (int it = 0; it < nt; it++) {
+            size_t ip = (size_t)ix * nt + it;
+            tmp += frms[ip] * dt;
+            frms[ip] = tmp;
+        }
+    }
+    for (int ix = 0; ix < nrec; ix++) {
+        T tmp = 0.0;
+        for (int it = 0; it < nt; it++) {
+            size_t ip = (size_t)ix * nt + it;
+            tmp += frms[ip] * dt;
+            rms[ip] = -tmp;
+        }
+    }
+    free(frms);
+}
+
+void FN(orc_rtm_backward)(const orc_model *m, const orc_geom *g, const float *rick,
+                          const T *rms, const T *strips, const T *final_state,
+                          T *img, T *illum_s, T *illum_r)
+{
+    FN(orc_mdl) M;
+    FN(mdl_init)(&M, m);
+    const int ntx = M.ntx, ntz = M.ntz, Lc = M.Lc, nt = M.nt, pmlc = M.pmlc;
+    const size_t ntp = (size_t)ntx * ntz;
+    const int slen = orc_strip_len(m);
+    FN(orc_fld) s, r;
+    FN(fld_alloc)(&s, ntp);
+    FN(fld_alloc)(&r, ntp);
+    T *dpdt = (T *)calloc(ntp, sizeof(T));
+    memcpy(s.vx, final_state, sizeof(T) * ntp);
+    memcpy(s.vz, final_state + ntp, sizeof(T) * ntp);
+    memcpy(s.p, final_state + 2 * ntp, sizeof(T) * ntp);
+    memset(img, 0, sizeof(T) * ntp);
+    memset(illum_s, 0, sizeof(T) * ntp);
+    if (illum_r) memset(illum_r, 0, sizeof(T) * ntp);
+    const size_t src = (size_t)g->s_ix * ntz + g->s_iz;
+    const T odx = (T)(1.0 / (double)m->dx), odz = (T)(1.0 / (double)m->dz);
+    const T mdt = -M.dt;
+    for (int it = nt - 2; it >= 0; it--) {
+        /* source wavefield: p (interior, -dt) and dp_dt -- fdtd_2d_GPU_kernel_p_backward :434-485 */
+#pragma omp parallel for schedule(static)
+        for (int ix = pmlc; ix <= ntx - pmlc - 1; ix++)
+            for (int iz = pmlc; iz <= ntz - pmlc - 1; iz++) {
+                size_t ip = (size_t)ix * ntz + iz;
+                T dvx = 0.0, dvz = 0.0;
+                for (int ic = 0; ic < Lc; ic++) {
+                    dvx += M.rc[ic] * (s.vx[ip + ic * ntz] - s.vx[ip - (ic + 1) * ntz]) * odx;
+                    dvz += M.rc[ic] * (s.vz[ip + ic] - s.vz[ip - (ic + 1)]) * odz;
+                }
+                s.p[ip] = mdt * M.rho[ip] * M.vp[ip] * M.vp[ip] * (dvx + dvz) + s.p[ip];
+                dpdt[ip] = M.rho[ip] * M.vp[ip] * M.vp[ip] * (dvx + dvz);
+            }
+        s.p[src] -= rick[it + 1];
+        /* strip overwrite -- :575-620 */
+        FN(strips_io)(&M, s.p, (T *)strips + (size_t)it * slen, 1);
+        /* vx, vz (interior, -dt) -- :488-573 */
+#pragma omp parallel for schedule(static)
+        for (int ix = pmlc; ix <= ntx - pmlc - 1; ix++)
+            for (int iz = pmlc; iz <= ntz - pmlc - 1; iz++) {
+                size_t ip = (size_t)ix * ntz + iz;
+                T d = 0.0;
+                for (int ic = 0; ic < Lc; ic++) d += M.rc[ic] * (s.p[ip + (ic + 1) * ntz] - s.p[ip - ic * ntz]) * odx;
+                T orho = (T)(1 / (0.5 * (M.rho[ip] + M.rho[ip + 1 * ntz])));
+                s.vx[ip] = mdt * orho * d + s.vx[ip];
+            }
+#pragma omp parallel for schedule(static)
+        for (int ix = pmlc; ix <= ntx - pmlc - 1; ix++)
+            for (int iz = pmlc; iz <= ntz - pmlc - 1; iz++) {
+                size_t ip = (size_t)ix * ntz + iz;
+                T d = 0.0;
+                for (int ic = 0; ic < Lc; ic++) d += M.rc[ic] * (s.p[ip + (ic + 1)] - s.p[ip - ic]) * odz;
+                T orho = (T)(1 / (0.5 * (M.rho[ip] + M.rho[ip + 1])));
+                s.vz[ip] = mdt * orho * d + s.vz[ip];
+            }
+        /* receiver wavefield with -dx,-dz and hard injection -- :623-782, launches :1111-1140 */
+        FN(upd_vx)(&M, &r, -m->dx, 0, ntz - 1, Lc - 1, ntx - Lc - 1);
+        FN(upd_vz)(&M, &r, -m->dz, Lc - 1, ntz - Lc - 1, 0, ntx - 1);
+        FN(upd_p)(&M, &r, -m->dx, -m->dz);
+        for (int k = 0; k < g->nrec; k++)
+            r.p[(size_t)g->r_ix[k] * ntz + g->r_iz[k]] = rms[(size_t)k * nt + it];
+        /* imaging condition -- sum_image_GPU_kernel_image :785-817 */
+#pragma omp parallel for schedule(static)
+        for (int ix = pmlc; ix <= ntx - pmlc - 1; ix++)
+            for (int iz = pmlc; iz <= ntz - pmlc - 1; iz++) {
+                size_t ip = (size_t)ix * ntz + iz;
+                img[ip] += dpdt[ip] * r.p[ip];
+                illum_s[ip] += dpdt[ip] * dpdt[ip];
+                if (illum_r) illum_r[ip] += r.p[ip] * r.p[ip];
+            }
+    }
+    free(dpdt);
+    FN(fld_free)(&s);
+    FN(fld_free)(&r);
+    FN(mdl_free)(&M);
+}
+
+void FN(orc_rtm_post)(const orc_model *m, const T *img, const T *illum_s, T *img_norm, T *fimage)
+{
+    const int ntx = m->ntx, ntz = m->ntz, pmlc = m->pmlc;
+    const int nz = ntz - 2 * pmlc;
+    const size_t ntp = (size_t)ntx * ntz;
+    const T dx = (T)m->dx, dz = (T)m->dz;
+    T remax = 0;
+    for (size_t ip = 0; ip < ntp; ip++) {
+        T a = illum_s[ip] < 0 ? -illum_s[ip] : illum_s[ip];
+        if (remax < a) remax = a;
+    }
+    for (size_t ip = 0; ip < ntp; ip++) img_norm[ip] = (T)(img[ip] / (illum_s[ip] + 1.0e-3 * remax));
+    for (int iz = pmlc; iz <= ntz - pmlc - 1; iz++)
+        for (int ix = pmlc; ix <= ntx - pmlc - 1; ix++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            size_t ipp = (size_t)(ix - pmlc) * nz + iz - pmlc;
+            const T *I = img_norm;
+            T v = (T)m->vp[ip];
+            fimage[ipp] = (T)(-((I[ip + ntz] - 2.0 * I[ip] + I[ip - ntz]) / (dx * dx) +
+                                (I[ip + 1] - 2.0 * I[ip] + I[ip - 1]) / (dz * dz)) * v * v);
+        }
+}
+
+#undef FN
+#undef ORC_CAT
+#undef ORC_CAT_
