@@ -1,0 +1,185 @@
+/*
+ * swd.h -- C ABI of libswd, the B200 (sm_100a) engine for single-GPU VSP reverse-time
+ * migration with scatter-point PSFs and windowed wavenumber PSF deconvolution.
+ *
+ * The reference programs (AFor, AVSPRTM, decon2d_mine) talk to their GPU code through
+ * extern "C" functions taking POD structs (forward/headrtm.h, headrtm.h).  This header
+ * replaces that seam with an opaque context and plain pointers; each entry point names
+ * the reference interface it stands in for.
+ *
+ * Conventions
+ *  - Grids are the reference's padded grids: ntx = nx + 2*pmlc, ntz = nz + 2*pmlc,
+ *    pmlc = pml + Lc, cell (ix, iz) at ix*ntz + iz (z fastest), float32 little-endian.
+ *  - Every pointer argument may be a host pointer or a device pointer on the context's
+ *    device; the library detects which (cudaPointerGetAttributes).  Host results are
+ *    complete when the call returns.
+ *  - Every call returns an int status (SWD_OK = 0); swd_last_error() describes the last
+ *    failure on a context.  A context is used by one host thread at a time and owns one
+ *    CUDA stream (swd_set_stream() may substitute the caller's).
+ *  - Seismograms are trace-major [r_n][nt]; images nx*nz unless stated otherwise.
+ */
+#ifndef SWD_H
+#define SWD_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWD_OK 0
+#define SWD_ERR_ARG 1        /* invalid argument or size */
+#define SWD_ERR_CUDA 2       /* CUDA runtime error (message in swd_last_error) */
+#define SWD_ERR_ALLOC 3      /* device or host allocation failed */
+#define SWD_ERR_STATE 4      /* call made before the data it needs was set */
+#define SWD_ERR_DEVICE 5     /* a kernel reported an error status */
+
+/* strip storage precision for the source-wavefield reconstruction */
+#define SWD_STRIP_F32 0
+#define SWD_STRIP_F16 1      /* IEEE half with a per-(step, tile) scale */
+#define SWD_STRIP_BF16 2     /* bfloat16 with a per-(step, tile) scale */
+
+/* flags of swd_rtm_shot */
+#define SWD_RTM_PREPROCESS 1u     /* apply rms = -int int d dt dt to the data first (reference default) */
+#define SWD_RTM_ILLUM_RCV 2u      /* also accumulate the receiver illumination R = sum p_r^2 */
+#define SWD_RTM_NO_STACK 4u       /* do not add this shot's filtered image to the stack */
+
+typedef struct swd_ctx swd_ctx;
+
+typedef struct {
+    int nx, nz;          /* interior grid */
+    int pml, Lc;         /* CPML cells and half stencil length; pmlc = pml + Lc */
+    float dx, dz, dt;
+    int nt_max;          /* longest record the context will run */
+    int device;          /* CUDA device ordinal */
+} swd_grid;
+
+/* One shot: source cell and receiver cells, padded-grid coordinates.
+ * Replaces struct Source (headrtm.h:8-13, forward/headrtm.h:12-17), whose receivers are
+ * the depth list r_iz[] recorded at the two edge wells (acoustic_HLVSPRTMLc.cu:180-197). */
+typedef struct {
+    int s_ix, s_iz;
+    int nt;              /* record length of this shot (<= nt_max) */
+    int r_n;
+    const int *r_ix;     /* [r_n] */
+    const int *r_iz;     /* [r_n] */
+} swd_shot;
+
+/* ---- context ------------------------------------------------------------------------
+ * Replaces getdevice/variables_malloc/variables_free (headrtm.h:5-6,176-186;
+ * acoustic_HLVSPRTMLc.cu:1613-1845; forward/acoustic_hilbert_fftkz_HLForLc.cu:1425-1692). */
+int swd_version(void);
+int swd_device_count(int *n);
+int swd_create(swd_ctx **out, const swd_grid *grid);
+int swd_destroy(swd_ctx *ctx);
+const char *swd_last_error(const swd_ctx *ctx);
+int swd_set_stream(swd_ctx *ctx, void *cuda_stream);
+int swd_synchronize(swd_ctx *ctx);
+/* bytes of device memory the context holds right now */
+size_t swd_device_bytes(const swd_ctx *ctx);
+
+/* ---- model and operator setup (the H2D block of fdtd_2d_GPU_forward,
+ *      acoustic_HLVSPRTMLc.cu:274-304) ------------------------------------------------ */
+int swd_set_stencil(swd_ctx *ctx, const float *rc);                 /* rc[Lc], cal_xishu */
+int swd_set_cpml(swd_ctx *ctx, const float *a_x, const float *a_x_half,
+                 const float *a_z, const float *a_z_half,
+                 const float *b_x, const float *b_x_half,
+                 const float *b_z, const float *b_z_half);
+int swd_set_model(swd_ctx *ctx, const float *vp, const float *rho);   /* padded ntx*ntz */
+int swd_set_strip_precision(swd_ctx *ctx, int strip_precision);       /* SWD_STRIP_* */
+
+/* ---- forward modelling --------------------------------------------------------------
+ * Replaces fdtd_2d_GPU_forward of AFor (forward/headrtm.h:159-171,
+ * forward/acoustic_hilbert_fftkz_HLForLc.cu:576-863) and, with hrick = kz_coef = NULL, the
+ * inv_flag=0 call of fdtd_2d_GPU_forward in AVSPRTM (headrtm.h:129-141).
+ *   seis      [r_n][nt]  pressure at the receivers (required)
+ *   hrick     Hilbert-transformed wavelet; with kz_coef it propagates the twin wavefield
+ *   kz_coef   [nfftz] kz taper; nfftz = 2^ceil(log2(ntz)) as the reference computes it
+ *   seis_up / seis_down  [r_n][nt] kz-separated traces, scaled by nfftz like the
+ *             reference's unnormalised inverse cuFFT (both NULL unless hrick and kz_coef). */
+int swd_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *hrick,
+                const float *kz_coef, float *seis, float *seis_up, float *seis_down);
+
+/* ---- RTM of one shot ---------------------------------------------------------------
+ * Replaces the fdtd_2d_GPU_forward(inv_flag=1) + fdtd_2d_GPU_backward pair and the per-shot
+ * host steps of AVSPRTM (acoustic_HLVSPRTMC.cpp:576-745; acoustic_HLVSPRTMLc.cu:239-432,
+ * 946-1215).  The final forward wavefield stays in HBM (no disk round trip).
+ *   data      [r_n][nt] receiver data (the up-going file in the reference flow)
+ *   syn       [r_n][nt] synthetic data of the forward pass (nullable)
+ *   image_pp  nx*nz  I/(S + 1e-3 max S) as written to image_pp%d / image_psf%d (nullable)
+ *   image_src nx*nz  S (image_sources%d) (nullable)
+ *   fimage    nx*nz  -vp^2 Laplacian of image_pp, fimage_pp%d (nullable)
+ * Unless SWD_RTM_NO_STACK, fimage is added to the context's FP64 stack. */
+int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *data,
+                 unsigned flags, float *syn, float *image_pp, float *image_src, float *fimage);
+/* raw accumulators of the last shot on the padded grid: I, S (and R if accumulated), FP64 */
+int swd_rtm_raw(swd_ctx *ctx, double *image, double *illum_src, double *illum_rcv);
+/* the stacked image nx*nz, optionally with the reference's edge zeroing
+ * (acoustic_HLVSPRTMC.cpp:750-768); reset clears it */
+int swd_stack_get(swd_ctx *ctx, int edge_zero, float *migration);
+int swd_stack_reset(swd_ctx *ctx);
+
+/* ---- batched RTM: many shots of uneven nt and aperture, stacked --------------------- */
+int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *const *ricks,
+                  const float *const *data, unsigned flags);
+
+/* ---- helpers that run on the GPU ----------------------------------------------------
+ * swd_hilbert replaces hilbert_transform1d (forward/headrtm.h:228-229,
+ * forward/acoustic_hilbert_fftkz_HLForLc.cu:1257-1324).
+ * swd_smooth replaces ini_model_mine (acoustic_HLVSPRTMC.cpp:1473-1569): in place on a
+ * padded ntx*ntz model, same double accumulation order.
+ * swd_preprocess applies the reference's -int int dt dt to [r_n][nt] traces
+ * (acoustic_HLVSPRTMC.cpp:606-637). */
+int swd_hilbert(swd_ctx *ctx, int nt, const float *rick, float *hrick);
+int swd_smooth(swd_ctx *ctx, int ntx, int ntz, int pmlc, int window, float *vp);
+int swd_preprocess(swd_ctx *ctx, int r_n, int nt, float dt, const float *d, float *rms);
+
+/* ---- windowed wavenumber PSF deconvolution -----------------------------------------
+ * Replaces the window loop of decon2d_mine
+ * (kkdecon_acoustic/kk_decon_interp_psf_minewindow.cpp:84-132,303-383,543-674).
+ * fft_nx/fft_nz = 0 keep the reference's FFT size filterwin+psfwin-1; larger values select
+ * a zero-padded FFT (project option).  Outputs are nx*nz like the reference's files. */
+typedef struct {
+    int nx, nz;
+    int psfwinx, psfwinz, filterwinx, filterwinz, snapwinx, snapwinz;
+    float epsilon;
+    int fft_nx, fft_nz;
+} swd_decon_params;
+int swd_decon_geometry(const swd_decon_params *p, int *windows, int *fft_nx, int *fft_nz);
+int swd_decon(swd_ctx *ctx, const swd_decon_params *p, const float *migreal,
+              const float *migpsf, float *mig_dec, float *mig_coef);
+
+/* ---- instrumentation (no reference counterpart; the reference only prints clock()) ---
+ * swd_profile(ctx, every): bracket each kernel launch of every `every`-th time step with
+ * CUDA events on the context stream (0 disables).  swd_profile_read fills, per kernel id
+ * (0 forward-v, 1 forward-p, 2 backward-1, 3 backward-2), the summed milliseconds and the
+ * number of timed launches, and clears them.  swd_launch_count is the number of kernels the
+ * context has launched since it was created. */
+#define SWD_NKERNELS 4
+int swd_profile(swd_ctx *ctx, int every);
+int swd_profile_read(swd_ctx *ctx, double *ms, long long *launches);
+long long swd_launch_count(const swd_ctx *ctx);
+
+/* ---- host preparation (the reference's host functions, restated) ------------------- */
+/* cal_xishu, acoustic_HLVSPRTMC.cpp:1858-1878 */
+void swd_prep_xishu(int Lc, float *rc);
+/* get_absorbing_parameters, acoustic_HLVSPRTMC.cpp:891-1129 (pml argument = pmlc) */
+void swd_prep_cpml(int ntx, int ntz, int pmlc, float dx, float dz, float dt,
+                   float *a_x, float *a_x_half, float *a_z, float *a_z_half,
+                   float *b_x, float *b_x_half, float *b_z, float *b_z_half);
+/* ricker_wave flag 2 with t0 = 1/f0, acoustic_HLVSPRTMC.cpp:1249-1299 */
+void swd_prep_ricker(int nt, float f0, float dt, float *rick);
+/* get_acc_model edge replication, acoustic_HLVSPRTMC.cpp:1136-1196 */
+void swd_prep_pad(int nx, int nz, int pmlc, const float *v_in, float *v_pad);
+/* 2^ceil(log2 n) exactly as the reference evaluates it (forward/...HLForC.cpp:299-300) */
+int swd_prep_pow2(int n);
+/* kz taper, forward/...HLForC.cpp:354-377; returns layerz or -1 if the reference aborts */
+int swd_prep_kz_taper(int nfftz, float dz, float *coef);
+/* two-edge-well receiver depths, acoustic_HLVSPRTMC.cpp:153-200 + acoustic_HLVSPRTMLc.cu:180-197;
+ * returns r_n; r_ix/r_iz may be NULL to query the count */
+int swd_prep_wells(int nx, int nz, int pmlc, float dz, float shotdep, float offsetz,
+                   int *r_ix, int *r_iz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,221 @@
+// decon.cuh -- windowed wavenumber-domain PSF deconvolution (decon2d_mine's window loop,
+// kkdecon_acoustic/kk_decon_interp_psf_minewindow.cpp:543-674) as one CTA per window.
+//
+// Per window, in shared memory:
+//   Z = M/|M|_1 + i*S/|S|_1 on an n0 x n1 buffer (M: filterwin^2 image patch centred at
+//   the buffer midpoint, S: nearest psfwin^2 PSF at the buffer corner);
+//   Z^ = DFT2(Z) once (the two real transforms packed into one complex one);
+//   M^(k) = (Z^(k) + conj Z^(-k))/2,  S^(k) = (Z^(k) - conj Z^(-k))/(2i);
+//   D(k) = M^ conj(S^) / (|S^|^2 + eps*max|S^|^2), numerator and quotient in FP64, the
+//   damped denominator rounded through float as the reference does (:636,648);
+//   d = IDFT2(D) (unnormalised); the outwin^2 centre, times the Hann-edged taper, is
+//   written to a per-window slot.  A second kernel overlap-adds the slots in window order.
+//
+// The buffer index is ixx*FZ + izz and the 2D transform is taken over (n0 rows x n1
+// columns) of that linear buffer, which is how the reference plans it
+// (fftw_plan_dft_2d(fullwz, fullwx) on an x-major buffer, :490-493).  Transforms are FP32
+// DFTs over shared-memory twiddle tables (any length up to 512, prime 101 included).
+// The L1 norms are accumulated serially in the reference's order with the reference's
+// float-through-double rounding, so the normalisation matches it exactly.
+#pragma once
+#include <cuda_runtime.h>
+#include "fft.cuh"
+
+namespace swd {
+
+struct DeconGeo {
+    int nx, nz;
+    int psfwinx, psfwinz, filterwinx, filterwinz, snapwinx, snapwinz;
+    int halfpsfwx, halfpsfwz, halfltwx, halfltwz, nxwpsf, nzwpsf;
+    int FX, FZ, n0, n1, midpx, midpz, ocx, ocz;
+    int outwinx, outwinz, halfoutwx, halfoutwz, stepwinx, stepwinz, stepnumx, stepnumz, totalnum, nxp, nzp;
+    float epsilon;
+};
+
+// expanded-image read (edge replication of :303-339): clamp to the last row/column
+__device__ __forceinline__ float img_at(const float *__restrict__ im, int nx, int nz, int ix, int iz)
+{
+    ix = ix < nx ? ix : nx - 1;
+    iz = iz < nz ? iz : nz - 1;
+    return __ldg(im + (size_t)ix * nz + iz);
+}
+
+// Batched direct DFTs of length L over B transforms of the linear buffer s:
+// element j of transform t at s[t*str + j*sin].  sign -1 forward, +1 inverse; tw[m] =
+// exp(-2*pi*i*m/L).  Whole transforms are processed per round so the in-place
+// write-back never overwrites inputs still being read.
+__device__ void dft_pass(float2 *s, const float2 *tw, int L, int B, int sin, int str, int sign)
+{
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int per = nthr / L;   // transforms per round (L <= nthr)
+    for (int t0 = 0; t0 < B; t0 += per) {
+        const int t = t0 + tid / L, k = tid % L;
+        const bool act = (tid / L) < per && t < B;
+        float2 y = make_float2(0.f, 0.f);
+        if (act) {
+            const float2 *x = s + (size_t)t * str;
+            int m = 0;
+            for (int j = 0; j < L; j++) {
+                const float2 w = tw[m];
+                const float wi = sign < 0 ? w.y : -w.y;
+                const float2 v = x[(size_t)j * sin];
+                y.x = fmaf(v.x, w.x, fmaf(-v.y, wi, y.x));
+                y.y = fmaf(v.x, wi, fmaf(v.y, w.x, y.y));
+                m += k;
+                if (m >= L) m -= L;
+            }
+        }
+        __syncthreads();
+        if (act) s[(size_t)t * str + (size_t)k * sin] = y;
+        __syncthreads();
+    }
+}
+
+__device__ void dft2(float2 *s, const float2 *tw0, const float2 *tw1, int n0, int n1, int sign)
+{
+    dft_pass(s, tw1, n1, n0, 1, n1, sign);   // rows (length n1)
+    dft_pass(s, tw0, n0, n1, n1, 1, sign);   // columns (length n0)
+}
+
+__global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *__restrict__ mig,
+                                                      const float *__restrict__ psf, const float *__restrict__ coefr,
+                                                      float *__restrict__ winout)
+{
+    extern __shared__ float2 sm[];
+    const int n = g.FX * g.FZ;
+    float2 *Z = sm;
+    float2 *tw0 = Z + n, *tw1 = tw0 + g.n0;
+    __shared__ float s_ppmax, s_psfmax;
+    __shared__ unsigned s_fmax;
+    const int w = blockIdx.x;
+    const int ix = g.stepwinx * (w / g.stepnumz), iz = g.stepwinz * (w % g.stepnumz);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    // nearest PSF on the lattice, indices clamped to [3, nwpsf-4] (:586-598)
+    int ixf = (ix - g.halfpsfwx) / g.psfwinx, izf = (iz - g.halfpsfwz) / g.psfwinz;
+    if (ixf <= 2) ixf = 3;
+    if (ixf >= g.nxwpsf - 3) ixf = g.nxwpsf - 4;
+    if (izf <= 2) izf = 3;
+    if (izf >= g.nzwpsf - 3) izf = g.nzwpsf - 4;
+    const int ixp = g.halfpsfwx + ixf * g.psfwinx, izp = g.halfpsfwz + izf * g.psfwinz;
+
+    for (int j = tid; j < n; j += nthr) Z[j] = make_float2(0.f, 0.f);
+    for (int j = tid; j < g.n0; j += nthr) {
+        float s, c;
+        sincospi(-2.0f * (float)j / (float)g.n0, &s, &c);
+        tw0[j] = make_float2(c, s);
+    }
+    for (int j = tid; j < g.n1; j += nthr) {
+        float s, c;
+        sincospi(-2.0f * (float)j / (float)g.n1, &s, &c);
+        tw1[j] = make_float2(c, s);
+    }
+    // L1 norms in the reference's order and rounding (:554-576, :618-620): thread 0 sums
+    // the image patch, thread 32 the PSF, while the rest of the block fills the buffer
+    if (tid == 0) {
+        float pp = 0.0f;
+        for (int ixx = 0; ixx < g.filterwinx; ixx++)
+            for (int izz = 0; izz < g.filterwinz; izz++) {
+                const int iix = ix - g.halfltwx + ixx, iiz = iz - g.halfltwz + izz;
+                if (iix >= 0 && iix < g.nxp && iiz >= 0 && iiz < g.nzp)
+                    pp = (float)((double)pp + fabs((double)img_at(mig, g.nx, g.nz, iix, iiz)));
+            }
+        if ((double)pp <= 1.0e-15) pp = 1.0e-10f;
+        s_ppmax = pp;
+    } else if (tid == 32) {
+        float ps = 0.0f;
+        for (int ixx = 0; ixx < g.psfwinx; ixx++)
+            for (int izz = 0; izz < g.psfwinz; izz++)
+                ps = (float)((double)ps + fabs((double)img_at(psf, g.nx, g.nz, ixp + ixx - g.halfpsfwx, izp + izz - g.halfpsfwz)));
+        s_psfmax = ps;
+    }
+    if (tid == 64) s_fmax = 0u;
+    __syncthreads();
+    const double ppm = (double)s_ppmax, psm = (double)s_psfmax;
+    for (int j = tid; j < g.filterwinx * g.filterwinz; j += nthr) {
+        const int ixx = j / g.filterwinz, izz = j % g.filterwinz;
+        const int iix = ix - g.halfltwx + ixx, iiz = iz - g.halfltwz + izz;
+        if (iix >= 0 && iix < g.nxp && iiz >= 0 && iiz < g.nzp) {
+            const int ip = (g.midpx - g.halfltwx + ixx) * g.FZ + g.midpz - g.halfltwz + izz;
+            Z[ip].x = (float)((double)img_at(mig, g.nx, g.nz, iix, iiz) / ppm);
+        }
+    }
+    for (int j = tid; j < g.psfwinx * g.psfwinz; j += nthr) {
+        const int ixx = j / g.psfwinz, izz = j % g.psfwinz;
+        Z[ixx * g.FZ + izz].y = (float)((double)img_at(psf, g.nx, g.nz, ixp + ixx - g.halfpsfwx, izp + izz - g.halfpsfwz) / psm);
+    }
+    __syncthreads();
+    dft2(Z, tw0, tw1, g.n0, g.n1, -1);
+    // |S^|^2 maximum over all bins (float compare of the double square, :625-633)
+    float fm = 0.f;
+    for (int j = tid; j < n; j += nthr) {
+        const int r = j / g.n1, c = j % g.n1;
+        const int jm = ((g.n0 - r) % g.n0) * g.n1 + (g.n1 - c) % g.n1;
+        const float2 a = Z[j], b = Z[jm];
+        const double sr = 0.5 * ((double)a.y + (double)b.y), si = -0.5 * ((double)a.x - (double)b.x);
+        fm = fmaxf(fm, (float)(sr * sr + si * si));
+    }
+    for (int o = 16; o > 0; o >>= 1) fm = fmaxf(fm, __shfl_xor_sync(0xffffffffu, fm, o));
+    if ((tid & 31) == 0) atomicMax(&s_fmax, __float_as_uint(fm));
+    __syncthreads();
+    float fft_max = __uint_as_float(s_fmax) * g.epsilon;
+    if (fft_max == 0.0f) fft_max = 1.0e-15f;
+    // D(k) and D(-k) from the pair (Z(k), Z(-k)); each pair handled once (j <= jm)
+    for (int j = tid; j < n; j += nthr) {
+        const int r = j / g.n1, c = j % g.n1;
+        const int jm = ((g.n0 - r) % g.n0) * g.n1 + (g.n1 - c) % g.n1;
+        if (j > jm) continue;
+        const float2 a = Z[j], b = Z[jm];
+        // bin k: M = ((a+b*)/2), S = ((a-b*)/2i); bin -k uses the conjugates
+        const double mr = 0.5 * ((double)a.x + (double)b.x), mi = 0.5 * ((double)a.y - (double)b.y);
+        const double sr = 0.5 * ((double)a.y + (double)b.y), si = -0.5 * ((double)a.x - (double)b.x);
+        const float den = (float)((sr * sr + si * si) + (double)fft_max);
+        const double dr = (mr * sr + mi * si) / (double)den;
+        const double di = (-mr * si + mi * sr) / (double)den;
+        Z[j] = make_float2((float)dr, (float)di);
+        if (jm != j) Z[jm] = make_float2((float)dr, (float)-di);   // D(-k) = conj D(k)
+    }
+    __syncthreads();
+    dft2(Z, tw0, tw1, g.n0, g.n1, +1);
+    const int nout = g.outwinx * g.outwinz;
+    float *o = winout + (size_t)w * nout;
+    for (int j = tid; j < nout; j += nthr) {
+        const int ixx = j / g.outwinz, izz = j % g.outwinz;
+        const int ip = (g.ocx - g.halfoutwx + ixx) * g.FZ + g.ocz - g.halfoutwz + izz;
+        o[j] = Z[ip].x;
+    }
+}
+
+// Overlap-add of the window slots in window order (:656-673), float accumulators with the
+// reference's double-then-round update, cropped to nx x nz (:724-731).
+__global__ void k_decon_gather(DeconGeo g, const float *__restrict__ winout, const float *__restrict__ coefr,
+                               float *__restrict__ dec, float *__restrict__ coef)
+{
+    const size_t np = (size_t)g.nx * g.nz;
+    const int nout = g.outwinx * g.outwinz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+        const int px = (int)(i / g.nz), pz = (int)(i % g.nz);
+        // windows a (x) with a*stepwinx - halfoutwx <= px <= a*stepwinx - halfoutwx + outwinx - 1
+        int alo = px + g.halfoutwx - g.outwinx + 1;
+        alo = alo <= 0 ? 0 : (alo + g.stepwinx - 1) / g.stepwinx;
+        int ahi = (px + g.halfoutwx) / g.stepwinx;
+        if (ahi > g.stepnumx - 1) ahi = g.stepnumx - 1;
+        int blo = pz + g.halfoutwz - g.outwinz + 1;
+        blo = blo <= 0 ? 0 : (blo + g.stepwinz - 1) / g.stepwinz;
+        int bhi = (pz + g.halfoutwz) / g.stepwinz;
+        if (bhi > g.stepnumz - 1) bhi = g.stepnumz - 1;
+        float acc = 0.f, cacc = 0.f;
+        for (int a = alo; a <= ahi; a++)
+            for (int b = blo; b <= bhi; b++) {
+                const int ixx = px - (a * g.stepwinx - g.halfoutwx), izz = pz - (b * g.stepwinz - g.halfoutwz);
+                const int ipc = ixx * g.outwinz + izz;
+                const float cr = __ldg(coefr + ipc);
+                const float v = winout[(size_t)(a * g.stepnumz + b) * nout + ipc];
+                acc = (float)((double)acc + (double)v * (double)cr);
+                cacc = cacc + cr;
+            }
+        dec[i] = acc;
+        coef[i] = cacc;
+    }
+}
+
+}  // namespace swd

@@ -1,0 +1,1174 @@
+// swd.cu -- libswd: C ABI, context, and orchestration of the sm_100a kernels.
+//
+// One context = one padded grid on one device with one stream.  It owns every device
+// buffer (model, CPML profiles, wavefields, strips, images, stack); nothing crosses the
+// host boundary inside a shot except the per-step wavelet sample, which is a kernel
+// argument.  The final forward wavefield stays in HBM for the backward pass (the
+// reference writes it to disk, acoustic_HLVSPRTMLc.cu:403-415 / :994-1004).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/swd.h"
+#include "prop.cuh"
+#include "fft.cuh"
+#include "decon.cuh"
+
+using namespace swd;
+
+// ------------------------------------------------------------------------------------
+// small helpers
+// ------------------------------------------------------------------------------------
+struct DevBuf {
+    void *p = nullptr;
+    size_t n = 0;
+};
+
+struct swd_ctx {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    swd_grid grid{};
+    int ntx = 0, ntz = 0, ldz = 0, pmlc = 0, Lc = 0, nx = 0, nz = 0;
+    float rc[MAXLC] = {0};
+    bool have_rc = false, have_cpml = false, have_model = false;
+    int strip_prec = SWD_STRIP_F32;
+    std::string err;
+    std::vector<DevBuf *> bufs;
+    // model / operator
+    DevBuf vp, rho, cpml[8];
+    // wavefields: w[0], w[1] (7 arrays each), dp/dt
+    DevBuf wave[2][7], dpdt;
+    // acquisition
+    DevBuf wcol, wmap, seis, seis2, rdata, colbuf, kzcoef, tw;
+    // strips
+    DevBuf strips, strip_scale;
+    // imaging
+    DevBuf I, S, R, stack, reduce;
+    bool have_R = false, have_shot = false;
+    DevBuf stage_in, stage_out;
+    // instrumentation
+    int prof_every = 0;
+    double prof_ms[SWD_NKERNELS] = {0};
+    long long prof_n[SWD_NKERNELS] = {0};
+    long long launches = 0;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+    std::vector<cudaEvent_t> ev_pool;
+    swd_ctx()
+    {
+        DevBuf *all[] = {&vp, &rho, &dpdt, &wcol, &wmap, &seis, &seis2, &rdata, &colbuf, &kzcoef, &tw,
+                         &strips, &strip_scale, &I, &S, &R, &stack, &reduce, &stage_in, &stage_out};
+        for (DevBuf *b : all) bufs.push_back(b);
+        for (auto &b : cpml) bufs.push_back(&b);
+        for (auto &w : wave)
+            for (auto &b : w) bufs.push_back(&b);
+    }
+};
+
+static int fail(swd_ctx *c, int code, const char *fmt, ...)
+{
+    char msg[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(msg, sizeof msg, fmt, ap);
+    va_end(ap);
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(ctx, SWD_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),  \
+                        __FILE__, __LINE__);                                               \
+    } while (0)
+
+#define CKR(expr)                          \
+    do {                                   \
+        int r_ = (expr);                   \
+        if (r_ != SWD_OK) return r_;       \
+    } while (0)
+
+static int ensure(swd_ctx *ctx, DevBuf &b, size_t bytes)
+{
+    if (b.n >= bytes && b.p) return SWD_OK;
+    if (b.p) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.n = 0;
+    }
+    if (bytes == 0) return SWD_OK;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return fail(ctx, SWD_ERR_ALLOC, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    b.n = bytes;
+    return SWD_OK;
+}
+
+static bool is_device_ptr(const void *p)
+{
+    if (!p) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// copy n elements of host-or-device src into device buffer dst
+static int to_dev(swd_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    CK(cudaMemcpyAsync(dst, src, bytes, is_device_ptr(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       ctx->stream));
+    return SWD_OK;
+}
+
+static int from_dev(swd_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    CK(cudaMemcpyAsync(dst, src, bytes, is_device_ptr(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    return SWD_OK;
+}
+
+// host copy of a small array that may live on the device
+template <typename T>
+static int host_copy(swd_ctx *ctx, std::vector<T> &out, const T *src, size_t n)
+{
+    out.resize(n);
+    if (n == 0) return SWD_OK;
+    if (is_device_ptr(src)) {
+        CK(cudaMemcpyAsync(out.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    } else {
+        memcpy(out.data(), src, n * sizeof(T));
+    }
+    return SWD_OK;
+}
+
+// padded-grid array (ntx x ntz, host layout) -> device layout with leading dimension ldz
+static int grid_to_dev(swd_ctx *ctx, float *dst, const float *src)
+{
+    CK(cudaMemcpy2DAsync(dst, ctx->ldz * sizeof(float), src, ctx->ntz * sizeof(float), ctx->ntz * sizeof(float),
+                         ctx->ntx, is_device_ptr(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                         ctx->stream));
+    return SWD_OK;
+}
+
+static inline float *F(DevBuf &b) { return (float *)b.p; }
+static inline double *D(DevBuf &b) { return (double *)b.p; }
+static inline int *I32(DevBuf &b) { return (int *)b.p; }
+
+static Geo make_geo(const swd_ctx *c)
+{
+    Geo g;
+    g.ntx = c->ntx; g.ntz = c->ntz; g.ldz = c->ldz; g.pmlc = c->pmlc; g.Lc = c->Lc;
+    g.odx = (float)(1.0 / (double)c->grid.dx);
+    g.odz = (float)(1.0 / (double)c->grid.dz);
+    g.dt = c->grid.dt;
+    for (int i = 0; i < MAXLC; i++) g.rc[i] = c->rc[i];
+    return g;
+}
+
+static Cpml make_cpml(swd_ctx *c)
+{
+    Cpml p;
+    p.ax = F(c->cpml[0]); p.axh = F(c->cpml[1]); p.az = F(c->cpml[2]); p.azh = F(c->cpml[3]);
+    p.bx = F(c->cpml[4]); p.bxh = F(c->cpml[5]); p.bz = F(c->cpml[6]); p.bzh = F(c->cpml[7]);
+    return p;
+}
+
+static Wave make_wave(swd_ctx *c, int k)
+{
+    Wave w;
+    w.p = F(c->wave[k][0]); w.vx = F(c->wave[k][1]); w.vz = F(c->wave[k][2]);
+    w.ppx = F(c->wave[k][3]); w.ppz = F(c->wave[k][4]); w.pvx = F(c->wave[k][5]); w.pvz = F(c->wave[k][6]);
+    return w;
+}
+
+// ---- per-kernel event timing on a subsample of steps --------------------------------
+static cudaEvent_t ev_get(swd_ctx *c)
+{
+    if (!c->ev_pool.empty()) {
+        cudaEvent_t e = c->ev_pool.back();
+        c->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct ProfScope {   // records a (start, end) event pair around one launch when active
+    swd_ctx *c;
+    int k;
+    bool on;
+    cudaEvent_t a{}, b{};
+    ProfScope(swd_ctx *c_, int k_, bool on_) : c(c_), k(k_), on(on_)
+    {
+        if (on) { a = ev_get(c); b = ev_get(c); cudaEventRecord(a, c->stream); }
+    }
+    ~ProfScope()
+    {
+        if (on) { cudaEventRecord(b, c->stream); c->prof_pending.push_back({k, {a, b}}); }
+    }
+};
+
+static void prof_collect(swd_ctx *c)
+{
+    if (c->prof_pending.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (auto &p : c->prof_pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
+            c->prof_ms[p.first] += ms;
+            c->prof_n[p.first] += 1;
+        }
+        c->ev_pool.push_back(p.second.first);
+        c->ev_pool.push_back(p.second.second);
+    }
+    c->prof_pending.clear();
+    cudaGetLastError();
+}
+
+static size_t grid_bytes(const swd_ctx *c) { return (size_t)c->ntx * c->ldz * sizeof(float); }
+
+static int zero_wave(swd_ctx *ctx, int k)
+{
+    for (int i = 0; i < 7; i++) {
+        CKR(ensure(ctx, ctx->wave[k][i], grid_bytes(ctx)));
+        CK(cudaMemsetAsync(ctx->wave[k][i].p, 0, grid_bytes(ctx), ctx->stream));
+    }
+    return SWD_OK;
+}
+
+static dim3 grid_blocks(const swd_ctx *c) { return dim3((c->ntz + 31) / 32, (c->ntx + 7) / 8); }
+
+// ------------------------------------------------------------------------------------
+// acquisition: receivers grouped by well column
+// ------------------------------------------------------------------------------------
+struct ShotPlan {
+    int nwells = 0;
+    std::vector<int> wcol;              // [ntx]
+    std::vector<int> wmap;              // [nwells][ldz]
+    std::vector<std::pair<int, int>> alias;  // (dst trace, src trace) for duplicate cells
+    std::vector<int> well_x;
+};
+
+static int plan_shot(swd_ctx *ctx, const swd_shot *s, ShotPlan &P)
+{
+    if (!s) return fail(ctx, SWD_ERR_ARG, "shot is NULL");
+    if (s->nt < 2 || s->nt > ctx->grid.nt_max) return fail(ctx, SWD_ERR_ARG, "shot nt=%d outside [2, nt_max=%d]", s->nt, ctx->grid.nt_max);
+    if (s->r_n < 1 || !s->r_ix || !s->r_iz) return fail(ctx, SWD_ERR_ARG, "shot needs r_n >= 1 receivers");
+    if (s->s_ix < 0 || s->s_ix >= ctx->ntx || s->s_iz < 0 || s->s_iz >= ctx->ntz)
+        return fail(ctx, SWD_ERR_ARG, "source cell (%d,%d) outside the %dx%d grid", s->s_ix, s->s_iz, ctx->ntx, ctx->ntz);
+    std::vector<int> rx, rz;
+    CKR(host_copy(ctx, rx, s->r_ix, s->r_n));
+    CKR(host_copy(ctx, rz, s->r_iz, s->r_n));
+    P.wcol.assign(ctx->ntx, -1);
+    P.nwells = 0;
+    for (int r = 0; r < s->r_n; r++) {
+        if (rx[r] < 0 || rx[r] >= ctx->ntx || rz[r] < 0 || rz[r] >= ctx->ntz)
+            return fail(ctx, SWD_ERR_ARG, "receiver %d cell (%d,%d) outside the grid", r, rx[r], rz[r]);
+        if (P.wcol[rx[r]] < 0) { P.wcol[rx[r]] = P.nwells++; P.well_x.push_back(rx[r]); }
+    }
+    P.wmap.assign((size_t)P.nwells * ctx->ldz, -1);
+    for (int r = 0; r < s->r_n; r++) {
+        int &slot = P.wmap[(size_t)P.wcol[rx[r]] * ctx->ldz + rz[r]];
+        // injection keeps the last trace for a cell (the reference loop order); recorded
+        // traces of the other duplicates are copied from it afterwards
+        if (slot >= 0) P.alias.push_back({slot, r});
+        slot = r;
+    }
+    for (auto &a : P.alias) {   // make every alias point at the surviving trace
+        int keep = P.wmap[(size_t)P.wcol[rx[a.first]] * ctx->ldz + rz[a.first]];
+        a.second = keep;
+    }
+    CKR(ensure(ctx, ctx->wcol, sizeof(int) * ctx->ntx));
+    CKR(ensure(ctx, ctx->wmap, sizeof(int) * P.wmap.size()));
+    CK(cudaMemcpyAsync(ctx->wcol.p, P.wcol.data(), sizeof(int) * ctx->ntx, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->wmap.p, P.wmap.data(), sizeof(int) * P.wmap.size(), cudaMemcpyHostToDevice, ctx->stream));
+    // pageable H2D copies above complete before returning, so the vectors may go away
+    return SWD_OK;
+}
+
+static int copy_aliases(swd_ctx *ctx, const ShotPlan &P, float *dev_seis, int nt)
+{
+    for (auto &a : P.alias)
+        if (a.first != a.second)
+            CK(cudaMemcpyAsync(dev_seis + (size_t)a.first * nt, dev_seis + (size_t)a.second * nt, sizeof(float) * nt,
+                               cudaMemcpyDeviceToDevice, ctx->stream));
+    return SWD_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// kernels: data preprocessing, kz split, Hilbert, imaging post, smoothing, reductions
+// ------------------------------------------------------------------------------------
+// rms = -sum(sum(d*dt)*dt), one thread per trace, float ops in the reference's order
+// without contraction (acoustic_HLVSPRTMC.cpp:606-637).
+__global__ void k_preprocess(const float *__restrict__ d, float *__restrict__ out, int r_n, int nt, float dt)
+{
+    const int tr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tr >= r_n) return;
+    const float *src = d + (size_t)tr * nt;
+    float *dst = out + (size_t)tr * nt;
+    float t = 0.f;
+    for (int it = 0; it < nt; it++) { t = __fadd_rn(t, __fmul_rn(src[it], dt)); dst[it] = t; }
+    float u = 0.f;
+    for (int it = 0; it < nt; it++) { u = __fadd_rn(u, __fmul_rn(dst[it], dt)); dst[it] = -u; }
+}
+
+// kz up/down split of the recorded well columns: forward FFT of (p + i*p_twin) along z,
+// up = bins [0, N/2] x taper, down = bins (N/2, N) x taper, inverse FFTs, real part at the
+// receiver depths (forward/acoustic_hilbert_fftkz_HLForLc.cu:52-137,761-777).
+__global__ void __launch_bounds__(256) k_kzsep(const float2 *__restrict__ colbuf, const float *__restrict__ coef,
+                                               const float2 *__restrict__ tw, const int *__restrict__ wmap,
+                                               float *up, float *down, int nt, int ntz, int ldz, int N, int logN)
+{
+    extern __shared__ float2 sm[];
+    float2 *su = sm, *sd = sm + N;
+    const int c = blockIdx.y, it = blockIdx.x;
+    const float2 *src = colbuf + ((size_t)c * nt + it) * ldz;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) su[j] = j < ntz ? src[j] : make_float2(0.f, 0.f);
+    __syncthreads();
+    block_fft_dif(su, N, tw);
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        const int k = bitrev(j, logN);
+        const float cf = __ldg(coef + k);
+        const float2 v = make_float2(su[j].x * cf, su[j].y * cf);
+        if (k <= N / 2) { su[j] = v; sd[j] = make_float2(0.f, 0.f); }
+        else { sd[j] = v; su[j] = make_float2(0.f, 0.f); }
+    }
+    __syncthreads();
+    block_ifft_dit(su, N, tw);
+    block_ifft_dit(sd, N, tw);
+    const int *m = wmap + (size_t)c * ldz;
+    for (int z = threadIdx.x; z < ntz; z += blockDim.x) {
+        const int tr = __ldg(m + z);
+        if (tr >= 0) {
+            up[(size_t)tr * nt + it] = su[z].x;
+            down[(size_t)tr * nt + it] = sd[z].x;
+        }
+    }
+}
+
+// Hilbert transform of the wavelet on NZ = 2^ceil(log2 nt) points: -i on bins [1, NZ/2),
+// +i on [NZ/2, NZ), bin 0 zeroed, inverse / NZ (forward/...HLForLc.cu:1257-1324).
+__global__ void __launch_bounds__(256) k_hilbert(const float *__restrict__ rick, float *hr, const float2 *__restrict__ tw,
+                                                  int nt, int N, int logN)
+{
+    extern __shared__ float2 sm[];
+    for (int j = threadIdx.x; j < N; j += blockDim.x) sm[j] = make_float2(j < nt ? rick[j] : 0.f, 0.f);
+    __syncthreads();
+    block_fft_dif(sm, N, tw);
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        const int k = bitrev(j, logN);
+        const float2 f = sm[j];
+        if (k == 0) sm[j] = make_float2(0.f, 0.f);
+        else if (k < N / 2) sm[j] = make_float2(f.y, -f.x);
+        else sm[j] = make_float2(-f.y, f.x);
+    }
+    __syncthreads();
+    block_ifft_dit(sm, N, tw);
+    for (int j = threadIdx.x; j < nt; j += blockDim.x) hr[j] = sm[j].x / (float)N;
+}
+
+// max of a non-negative double array (bit patterns of non-negative doubles order like
+// the values, so an integer atomicMax is exact)
+__global__ void k_max_nonneg(const double *__restrict__ a, size_t n, unsigned long long *out)
+{
+    double m = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(a[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// Per-shot post (acoustic_HLVSPRTMC.cpp:663-743): In = I/(S + 1e-3*max S) on the padded
+// grid, -vp^2 * (5-point Laplacian of In) on the interior, stacked in FP64.
+__global__ void k_rtm_post(const double *__restrict__ I, const double *__restrict__ S, const float *__restrict__ vp,
+                           const unsigned long long *__restrict__ smax, int ntx, int ntz, int ldz, int pmlc,
+                           float dx, float dz, float *img_pp, float *img_src, float *fimage, double *stack)
+{
+    const int nz = ntz - 2 * pmlc, nx = ntx - 2 * pmlc;
+    const int iz = blockIdx.x * 32 + threadIdx.x, ixi = blockIdx.y * 8 + threadIdx.y;
+    if (iz >= nz || ixi >= nx) return;
+    const double rem = 1.0e-3 * __longlong_as_double((long long)*smax);
+    const int x = ixi + pmlc, z = iz + pmlc;
+    auto In = [&](int xx, int zz) -> float {
+        const size_t q = (size_t)xx * ldz + zz;
+        return (float)(I[q] / (S[q] + rem));
+    };
+    const size_t ip = (size_t)x * ldz + z;
+    const float c = In(x, z);
+    const double lap = (In(x + 1, z) - 2.0 * c + In(x - 1, z)) / (double)(dx * dx) +
+                       (In(x, z + 1) - 2.0 * c + In(x, z - 1)) / (double)(dz * dz);
+    const double v = (double)vp[ip];
+    const float f = (float)(-lap * v * v);
+    const size_t o = (size_t)ixi * nz + iz;
+    if (img_pp) img_pp[o] = c;
+    if (img_src) img_src[o] = (float)S[ip];
+    if (fimage) fimage[o] = f;
+    if (stack) stack[o] += (double)f;
+}
+
+// stacked image -> float, reference edge zeroing (acoustic_HLVSPRTMC.cpp:754-768)
+__global__ void k_stack_out(const double *__restrict__ st, float *out, int nx, int nz, int Lc, int edge)
+{
+    const size_t n = (size_t)nx * nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / nz), iz = (int)(i % nz);
+        float v = (float)st[i];
+        if (edge && (ix <= 3 || ix >= nx - Lc || iz < 7 || iz >= nz - Lc)) v = 0.f;
+        out[i] = v;
+    }
+}
+
+// Gaussian smoothing of ini_model_mine (acoustic_HLVSPRTMC.cpp:1514-1556): double
+// accumulation in the reference's loop order with unfused multiply and add, clamped
+// indices, rows iz < pml+8 unchanged.  Coefficients come from the host.
+__global__ void k_smooth(const float *__restrict__ vin, float *vout, const double *__restrict__ coef, int ntx, int ntz,
+                         int pml, int w)
+{
+    const int iz = blockIdx.x * 32 + threadIdx.x + pml, ix = blockIdx.y * 8 + threadIdx.y + pml;
+    if (iz > ntz - pml - 1 || ix > ntx - pml - 1) return;
+    const int wx = 2 * w + 1;
+    double s = 0.0;
+    for (int izw = iz - w; izw <= iz + w; izw++) {
+        const int iz1 = izw < 0 ? 0 : (izw > ntz - 1 ? ntz - 1 : izw);
+        for (int ixw = ix - w; ixw <= ix + w; ixw++) {
+            const int ix1 = ixw < 0 ? 0 : (ixw > ntx - 1 ? ntx - 1 : ixw);
+            s = __dadd_rn(s, __dmul_rn((double)vin[(size_t)ix1 * ntz + iz1], coef[(izw - iz + w) * wx + (ixw - ix + w)]));
+        }
+    }
+    const size_t ip = (size_t)ix * ntz + iz;
+    vout[ip] = iz < pml + 8 ? vin[ip] : (float)s;
+}
+
+// model_in_pml (acoustic_HLVSPRTMC.cpp:1428-1468): x-edges for interior rows, then z-edges
+__global__ void k_pml_x(float *v, int ntx, int ntz, int pml)
+{
+    const int iz = blockIdx.x * blockDim.x + threadIdx.x + pml;
+    if (iz > ntz - pml - 1) return;
+    for (int ix = 0; ix <= pml - 1; ix++) v[(size_t)ix * ntz + iz] = v[(size_t)pml * ntz + iz];
+    for (int ix = ntx - pml; ix < ntx; ix++) v[(size_t)ix * ntz + iz] = v[(size_t)(ntx - pml - 1) * ntz + iz];
+}
+__global__ void k_pml_z(float *v, int ntx, int ntz, int pml)
+{
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ix >= ntx) return;
+    for (int iz = 0; iz <= pml - 1; iz++) v[(size_t)ix * ntz + iz] = v[(size_t)ix * ntz + pml];
+    for (int iz = ntz - pml; iz < ntz; iz++) v[(size_t)ix * ntz + iz] = v[(size_t)ix * ntz + (ntz - pml - 1)];
+}
+
+// ------------------------------------------------------------------------------------
+// launch dispatch on the stencil half-length
+// ------------------------------------------------------------------------------------
+template <int LC>
+static void launch_fwd(swd_ctx *c, const FwdArgs &a, int nw, dim3 grid, bool prof)
+{
+    dim3 blk(32, 8);
+    cudaStream_t s = c->stream;
+    {
+        ProfScope ps(c, 0, prof);
+        if (nw == 2) k_fwd_v<LC, 2><<<grid, blk, 0, s>>>(a);
+        else k_fwd_v<LC, 1><<<grid, blk, 0, s>>>(a);
+    }
+    {
+        ProfScope ps(c, 1, prof);
+        if (nw == 2) k_fwd_p<LC, 2><<<grid, blk, 0, s>>>(a);
+        else k_fwd_p<LC, 1><<<grid, blk, 0, s>>>(a);
+    }
+    c->launches += 2;
+}
+
+template <int LC>
+static void launch_bwd(swd_ctx *c, const BwdArgs &a, dim3 grid, bool prof)
+{
+    dim3 blk(32, 8);
+    {
+        ProfScope ps(c, 2, prof);
+        k_bwd_1<LC><<<grid, blk, 0, c->stream>>>(a);
+    }
+    {
+        ProfScope ps(c, 3, prof);
+        k_bwd_2<LC><<<grid, blk, 0, c->stream>>>(a);
+    }
+    c->launches += 2;
+}
+
+#define LC_DISPATCH(LCV, FN, ...)                                \
+    switch (LCV) {                                               \
+        case 1: FN<1>(__VA_ARGS__); break;                       \
+        case 2: FN<2>(__VA_ARGS__); break;                       \
+        case 3: FN<3>(__VA_ARGS__); break;                       \
+        case 4: FN<4>(__VA_ARGS__); break;                       \
+        case 5: FN<5>(__VA_ARGS__); break;                       \
+        case 6: FN<6>(__VA_ARGS__); break;                       \
+        case 7: FN<7>(__VA_ARGS__); break;                       \
+        default: FN<8>(__VA_ARGS__); break;                      \
+    }
+
+// twiddle table exp(-2 pi i j / N), j < N/2, built in double on the host
+static int make_twiddles(swd_ctx *ctx, DevBuf &buf, int N)
+{
+    std::vector<float2> h(N / 2);
+    for (int j = 0; j < N / 2; j++) {
+        const double a = -2.0 * M_PI * (double)j / (double)N;
+        h[j] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    CKR(ensure(ctx, buf, sizeof(float2) * h.size()));
+    CK(cudaMemcpyAsync(buf.p, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SWD_OK;
+}
+
+static int ilog2(int n)
+{
+    int l = 0;
+    while ((1 << l) < n) l++;
+    return l;
+}
+
+// ------------------------------------------------------------------------------------
+// forward pass shared by swd_forward and swd_rtm_shot
+// ------------------------------------------------------------------------------------
+struct FwdJob {
+    const swd_shot *shot;
+    std::vector<float> rick, hrick;
+    bool twin = false, save_strips = false;
+    float *seis_dev = nullptr;
+    float2 *colbuf = nullptr;
+};
+
+static int strip_len(const swd_ctx *c) { return 2 * c->Lc * c->nx + 2 * c->Lc * (c->nz - 2 * c->Lc); }
+
+static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
+{
+    const swd_shot *s = J.shot;
+    const int nt = s->nt;
+    CKR(zero_wave(ctx, 0));
+    if (J.twin) CKR(zero_wave(ctx, 1));
+    FwdArgs a;
+    memset(&a, 0, sizeof a);
+    a.g = make_geo(ctx);
+    a.c = make_cpml(ctx);
+    a.vp = F(ctx->vp);
+    a.rho = F(ctx->rho);
+    a.w[0] = make_wave(ctx, 0);
+    a.w[1] = J.twin ? make_wave(ctx, 1) : make_wave(ctx, 0);
+    a.sx = s->s_ix;
+    a.sz = s->s_iz;
+    a.nt = nt;
+    a.wells.wcol = I32(ctx->wcol);
+    a.wells.wmap = I32(ctx->wmap);
+    a.seis = J.seis_dev;
+    a.colmap = J.colbuf ? I32(ctx->wcol) : nullptr;
+    a.colbuf = J.colbuf;
+    const dim3 grid = grid_blocks(ctx);
+    if (J.save_strips) {
+        const int slen = strip_len(ctx);
+        const int nscale = grid.x * grid.y;
+        const size_t esz = ctx->strip_prec == SWD_STRIP_F32 ? 4 : 2;
+        CKR(ensure(ctx, ctx->strips, esz * (size_t)slen * nt));
+        a.strips.buf = ctx->strips.p;
+        a.strips.slen = slen;
+        a.strips.prec = ctx->strip_prec;
+        a.strips.nscale = nscale;
+        if (ctx->strip_prec != SWD_STRIP_F32) {
+            CKR(ensure(ctx, ctx->strip_scale, sizeof(float) * (size_t)nscale * nt));
+            a.strips.scale = F(ctx->strip_scale);
+        }
+    }
+    for (int it = 0; it < nt; it++) {
+        a.it = it;
+        a.amp[0] = J.rick[it];
+        a.amp[1] = J.twin ? J.hrick[it] : 0.f;
+        const bool prof = ctx->prof_every > 0 && it % ctx->prof_every == 0;
+        LC_DISPATCH(ctx->Lc, launch_fwd, ctx, a, J.twin ? 2 : 1, grid, prof);
+    }
+    CK(cudaGetLastError());
+    return SWD_OK;
+}
+
+static int check_ready(swd_ctx *ctx)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    if (!ctx->have_rc) return fail(ctx, SWD_ERR_STATE, "stencil coefficients not set (swd_set_stencil)");
+    if (!ctx->have_cpml) return fail(ctx, SWD_ERR_STATE, "CPML profiles not set (swd_set_cpml)");
+    if (!ctx->have_model) return fail(ctx, SWD_ERR_STATE, "model not set (swd_set_model)");
+    CK(cudaSetDevice(ctx->dev));
+    return SWD_OK;
+}
+
+
+// ------------------------------------------------------------------------------------
+// decon geometry (kk_decon_interp_psf_minewindow.cpp:84-132)
+// ------------------------------------------------------------------------------------
+static int decon_geo(const swd_decon_params *p, DeconGeo &g)
+{
+    if (!p || p->nx < 1 || p->nz < 1) return SWD_ERR_ARG;
+    if (p->psfwinx % 2 == 0 || p->psfwinz % 2 == 0 || p->filterwinx % 2 == 0 || p->filterwinz % 2 == 0) return SWD_ERR_ARG;
+    if (p->psfwinx < 1 || p->psfwinz < 1 || p->snapwinx < 2 || p->snapwinz < 2) return SWD_ERR_ARG;
+    memset(&g, 0, sizeof g);
+    g.nx = p->nx; g.nz = p->nz;
+    g.psfwinx = p->psfwinx; g.psfwinz = p->psfwinz; g.filterwinx = p->filterwinx; g.filterwinz = p->filterwinz;
+    g.snapwinx = p->snapwinx; g.snapwinz = p->snapwinz; g.epsilon = p->epsilon;
+    g.halfpsfwx = p->psfwinx / 2; g.halfpsfwz = p->psfwinz / 2;
+    g.halfltwx = p->filterwinx / 2; g.halfltwz = p->filterwinz / 2;
+    g.nzwpsf = (int)ceil(1.0 * p->nz / p->psfwinz);
+    g.nxwpsf = (int)ceil(1.0 * p->nx / p->psfwinx);
+    const int fullwx = p->filterwinx + p->psfwinx - 1, fullwz = p->filterwinz + p->psfwinz - 1;
+    if (p->fft_nx > 0 && p->fft_nz > 0) {
+        if (p->fft_nx < fullwx || p->fft_nz < fullwz) return SWD_ERR_ARG;
+        g.FX = p->fft_nx; g.FZ = p->fft_nz; g.n0 = g.FX; g.n1 = g.FZ;
+    } else {
+        g.FX = fullwx; g.FZ = fullwz; g.n0 = fullwz; g.n1 = fullwx;
+    }
+    g.midpx = g.FX / 2; g.midpz = g.FZ / 2;
+    g.ocx = g.midpx - g.halfpsfwx; g.ocz = g.midpz - g.halfpsfwz;
+    g.outwinx = 2 * (p->psfwinx / 10) + 2 * p->snapwinx + 1;
+    g.outwinz = 2 * (p->psfwinz / 10) + 2 * p->snapwinz + 1;
+    g.halfoutwx = g.outwinx / 2; g.halfoutwz = g.outwinz / 2;
+    g.stepwinx = g.outwinx - p->snapwinx; g.stepwinz = g.outwinz - p->snapwinz;
+    g.stepnumx = (int)ceil(1.0 * (p->nx + fullwx) / g.stepwinx) + 1;
+    g.stepnumz = (int)ceil(1.0 * (p->nz + fullwz) / g.stepwinz) + 1;
+    g.totalnum = g.stepnumx * g.stepnumz;
+    g.nxp = g.stepnumx * g.stepwinx; g.nzp = g.stepnumz * g.stepwinz;
+    if (p->filterwinx < p->psfwinx || p->filterwinz < p->psfwinz) return SWD_ERR_ARG;
+    if (p->filterwinx < g.outwinx || p->filterwinz < g.outwinz) return SWD_ERR_ARG;
+    if (g.n0 > 512 || g.n1 > 512 || (size_t)g.FX * g.FZ * 8 + (g.n0 + g.n1) * 8 > 200 * 1024) return SWD_ERR_ARG;
+    // the PSF lattice must hold at least 7 cells per axis so the clamp range [3, n-4] exists
+    if (g.nxwpsf < 7 || g.nzwpsf < 7) return SWD_ERR_ARG;
+    return SWD_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------
+extern "C" {
+
+int swd_version(void) { return 10000; }
+
+int swd_device_count(int *n)
+{
+    if (!n) return SWD_ERR_ARG;
+    cudaError_t e = cudaGetDeviceCount(n);
+    if (e != cudaSuccess) { *n = 0; return SWD_ERR_CUDA; }
+    return SWD_OK;
+}
+
+int swd_create(swd_ctx **out, const swd_grid *g)
+{
+    if (!out || !g) return SWD_ERR_ARG;
+    *out = nullptr;
+    if (g->nx < 1 || g->nz < 1 || g->pml < 0 || g->Lc < 1 || g->Lc > MAXLC || g->nt_max < 2 || !(g->dx > 0) ||
+        !(g->dz > 0) || !(g->dt > 0))
+        return SWD_ERR_ARG;
+    if (g->nx < 2 * g->Lc + 1 || g->nz < 2 * g->Lc + 1) return SWD_ERR_ARG;
+    swd_ctx *ctx = new swd_ctx();
+    ctx->grid = *g;
+    ctx->dev = g->device;
+    ctx->Lc = g->Lc;
+    ctx->pmlc = g->pml + g->Lc;
+    ctx->nx = g->nx;
+    ctx->nz = g->nz;
+    ctx->ntx = g->nx + 2 * ctx->pmlc;
+    ctx->ntz = g->nz + 2 * ctx->pmlc;
+    ctx->ldz = (ctx->ntz + 31) / 32 * 32;
+    cudaError_t e = cudaSetDevice(ctx->dev);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return SWD_ERR_CUDA;
+    }
+    *out = ctx;
+    return SWD_OK;
+}
+
+int swd_destroy(swd_ctx *ctx)
+{
+    if (!ctx) return SWD_OK;
+    cudaSetDevice(ctx->dev);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (DevBuf *b : ctx->bufs)
+        if (b->p) cudaFree(b->p);
+    prof_collect(ctx);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SWD_OK;
+}
+
+const char *swd_last_error(const swd_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int swd_set_stream(swd_ctx *ctx, void *stream)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    if (ctx->own_stream && ctx->stream) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(cudaStreamDestroy(ctx->stream));
+    }
+    ctx->stream = (cudaStream_t)stream;
+    ctx->own_stream = false;
+    return SWD_OK;
+}
+
+int swd_synchronize(swd_ctx *ctx)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SWD_OK;
+}
+
+size_t swd_device_bytes(const swd_ctx *ctx)
+{
+    size_t n = 0;
+    if (ctx)
+        for (const DevBuf *b : ctx->bufs) n += b->n;
+    return n;
+}
+
+int swd_profile(swd_ctx *ctx, int every)
+{
+    if (!ctx || every < 0) return SWD_ERR_ARG;
+    ctx->prof_every = every;
+    return SWD_OK;
+}
+
+int swd_profile_read(swd_ctx *ctx, double *ms, long long *launches)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    prof_collect(ctx);
+    for (int k = 0; k < SWD_NKERNELS; k++) {
+        if (ms) ms[k] = ctx->prof_ms[k];
+        if (launches) launches[k] = ctx->prof_n[k];
+        ctx->prof_ms[k] = 0.0;
+        ctx->prof_n[k] = 0;
+    }
+    return SWD_OK;
+}
+
+long long swd_launch_count(const swd_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int swd_set_stencil(swd_ctx *ctx, const float *rc)
+{
+    if (!ctx || !rc) return fail(ctx, SWD_ERR_ARG, "rc is NULL");
+    std::vector<float> h;
+    CKR(host_copy(ctx, h, rc, ctx->Lc));
+    for (int i = 0; i < MAXLC; i++) ctx->rc[i] = i < ctx->Lc ? h[i] : 0.f;
+    ctx->have_rc = true;
+    return SWD_OK;
+}
+
+int swd_set_cpml(swd_ctx *ctx, const float *a_x, const float *a_x_half, const float *a_z, const float *a_z_half,
+                 const float *b_x, const float *b_x_half, const float *b_z, const float *b_z_half)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    const float *src[8] = {a_x, a_x_half, a_z, a_z_half, b_x, b_x_half, b_z, b_z_half};
+    CK(cudaSetDevice(ctx->dev));
+    for (int i = 0; i < 8; i++) {
+        if (!src[i]) return fail(ctx, SWD_ERR_ARG, "CPML array %d is NULL", i);
+        const int n = (i % 4) < 2 ? ctx->ntx : ctx->ntz;
+        CKR(ensure(ctx, ctx->cpml[i], sizeof(float) * n));
+        CKR(to_dev(ctx, ctx->cpml[i].p, src[i], sizeof(float) * n));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->have_cpml = true;
+    return SWD_OK;
+}
+
+int swd_set_model(swd_ctx *ctx, const float *vp, const float *rho)
+{
+    if (!ctx || !vp || !rho) return fail(ctx, SWD_ERR_ARG, "vp/rho is NULL");
+    CK(cudaSetDevice(ctx->dev));
+    // one extra column and row of padding so the half-node buoyancy reads at x+1 / z+1
+    // of the last cells stay inside the allocation
+    const size_t bytes = (size_t)(ctx->ntx + 1) * ctx->ldz * sizeof(float);
+    CKR(ensure(ctx, ctx->vp, bytes));
+    CKR(ensure(ctx, ctx->rho, bytes));
+    CK(cudaMemsetAsync(ctx->vp.p, 0, bytes, ctx->stream));
+    CK(cudaMemsetAsync(ctx->rho.p, 0, bytes, ctx->stream));
+    CKR(grid_to_dev(ctx, F(ctx->vp), vp));
+    CKR(grid_to_dev(ctx, F(ctx->rho), rho));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->have_model = true;
+    return SWD_OK;
+}
+
+int swd_set_strip_precision(swd_ctx *ctx, int prec)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    if (prec != SWD_STRIP_F32 && prec != SWD_STRIP_F16 && prec != SWD_STRIP_BF16)
+        return fail(ctx, SWD_ERR_ARG, "unknown strip precision %d", prec);
+    ctx->strip_prec = prec;
+    return SWD_OK;
+}
+
+int swd_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *hrick, const float *kz_coef,
+                float *seis, float *seis_up, float *seis_down)
+{
+    CKR(check_ready(ctx));
+    if (!rick || !seis) return fail(ctx, SWD_ERR_ARG, "rick and seis are required");
+    const bool twin = hrick != nullptr && kz_coef != nullptr;
+    if ((seis_up || seis_down) && !twin) return fail(ctx, SWD_ERR_ARG, "seis_up/seis_down need hrick and kz_coef");
+    ShotPlan P;
+    CKR(plan_shot(ctx, shot, P));
+    const int nt = shot->nt, r_n = shot->r_n;
+    FwdJob J;
+    J.shot = shot;
+    CKR(host_copy(ctx, J.rick, rick, nt));
+    if (twin) CKR(host_copy(ctx, J.hrick, hrick, nt));
+    J.twin = twin;
+    CKR(ensure(ctx, ctx->seis, sizeof(float) * (size_t)r_n * nt));
+    CK(cudaMemsetAsync(ctx->seis.p, 0, sizeof(float) * (size_t)r_n * nt, ctx->stream));
+    J.seis_dev = F(ctx->seis);
+    const int N = swd_prep_pow2(ctx->ntz);
+    if (twin) {
+        CKR(ensure(ctx, ctx->colbuf, sizeof(float2) * (size_t)P.nwells * nt * ctx->ldz));
+        J.colbuf = (float2 *)ctx->colbuf.p;
+    }
+    CKR(run_forward(ctx, J, P));
+    CKR(copy_aliases(ctx, P, F(ctx->seis), nt));
+    CKR(from_dev(ctx, seis, ctx->seis.p, sizeof(float) * (size_t)r_n * nt));
+    if (twin) {
+        CKR(ensure(ctx, ctx->kzcoef, sizeof(float) * N));
+        CKR(to_dev(ctx, ctx->kzcoef.p, kz_coef, sizeof(float) * N));
+        CKR(make_twiddles(ctx, ctx->tw, N));
+        CKR(ensure(ctx, ctx->seis2, sizeof(float) * 2 * (size_t)r_n * nt));
+        float *up = F(ctx->seis2), *dn = up + (size_t)r_n * nt;
+        CK(cudaMemsetAsync(up, 0, sizeof(float) * 2 * (size_t)r_n * nt, ctx->stream));
+        const size_t sm = 2 * sizeof(float2) * N;
+        CK(cudaFuncSetAttribute(k_kzsep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_kzsep<<<dim3(nt, P.nwells), 256, sm, ctx->stream>>>((const float2 *)ctx->colbuf.p, F(ctx->kzcoef),
+                                                               (const float2 *)ctx->tw.p, I32(ctx->wmap), up, dn, nt,
+                                                               ctx->ntz, ctx->ldz, N, ilog2(N));
+        ctx->launches++;
+        CK(cudaGetLastError());
+        CKR(copy_aliases(ctx, P, up, nt));
+        CKR(copy_aliases(ctx, P, dn, nt));
+        if (seis_up) CKR(from_dev(ctx, seis_up, up, sizeof(float) * (size_t)r_n * nt));
+        if (seis_down) CKR(from_dev(ctx, seis_down, dn, sizeof(float) * (size_t)r_n * nt));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    prof_collect(ctx);
+    return SWD_OK;
+}
+
+int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *data, unsigned flags, float *syn,
+                 float *image_pp, float *image_src, float *fimage)
+{
+    CKR(check_ready(ctx));
+    if (!rick || !data) return fail(ctx, SWD_ERR_ARG, "rick and data are required");
+    ShotPlan P;
+    CKR(plan_shot(ctx, shot, P));
+    const int nt = shot->nt, r_n = shot->r_n;
+    const size_t ntr = (size_t)r_n * nt;
+    FwdJob J;
+    J.shot = shot;
+    CKR(host_copy(ctx, J.rick, rick, nt));
+    J.save_strips = true;
+    CKR(ensure(ctx, ctx->seis, sizeof(float) * ntr));
+    CK(cudaMemsetAsync(ctx->seis.p, 0, sizeof(float) * ntr, ctx->stream));
+    J.seis_dev = F(ctx->seis);
+    // 1. forward pass with boundary strips; the final state stays in wave[0]
+    CKR(run_forward(ctx, J, P));
+    if (syn) {
+        CKR(copy_aliases(ctx, P, F(ctx->seis), nt));
+        CKR(from_dev(ctx, syn, ctx->seis.p, sizeof(float) * ntr));
+    }
+    // 2. receiver data, -int int dt dt
+    CKR(ensure(ctx, ctx->rdata, sizeof(float) * 2 * ntr));
+    float *raw = F(ctx->rdata), *rms = raw + ntr;
+    CKR(to_dev(ctx, raw, data, sizeof(float) * ntr));
+    if (flags & SWD_RTM_PREPROCESS) {
+        k_preprocess<<<(r_n + 127) / 128, 128, 0, ctx->stream>>>(raw, rms, r_n, nt, ctx->grid.dt);
+        ctx->launches++;
+        CK(cudaGetLastError());
+    } else {
+        CK(cudaMemcpyAsync(rms, raw, sizeof(float) * ntr, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    // 3. backward: reconstruction + receiver back-propagation + FP64 imaging
+    CKR(zero_wave(ctx, 1));
+    const size_t gb = (size_t)ctx->ntx * ctx->ldz;
+    CKR(ensure(ctx, ctx->dpdt, sizeof(float) * gb));
+    CK(cudaMemsetAsync(ctx->dpdt.p, 0, sizeof(float) * gb, ctx->stream));
+    CKR(ensure(ctx, ctx->I, sizeof(double) * gb));
+    CKR(ensure(ctx, ctx->S, sizeof(double) * gb));
+    CK(cudaMemsetAsync(ctx->I.p, 0, sizeof(double) * gb, ctx->stream));
+    CK(cudaMemsetAsync(ctx->S.p, 0, sizeof(double) * gb, ctx->stream));
+    ctx->have_R = (flags & SWD_RTM_ILLUM_RCV) != 0;
+    if (ctx->have_R) {
+        CKR(ensure(ctx, ctx->R, sizeof(double) * gb));
+        CK(cudaMemsetAsync(ctx->R.p, 0, sizeof(double) * gb, ctx->stream));
+    }
+    BwdArgs b;
+    memset(&b, 0, sizeof b);
+    b.g = make_geo(ctx);
+    b.c = make_cpml(ctx);
+    b.vp = F(ctx->vp);
+    b.rho = F(ctx->rho);
+    b.s = make_wave(ctx, 0);
+    b.r = make_wave(ctx, 1);
+    b.dpdt = F(ctx->dpdt);
+    b.sx = shot->s_ix;
+    b.sz = shot->s_iz;
+    b.nt = nt;
+    b.strips.buf = ctx->strips.p;
+    b.strips.scale = F(ctx->strip_scale);
+    b.strips.slen = strip_len(ctx);
+    b.strips.prec = ctx->strip_prec;
+    b.strips.nscale = grid_blocks(ctx).x * grid_blocks(ctx).y;
+    b.wells.wcol = I32(ctx->wcol);
+    b.wells.wmap = I32(ctx->wmap);
+    b.rdata = rms;
+    b.I = D(ctx->I);
+    b.S = D(ctx->S);
+    b.R = ctx->have_R ? D(ctx->R) : nullptr;
+    const dim3 grid = grid_blocks(ctx);
+    for (int it = nt - 2; it >= 0; it--) {
+        b.it = it;
+        b.sub = J.rick[it + 1];
+        const bool prof = ctx->prof_every > 0 && it % ctx->prof_every == 0;
+        LC_DISPATCH(ctx->Lc, launch_bwd, ctx, b, grid, prof);
+    }
+    CK(cudaGetLastError());
+    // 4. per-shot post and stack
+    CKR(ensure(ctx, ctx->reduce, 64));
+    CK(cudaMemsetAsync(ctx->reduce.p, 0, 8, ctx->stream));
+    k_max_nonneg<<<592, 256, 0, ctx->stream>>>(D(ctx->S), gb, (unsigned long long *)ctx->reduce.p);
+    ctx->launches += 2;   // with k_rtm_post below
+    const size_t nimg = (size_t)ctx->nx * ctx->nz;
+    if (!ctx->stack.p) {
+        CKR(ensure(ctx, ctx->stack, sizeof(double) * nimg));
+        CK(cudaMemsetAsync(ctx->stack.p, 0, sizeof(double) * nimg, ctx->stream));
+    }
+    CKR(ensure(ctx, ctx->stage_out, sizeof(float) * 3 * nimg));
+    float *o_pp = F(ctx->stage_out), *o_src = o_pp + nimg, *o_f = o_src + nimg;
+    k_rtm_post<<<dim3((ctx->nz + 31) / 32, (ctx->nx + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(
+        D(ctx->I), D(ctx->S), F(ctx->vp), (const unsigned long long *)ctx->reduce.p, ctx->ntx, ctx->ntz, ctx->ldz,
+        ctx->pmlc, ctx->grid.dx, ctx->grid.dz, o_pp, o_src, o_f, (flags & SWD_RTM_NO_STACK) ? nullptr : D(ctx->stack));
+    CK(cudaGetLastError());
+    if (image_pp) CKR(from_dev(ctx, image_pp, o_pp, sizeof(float) * nimg));
+    if (image_src) CKR(from_dev(ctx, image_src, o_src, sizeof(float) * nimg));
+    if (fimage) CKR(from_dev(ctx, fimage, o_f, sizeof(float) * nimg));
+    CK(cudaStreamSynchronize(ctx->stream));
+    prof_collect(ctx);
+    ctx->have_shot = true;
+    return SWD_OK;
+}
+
+int swd_rtm_raw(swd_ctx *ctx, double *image, double *illum_src, double *illum_rcv)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    if (!ctx->have_shot) return fail(ctx, SWD_ERR_STATE, "no RTM shot has run");
+    if (illum_rcv && !ctx->have_R) return fail(ctx, SWD_ERR_STATE, "receiver illumination was not accumulated");
+    CK(cudaSetDevice(ctx->dev));
+    double *dst[3] = {image, illum_src, illum_rcv};
+    DevBuf *src[3] = {&ctx->I, &ctx->S, &ctx->R};
+    for (int k = 0; k < 3; k++) {
+        if (!dst[k]) continue;
+        CK(cudaMemcpy2DAsync(dst[k], ctx->ntz * sizeof(double), src[k]->p, ctx->ldz * sizeof(double),
+                             ctx->ntz * sizeof(double), ctx->ntx,
+                             is_device_ptr(dst[k]) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SWD_OK;
+}
+
+int swd_stack_get(swd_ctx *ctx, int edge_zero, float *migration)
+{
+    if (!ctx || !migration) return SWD_ERR_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    const size_t nimg = (size_t)ctx->nx * ctx->nz;
+    if (!ctx->stack.p) {
+        CKR(ensure(ctx, ctx->stack, sizeof(double) * nimg));
+        CK(cudaMemsetAsync(ctx->stack.p, 0, sizeof(double) * nimg, ctx->stream));
+    }
+    CKR(ensure(ctx, ctx->stage_in, sizeof(float) * nimg));
+    k_stack_out<<<296, 256, 0, ctx->stream>>>(D(ctx->stack), F(ctx->stage_in), ctx->nx, ctx->nz, ctx->Lc, edge_zero);
+    CK(cudaGetLastError());
+    CKR(from_dev(ctx, migration, ctx->stage_in.p, sizeof(float) * nimg));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SWD_OK;
+}
+
+int swd_stack_reset(swd_ctx *ctx)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    if (ctx->stack.p) CK(cudaMemsetAsync(ctx->stack.p, 0, ctx->stack.n, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SWD_OK;
+}
+
+int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *const *ricks, const float *const *data,
+                  unsigned flags)
+{
+    if (!ctx || nshots < 0 || (nshots > 0 && (!shots || !ricks || !data))) return fail(ctx, SWD_ERR_ARG, "bad batch");
+    for (int i = 0; i < nshots; i++)
+        CKR(swd_rtm_shot(ctx, &shots[i], ricks[i], data[i], flags, nullptr, nullptr, nullptr, nullptr));
+    return SWD_OK;
+}
+
+int swd_hilbert(swd_ctx *ctx, int nt, const float *rick, float *hrick)
+{
+    if (!ctx || !rick || !hrick || nt < 2) return fail(ctx, SWD_ERR_ARG, "bad hilbert arguments");
+    CK(cudaSetDevice(ctx->dev));
+    const int N = swd_prep_pow2(nt);
+    if (N < 32 || N > 16384) return fail(ctx, SWD_ERR_ARG, "Hilbert length %d outside [32, 16384]", N);
+    DevBuf tw, io;
+    CKR(make_twiddles(ctx, tw, N));
+    CKR(ensure(ctx, io, sizeof(float) * 2 * nt));
+    CKR(to_dev(ctx, io.p, rick, sizeof(float) * nt));
+    const size_t sm = sizeof(float2) * N;
+    CK(cudaFuncSetAttribute(k_hilbert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_hilbert<<<1, 256, sm, ctx->stream>>>(F(io), F(io) + nt, (const float2 *)tw.p, nt, N, ilog2(N));
+    cudaError_t e = cudaGetLastError();
+    int rc = SWD_OK;
+    if (e != cudaSuccess) rc = fail(ctx, SWD_ERR_CUDA, "k_hilbert: %s", cudaGetErrorString(e));
+    if (rc == SWD_OK) rc = from_dev(ctx, hrick, F(io) + nt, sizeof(float) * nt);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(tw.p);
+    cudaFree(io.p);
+    return rc;
+}
+
+int swd_smooth(swd_ctx *ctx, int ntx, int ntz, int pml, int window, float *vp)
+{
+    if (!ctx || !vp || ntx <= 2 * pml || ntz <= 2 * pml || window < 0 || window > 64)
+        return fail(ctx, SWD_ERR_ARG, "bad smoothing arguments");
+    CK(cudaSetDevice(ctx->dev));
+    // normalised Gaussian of ini_model_mine (acoustic_HLVSPRTMC.cpp:1475-1501), built on the host
+    const int wx = 2 * window + 1;
+    const double PI = 3.1415926, sigma = window / 2.0;
+    std::vector<double> coef(wx * wx);
+    double sum = 0.0;
+    for (int ix = 0; ix < wx; ix++)
+        for (int iz = 0; iz < wx; iz++) {
+            int ip = ix * wx + iz;
+            coef[ip] = 1.0 / (2.0 * PI * sigma * sigma) *
+                       exp(-((ix - window) * (ix - window) + (iz - window) * (iz - window)) / (2.0 * sigma * sigma));
+            sum += coef[ip];
+        }
+    for (auto &c : coef) c /= sum;
+    const size_t n = (size_t)ntx * ntz;
+    DevBuf a, b, cf;
+    int rc = ensure(ctx, a, sizeof(float) * n);
+    if (rc == SWD_OK) rc = ensure(ctx, b, sizeof(float) * n);
+    if (rc == SWD_OK) rc = ensure(ctx, cf, sizeof(double) * coef.size());
+    if (rc == SWD_OK) rc = to_dev(ctx, a.p, vp, sizeof(float) * n);
+    if (rc == SWD_OK) {
+        cudaMemcpyAsync(cf.p, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(b.p, a.p, sizeof(float) * n, cudaMemcpyDeviceToDevice, ctx->stream);
+        k_smooth<<<dim3((ntz - 2 * pml + 31) / 32, (ntx - 2 * pml + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(
+            F(a), F(b), D(cf), ntx, ntz, pml, window);
+        k_pml_x<<<(ntz + 127) / 128, 128, 0, ctx->stream>>>(F(b), ntx, ntz, pml);
+        k_pml_z<<<(ntx + 127) / 128, 128, 0, ctx->stream>>>(F(b), ntx, ntz, pml);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(ctx, SWD_ERR_CUDA, "smoothing kernels: %s", cudaGetErrorString(e));
+        else rc = from_dev(ctx, vp, b.p, sizeof(float) * n);
+    }
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(a.p);
+    cudaFree(b.p);
+    cudaFree(cf.p);
+    return rc;
+}
+
+int swd_preprocess(swd_ctx *ctx, int r_n, int nt, float dt, const float *d, float *rms)
+{
+    if (!ctx || !d || !rms || r_n < 1 || nt < 1) return fail(ctx, SWD_ERR_ARG, "bad preprocess arguments");
+    CK(cudaSetDevice(ctx->dev));
+    const size_t n = (size_t)r_n * nt;
+    CKR(ensure(ctx, ctx->stage_in, sizeof(float) * 2 * n));
+    float *a = F(ctx->stage_in), *b = a + n;
+    CKR(to_dev(ctx, a, d, sizeof(float) * n));
+    k_preprocess<<<(r_n + 127) / 128, 128, 0, ctx->stream>>>(a, b, r_n, nt, dt);
+    CK(cudaGetLastError());
+    CKR(from_dev(ctx, rms, b, sizeof(float) * n));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SWD_OK;
+}
+
+
+int swd_decon_geometry(const swd_decon_params *p, int *windows, int *fft_nx, int *fft_nz)
+{
+    DeconGeo g;
+    int rc = decon_geo(p, g);
+    if (rc) return rc;
+    if (windows) *windows = g.totalnum;
+    if (fft_nx) *fft_nx = g.FX;
+    if (fft_nz) *fft_nz = g.FZ;
+    return SWD_OK;
+}
+
+int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, const float *migpsf, float *mig_dec,
+              float *mig_coef)
+{
+    // a NULL context runs on the current device with a temporary stream
+    swd_ctx tmp;
+    swd_ctx *ctx = ctx_in ? ctx_in : &tmp;
+    if (!ctx_in) {
+        cudaGetDevice(&tmp.dev);
+        if (cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking) != cudaSuccess) return SWD_ERR_CUDA;
+    }
+    int rc = SWD_OK;
+    do {
+        DeconGeo g;
+        if (!migreal || !migpsf || !mig_dec || !mig_coef) { rc = fail(ctx, SWD_ERR_ARG, "decon: NULL array"); break; }
+        if (decon_geo(p, g) != SWD_OK) { rc = fail(ctx, SWD_ERR_ARG, "decon: invalid window geometry"); break; }
+        if (cudaSetDevice(ctx->dev) != cudaSuccess) { rc = fail(ctx, SWD_ERR_CUDA, "cudaSetDevice"); break; }
+        // Hann-edged output taper (:355-383), built on the host with the reference's arithmetic
+        const double PI = 3.1415926;
+        std::vector<float> coefr((size_t)g.outwinx * g.outwinz);
+        for (int ix = 0; ix < g.outwinx; ix++)
+            for (int iz = 0; iz < g.outwinz; iz++) {
+                float cx, cz;
+                if (ix <= p->snapwinx - 1) cx = 0.5000 - 0.5 * cos(PI * ix / (p->snapwinx - 1));
+                else if (ix >= g.outwinx - p->snapwinx) cx = 0.5000 + 0.5 * cos(PI * (ix - g.outwinx + p->snapwinx) / (p->snapwinx - 1));
+                else cx = 1.0;
+                if (iz <= p->snapwinz - 1) cz = 0.5000 - 0.5 * cos(PI * iz / (p->snapwinz - 1));
+                else if (iz >= g.outwinz - p->snapwinz) cz = 0.5000 + 0.5 * cos(PI * (iz - g.outwinz + p->snapwinz) / (p->snapwinz - 1));
+                else cz = 1.0;
+                coefr[(size_t)ix * g.outwinz + iz] = cx * cz;
+            }
+        const size_t np = (size_t)g.nx * g.nz, nout = coefr.size();
+        DevBuf bin, bcoef, bwin, bout;
+        rc = ensure(ctx, bin, sizeof(float) * 2 * np);
+        if (!rc) rc = ensure(ctx, bcoef, sizeof(float) * nout);
+        if (!rc) rc = ensure(ctx, bwin, sizeof(float) * nout * g.totalnum);
+        if (!rc) rc = ensure(ctx, bout, sizeof(float) * 2 * np);
+        if (!rc) rc = to_dev(ctx, bin.p, migreal, sizeof(float) * np);
+        if (!rc) rc = to_dev(ctx, F(bin) + np, migpsf, sizeof(float) * np);
+        if (!rc && cudaMemcpyAsync(bcoef.p, coefr.data(), sizeof(float) * nout, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+            rc = fail(ctx, SWD_ERR_CUDA, "decon: coefficient upload");
+        if (!rc) {
+            const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + g.n0 + g.n1);
+            cudaFuncSetAttribute(k_decon_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k_decon_window<<<g.totalnum, 512, sm, ctx->stream>>>(g, F(bin), F(bin) + np, F(bcoef), F(bwin));
+            k_decon_gather<<<592, 256, 0, ctx->stream>>>(g, F(bwin), F(bcoef), F(bout), F(bout) + np);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) rc = fail(ctx, SWD_ERR_CUDA, "decon kernels: %s", cudaGetErrorString(e));
+        }
+        if (!rc) rc = from_dev(ctx, mig_dec, bout.p, sizeof(float) * np);
+        if (!rc) rc = from_dev(ctx, mig_coef, F(bout) + np, sizeof(float) * np);
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (!rc && e != cudaSuccess) rc = fail(ctx, SWD_ERR_CUDA, "decon: %s", cudaGetErrorString(e));
+        cudaFree(bin.p); cudaFree(bcoef.p); cudaFree(bwin.p); cudaFree(bout.p);
+    } while (0);
+    if (!ctx_in) cudaStreamDestroy(tmp.stream);
+    return rc;
+}
+
+}  // extern "C"

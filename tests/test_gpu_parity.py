@@ -1,0 +1,257 @@
+"""GPU parity tests: libswd (through its C ABI) against the CPU oracle on the same seeded
+inputs, and against the outputs of the reference's own CUDA build.
+
+Tolerances (relative L2): seismograms, RTM images and PSF images 1e-4 against the FP32 and
+FP64 oracles; deconvolved image 1e-3; integer/index work, smoothing and preprocessing exact.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4        # FP32 seismograms / images
+TOL_DECON = 1e-3  # deconvolved image
+
+
+class Case:
+    """One small model set up identically for the engine and the oracle."""
+
+    def __init__(self, swd, orc, nx=100, nz=60, pml=10, Lc=4, nt=400, dx=5.0, dz=5.0, dt=5e-4, f0=25.0,
+                 seed=7, geometry="wells", smooth=0, rho_pert=False):
+        rng = np.random.default_rng(seed)
+        v = np.full((nx, nz), 1900.0, np.float32)
+        v[:, nz // 3:] = 2400.0
+        v[:, 2 * nz // 3:] = 3000.0
+        v += rng.uniform(-60, 60, v.shape).astype(np.float32)
+        self.nx, self.nz, self.pml, self.Lc, self.nt = nx, nz, pml, Lc, nt
+        self.pmlc = pmlc = pml + Lc
+        self.dx, self.dz, self.dt, self.f0 = dx, dz, dt, f0
+        self.vp = orc.pad_model(v, pmlc)
+        if smooth:
+            self.vp = orc.smooth(self.vp, pmlc, smooth)
+        self.rho = np.full_like(self.vp, 1000.0)
+        if rho_pert:
+            self.rho[pmlc + 20::11, pmlc + 20:-pmlc - 5:11] += self.vp[pmlc + 20::11, pmlc + 20:-pmlc - 5:11] * 1e-3
+        self.ntx, self.ntz = self.vp.shape
+        self.cp = orc.cpml(self.ntx, self.ntz, pmlc, dx, dz, dt)
+        self.rc = orc.cal_xishu(Lc)
+        self.rick = orc.ricker(nt, f0, dt)
+        if geometry == "wells":
+            self.rix, self.riz = orc.well_geometry(nx, nz, pmlc, dz, 0.0, 1e9)
+        else:   # scattered receivers incl. a duplicated cell and cells on the PML edge
+            self.rix = np.array([pmlc + 40, pmlc + 40, pmlc + 41, pmlc + 7, self.ntx - 1, 3, pmlc + 40], np.int32)
+            self.riz = np.array([pmlc + 5, pmlc + 30, pmlc + 5, pmlc + 50, self.ntz // 2, 2, pmlc + 5], np.int32)
+        self.sx, self.sz = pmlc + nx // 4, pmlc
+        self.M = orc.Model(self.vp, self.rho, self.cp, self.rc, pmlc, Lc, nt, dx, dz, dt)
+        self.G = orc.Geom(self.sx, self.sz, self.rix, self.riz)
+        self.E = swd.Engine(nx, nz, pml, Lc, dx, dz, dt, nt)
+        self.E.set_stencil(self.rc)
+        self.E.set_cpml(self.cp)
+        self.E.set_model(self.vp, self.rho)
+        self.shot = swd.ShotSpec(self.sx, self.sz, self.rix, self.riz, nt)
+
+
+@pytest.fixture(scope="module")
+def case(swd, orc):
+    return Case(swd, orc)
+
+
+def test_forward_matches_oracle(case, orc):
+    seis = case.E.forward(case.shot, case.rick)
+    o32 = orc.forward(case.M, case.G, case.rick)["seis"]
+    o64 = orc.forward(case.M, case.G, case.rick, dtype=np.float64)["seis"]
+    assert np.abs(seis).max() > 0
+    assert rel_l2(seis, o32) < TOL
+    assert rel_l2(seis, o64) < TOL
+
+
+@pytest.mark.parametrize("shape", [(37, 29, 5, 4), (64, 48, 10, 5), (97, 33, 3, 2), (130, 71, 30, 4)])
+def test_forward_odd_grids_and_orders(swd, orc, shape):
+    nx, nz, pml, Lc = shape
+    c = Case(swd, orc, nx=nx, nz=nz, pml=pml, Lc=Lc, nt=220)
+    seis = c.E.forward(c.shot, c.rick)
+    o64 = orc.forward(c.M, c.G, c.rick, dtype=np.float64)["seis"]
+    assert rel_l2(seis, o64) < TOL
+
+
+def test_forward_scattered_receivers_and_duplicates(swd, orc):
+    c = Case(swd, orc, geometry="scattered", nt=260)
+    seis = c.E.forward(c.shot, c.rick)
+    o64 = orc.forward(c.M, c.G, c.rick, dtype=np.float64)["seis"]
+    assert rel_l2(seis, o64) < TOL
+    assert np.array_equal(seis[0], seis[6])        # same cell -> same trace
+
+
+def test_hilbert_matches_oracle(case, orc):
+    for nt in (400, 2000, 2048, 6000):
+        r = orc.ricker(nt, 25.0, 5e-4)
+        assert rel_l2(case.E.hilbert(r), orc.hilbert1d(r)) < 1e-5
+
+
+def test_kz_separation_matches_oracle(case, swd, orc):
+    hr = orc.hilbert1d(case.rick)
+    nfftz = swd.pow2(case.ntz)
+    coef, layer = swd.kz_taper(nfftz, case.dz)
+    assert layer > 0
+    seis, up, dn = case.E.forward(case.shot, case.rick, hrick=hr, kz_coef=coef)
+    cols = [case.pmlc, case.ntx - case.pmlc - 1]
+    fw = orc.forward(case.M, case.G, case.rick, hrick=hr, col_ix=cols, dtype=np.float64)
+    rec_col = (case.rix != case.pmlc).astype(np.int32)
+    oup, odn = orc.kzsep(fw["cols"], case.ntz, nfftz, coef, rec_col, case.riz, np.float64)
+    assert rel_l2(seis, fw["seis"]) < TOL
+    assert rel_l2(up, oup) < TOL
+    assert rel_l2(dn, odn) < TOL
+    # the split is a partition of the kz axis apart from the taper: up + down ~ nfftz * p
+    assert rel_l2(up + dn, nfftz * seis) < 0.2
+
+
+def test_smoothing_bit_exact(case, orc):
+    kat = np.load(GOLDEN / "ini_vp_kat.npz")
+    a = kat["acc_corner"]
+    pmlc = 21
+    s = case.E.smooth(orc.pad_model(a, pmlc), pmlc, 5)[pmlc:-pmlc, pmlc:-pmlc]
+    assert np.array_equal(s[0:40, 0:40].view(np.uint32), kat["ini_corner"].view(np.uint32))
+    v = orc.pad_model(np.random.default_rng(2).uniform(1500, 4500, (83, 61)).astype(np.float32), 17)
+    for w in (2, 5, 7):
+        assert np.array_equal(case.E.smooth(v, 17, w).view(np.uint32), orc.smooth(v, 17, w).view(np.uint32))
+
+
+def test_preprocess_bit_exact(case, orc):
+    d = np.random.default_rng(3).standard_normal((23, 517)).astype(np.float32)
+    a = case.E.preprocess(d, case.dt)
+    b = orc.preprocess(d, case.dt)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def _rtm(case, orc, data, dtype):
+    sh = orc.rtm_shot(case.M, case.G, case.rick, data, dtype=dtype)
+    norm, fim = orc.rtm_post(case.M, sh["img"], sh["illum"], dtype)
+    return sh, norm, fim
+
+
+def test_rtm_shot_matches_oracle(case, swd, orc):
+    data = orc.forward(case.M, case.G, case.rick)["seis"] * 1.3
+    case.E.stack_reset()
+    out = case.E.rtm_shot(case.shot, case.rick, data, want=("image_pp", "image_src", "fimage", "syn"))
+    I, S, _ = case.E.rtm_raw()
+    p = case.pmlc
+    for dt in (np.float32, np.float64):
+        sh, norm, fim = _rtm(case, orc, data, dt)
+        assert rel_l2(out["syn"], sh["syn"]) < TOL
+        assert rel_l2(I, sh["img"]) < TOL
+        assert rel_l2(S, sh["illum"]) < TOL
+        assert rel_l2(out["image_pp"], norm[p:-p, p:-p]) < TOL
+        assert rel_l2(out["image_src"], sh["illum"][p:-p, p:-p]) < TOL
+        assert rel_l2(out["fimage"], fim) < TOL
+    stack = case.E.stack(edge_zero=True)
+    assert rel_l2(stack, orc.edge_zero(fim.astype(np.float32), case.Lc)) < TOL
+
+
+def test_rtm_receiver_illumination_and_stack_of_two(case, swd, orc):
+    data = orc.forward(case.M, case.G, case.rick)["seis"]
+    case.E.stack_reset()
+    f1 = case.E.rtm_shot(case.shot, case.rick, data, flags=swd.RTM_PREPROCESS | swd.RTM_ILLUM_RCV)["fimage"]
+    _, _, R = case.E.rtm_raw(rcv=True)
+    assert R.max() > 0
+    f2 = case.E.rtm_shot(case.shot, case.rick, 2 * data)["fimage"]
+    st = case.E.stack(edge_zero=False)
+    assert rel_l2(st, f1.astype(np.float64) + f2) < 1e-6
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 2e-3), (2, 1e-2)])
+def test_compressed_strips(case, swd, orc, prec, tol):
+    data = orc.forward(case.M, case.G, case.rick)["seis"]
+    case.E.set_strip_precision(0)
+    ref = case.E.rtm_shot(case.shot, case.rick, data, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK)["image_pp"]
+    case.E.set_strip_precision(prec)
+    got = case.E.rtm_shot(case.shot, case.rick, data, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK)["image_pp"]
+    case.E.set_strip_precision(0)
+    e = rel_l2(got, ref)
+    assert 0 < e < tol
+
+
+def test_psf_density_scatterers(swd, orc):
+    c = Case(swd, orc, rho_pert=True, nt=300, smooth=5)
+    seis = c.E.forward(c.shot, c.rick)
+    o64 = orc.forward(c.M, c.G, c.rick, dtype=np.float64)["seis"]
+    assert rel_l2(seis, o64) < TOL
+
+
+def test_decon_matches_oracle(swd, orc):
+    g = np.load(GOLDEN / "decon_ref.npz")
+    cases = [(120, 100, (11, 11), (21, 21), (5, 5), 5e-4), (130, 97, (11, 9), (25, 21), (5, 4), 1e-3)]
+    for k, (nx, nz, psf, flt, snap, eps) in enumerate(cases):
+        dec, coef = swd.decon(g[f"mig{k}"], g[f"psf{k}"], psf, flt, snap, eps)
+        assert np.array_equal(coef, g[f"coef{k}"])
+        assert rel_l2(dec, g[f"dec{k}"]) < TOL_DECON
+
+
+def test_decon_shipped_geometry(swd, orc):
+    """The reference's own parameters (31^2 PSFs, 71^2 filter, 101^2 prime FFT, 2484 windows)
+    on a seeded 845 x 702 image/PSF pair, against the oracle."""
+    rng = np.random.default_rng(11)
+    nx, nz = 845, 702
+    mig = rng.standard_normal((nx, nz)).astype(np.float32)
+    psf = np.zeros((nx, nz), np.float32)
+    psf[15::31, 15::31] = 1.0
+    psf[16::31, 15::31] = -0.5
+    psf[15::31, 16::31] = 0.25
+    dec, coef = swd.decon(mig, psf, (31, 31), (71, 71), (11, 11), 5e-4)
+    odec, ocoef = orc.decon(nx, nz, mig, psf, (31, 31), (71, 71), (11, 11), 5e-4)
+    assert np.array_equal(coef, ocoef)
+    assert rel_l2(dec, odec) < TOL_DECON
+
+
+@pytest.mark.skipif(not (GOLDEN / "ref_gpu_small.npz").exists(), reason="reference-GPU golden not generated")
+def test_engine_matches_reference_cuda_build(swd, orc):
+    """libswd vs the reference's own CUDA programs (AFor + AVSPRTM) on the golden case."""
+    g = np.load(GOLDEN / "ref_gpu_small.npz")
+    nx, nz, pml, Lc, nt, swin, window = [int(v) for v in g["case"]]
+    pmlc = pml + Lc
+    dx = dz = 5.0
+    dt, f0 = 5e-4, 25.0
+    E = swd.Engine(nx, nz, pml, Lc, dx, dz, dt, nt)
+    vp = swd.pad_model(g["acc_vp"], pmlc)
+    rho = np.full_like(vp, 1000.0)
+    E.setup_default(vp, rho)
+    rick = swd.ricker_wave(nt, f0, dt)
+    hr = E.hilbert(rick)
+    assert rel_l2(hr, g["rick_hilbert"]) < 1e-5
+    rix, riz = swd.well_geometry(nx, nz, pmlc, dz, 0.0, 100.0)
+    shot = swd.ShotSpec(pmlc + 20, pmlc, rix, riz, nt)
+    coef, _ = swd.kz_taper(swd.pow2(vp.shape[1]), dz)
+    obs, up, dn = E.forward(shot, rick, hrick=hr, kz_coef=coef)
+    assert rel_l2(obs, g["obs"]) < TOL
+    assert rel_l2(up, g["obsup"]) < TOL
+    assert rel_l2(dn, g["obsdown"]) < TOL
+    vs = E.smooth(vp, pmlc, window)
+    assert np.array_equal(vs[pmlc:-pmlc, pmlc:-pmlc], g["ini_vp"])
+    E.set_model(vs, rho)
+    E.stack_reset()
+    out = E.rtm_shot(shot, rick, g["obsup"], want=("image_pp", "image_src", "fimage", "syn"))
+    assert rel_l2(out["syn"], g["syn"]) < TOL
+    assert rel_l2(out["image_pp"], g["image_pp"]) < TOL
+    assert rel_l2(out["image_src"], g["image_sources"]) < TOL
+    assert rel_l2(out["fimage"], g["fimage_pp"]) < TOL
+    assert rel_l2(E.stack(edge_zero=True), g["migration_pp"]) < TOL
+    # PSF path: density scatterers on the smoothed model (forward/...HLForC.cpp:697-705)
+    rho_s = rho.copy()
+    for ix in range(pmlc + swin // 2, vp.shape[0] - pmlc - swin // 2):
+        for iz in range(pmlc + swin // 2, vp.shape[1] - pmlc - 5):
+            if (ix - (pmlc + swin // 2)) % swin == 0 and (iz - (pmlc + swin // 2)) % swin == 0:
+                rho_s[ix, iz] += vs[ix, iz] * np.float32(1.0e-3)
+    assert np.array_equal(rho_s[pmlc:-pmlc, pmlc:-pmlc], g["rho_scatter"])
+    E.set_model(vs, rho)
+    s0, u0, _ = E.forward(shot, rick, hrick=hr, kz_coef=coef)
+    E.set_model(vs, rho_s)
+    s1, u1, _ = E.forward(shot, rick, hrick=hr, kz_coef=coef)
+    # the scatter data is a small difference of two large records: compare on its own scale
+    assert rel_l2(s1 - s0, g["scatter"]) < 1e-2
+    assert rel_l2(u1 - u0, g["scatterup"]) < 1e-2
+    E.set_model(vs, rho)
+    E.stack_reset()
+    out = E.rtm_shot(shot, rick, g["scatterup"])
+    assert rel_l2(out["image_pp"], g["image_psf"]) < TOL
+    assert rel_l2(out["fimage"], g["fimage_psf"]) < TOL
