@@ -1,0 +1,342 @@
+#!/usr/bin/env python3
+"""Benchmark: RTM shots/s (and Gcell-updates/s) of one PSF-RTM shot on the 1601 x 801
+configuration (5 m grid, nt = 6000, dt = 0.4 ms, 30 Hz Ricker, 641 well receivers, 30-cell
+CPML, 8th-order stencil), with the roofline of the dominant kernel and a CPU baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one RTM shot: forward modelling with boundary-strip saving, -int int preprocessing
+of the receiver data, source-wavefield reconstruction + receiver back-propagation + FP64
+imaging, illumination normalisation, -vp^2 Laplacian and stacking.
+  value  shots/s with the inputs already in HBM (device pointers into the C ABI);
+  e2e    the same through the C ABI with pinned host buffers: the H2D copy of the data and
+         the D2H copy of the normalised and filtered images are inside the timed region.
+L2 is flushed (a 256 MiB write) before every timed step; steps are timed with CUDA events
+on the stream the library launches on.  Multi-GPU runs are replicas (one shot per rank per
+step, no collective in the data path): value = all ranks' shots / the slowest rank's time.
+
+--impl reference times the CPU implementation of the same shot on the host cores: the
+reference has no CPU propagator, so this is the project's OpenMP restatement of the
+reference's stencil, imaging and preprocessing loops (oracle/, kind "port"), run for a
+bounded number of time steps per sample and extrapolated to the full record.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "simple-wavenumber-deconvolution_b200"
+
+
+def load_pkg():
+    spec = importlib.util.spec_from_file_location("swd_b200", PKG / "__init__.py", submodule_search_locations=[str(PKG)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["swd_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------------------------------
+# workload
+# ------------------------------------------------------------------------------------------
+WORKLOAD = "c2 PSF-RTM shot: 1601x801 @5 m, nt=6000, dt=0.4 ms, 30 Hz, 641 well receivers, pml 30, 8th order"
+
+
+def algorithmic_bytes(kernel, w, cp, strip_len, r_n):
+    """Minimum bytes one launch of each kernel must move (each array touched once)."""
+    N = w.ntx * w.ntz
+    Ni = w.nx * w.nz
+    nzc = lambda a: int(np.count_nonzero(a))
+    x_v = nzc(cp["a_x_half"]) * w.ntz + nzc(cp["a_z_half"]) * w.ntx     # CPML cells of the v update
+    x_p = nzc(cp["a_x"]) * w.ntz + nzc(cp["a_z"]) * w.ntx               # CPML cells of the p update
+    if kernel == "fwd_v":      # p, vx r/w, vz r/w, rho; phi_p_x / phi_p_z r/w in the frame
+        return 24 * N + 8 * x_v
+    if kernel == "fwd_p":      # vx, vz, p r/w, vp, rho; phi_v r/w in the frame; strip save; traces
+        return 24 * N + 8 * x_p + 4 * strip_len + 4 * r_n
+    if kernel == "bwd_1":      # receiver p, v r/w, rho (all cells); source v, p r/w, vp, dp/dt (interior); strips
+        return 24 * N + 24 * Ni + 8 * x_v + 4 * strip_len
+    if kernel == "bwd_2":      # receiver v, p r/w, vp, rho; source p, v r/w, dp/dt, FP64 I,S r/w (interior)
+        return 24 * N + 56 * Ni + 8 * x_p + 4 * r_n
+    raise KeyError(kernel)
+
+
+def setup(swd, w, device):
+    import torch
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt, device=device)
+    pmlc = w.pmlc
+    vp_true = swd.pad_model(w.vp, pmlc)
+    vmig = swd.pad_model(w.vp_mig, pmlc)
+    rho = np.full_like(vmig, 1000.0)
+    E.setup_default(vmig, rho)
+    rick = swd.ricker_wave(w.nt, w.f0, w.dt)
+    rx, rz = w.receivers_padded()
+    sx, sz = w.source_padded()
+    shot = swd.ShotSpec(sx, sz, rx, rz, w.nt)
+    # PSF data: +1 % velocity scatter points on the migration model, minus the background
+    vs = vmig.copy()
+    for ix in w.scatter_x:
+        for iz in w.scatter_z:
+            vs[ix + pmlc, iz + pmlc] *= np.float32(1.01)
+    E.set_model(vs, rho)
+    d1 = E.forward(shot, rick)
+    E.set_model(vmig, rho)
+    d0 = E.forward(shot, rick)
+    data = (d1 - d0).astype(np.float32)
+    return E, shot, rick, data, swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    swd = load_pkg()
+    from swd_b200 import configs
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    w = configs.c2()
+    E, shot, rick, data, cp = setup(swd, w, dev)
+    stream = torch.cuda.current_stream()
+    E.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    r_n, nt = data.shape
+    # device-resident inputs / outputs for `value`
+    d_data = torch.from_numpy(data).cuda()
+    d_rick = torch.from_numpy(rick).cuda()
+    d_img = torch.empty((w.nx, w.nz), dtype=torch.float32, device="cuda")
+    d_fim = torch.empty((w.nx, w.nz), dtype=torch.float32, device="cuda")
+    # pinned host buffers for `e2e`
+    h_data = torch.from_numpy(data).pin_memory()
+    h_rick = torch.from_numpy(rick).pin_memory()
+    h_img = torch.empty((w.nx, w.nz), dtype=torch.float32).pin_memory()
+    h_fim = torch.empty((w.nx, w.nz), dtype=torch.float32).pin_memory()
+
+    import ctypes as C
+    sh, keep = E._shot(shot)
+
+    def step(dd, rk, img, fim):
+        rc = swd.lib().swd_rtm_shot(E._h, C.byref(sh), swd._ptr(rk), swd._ptr(dd), swd.RTM_PREPROCESS, None,
+                                    swd._ptr(img), None, swd._ptr(fim))
+        E._ck(rc)
+
+    def timed(dd, rk, img, fim, K, W, profile=False):
+        for _ in range(W):
+            step(dd, rk, img, fim)
+        if profile:
+            E.profile(8)
+            E.profile_read()
+        n0 = E.launch_count()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        total = 0.0
+        for _ in range(K):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(dd, rk, img, fim)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        launches = E.launch_count() - n0
+        prof = E.profile_read() if profile else None
+        E.profile(0)
+        return total, launches, prof
+
+    with ClockSampler(dev) as clk:
+        t_val, launches, prof = timed(d_data, d_rick, d_img, d_fim, args.steps, args.warmup, profile=True)
+        t_e2e, _, _ = timed(h_data, h_rick, h_img, h_fim, args.steps, max(1, args.warmup // 3))
+    if dist:
+        import torch.distributed as td
+        t = torch.tensor([t_val, t_e2e], dtype=torch.float64, device="cuda")
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        t_val, t_e2e = float(t[0]), float(t[1])
+    if rank != 0:
+        return None
+    shots = args.steps * world
+    value = shots / (t_val / 1e3)
+    e2e = shots / (t_e2e / 1e3)
+    N, Ni = w.ntx * w.ntz, w.nx * w.nz
+    cells_per_shot = nt * (N + Ni + N)
+    slen = 2 * w.Lc * w.nx + 2 * w.Lc * (w.nz - 2 * w.Lc)
+    # roofline of the dominant kernel (largest total time per step)
+    per_launch = {k: ms / n for k, (ms, n) in prof.items() if n}
+    launches_per_shot = {"fwd_v": nt, "fwd_p": nt, "bwd_1": nt - 1, "bwd_2": nt - 1}
+    dom = max(per_launch, key=lambda k: per_launch[k] * launches_per_shot[k])
+    peak, src = peaks()
+    ab = algorithmic_bytes(dom, w, cp, slen, r_n)
+    achieved = ab / (per_launch[dom] * 1e-3) / 1e9
+    traffic = None
+    tj = ROOT / "profiles" / "traffic.json"
+    if tj.exists():
+        t = json.loads(tj.read_text()).get(dom)
+        if t and "bytes_per_cell" in t:
+            traffic = t["bytes_per_cell"] * N
+    cpu = cpu_baseline(w, samples=1, nsteps=args.cpu_steps)
+    return {
+        "metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (FP64 imaging)", "data": "synthetic (seeded random-field model, PSF data)",
+        "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed step",
+                   "strips": "f32"},
+        "gcell_updates_per_s": value * cells_per_shot / 1e9,
+        "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(data.nbytes + rick.nbytes),
+                "d2h_bytes_per_step": int(2 * w.nx * w.nz * 4)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": src,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": ab, "avg_launch_us": per_launch[dom] * 1e3,
+                     "kernels_us": {k: v * 1e3 for k, v in per_launch.items()}},
+        "gpu_launches": launches,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+
+
+def cpu_baseline(w, samples=1, nsteps=24):
+    """OpenMP FP32 restatement of the reference loops (oracle/) on the host cores, for a
+    bounded number of time steps of the same shot, extrapolated to nt."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as orc
+    swd = sys.modules.get("swd_b200") or load_pkg()
+    pmlc = w.pmlc
+    vp = swd.pad_model(w.vp_mig, pmlc)
+    rho = np.full_like(vp, 1000.0)
+    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
+    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt)
+    rx, rz = w.receivers_padded()
+    sx, sz = w.source_padded()
+    G = orc.Geom(sx, sz, rx, rz)
+    rick = swd.ricker_wave(nsteps, w.f0, w.dt)
+    data = np.random.default_rng(0).standard_normal((len(rx), nsteps)).astype(np.float32)
+    best = None
+    for _ in range(samples):
+        t = time.perf_counter()
+        orc.rtm_shot(M, G, rick, data)
+        dt = time.perf_counter() - t
+        best = dt if best is None else min(best, dt)
+    per_shot = best * w.nt / nsteps
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": 1.0 / per_shot, "unit": "shots/s", "cores": cores, "kind": "port",
+            "sample": f"{nsteps} of {w.nt} time steps (forward + backward) of the same shot on the full grid, "
+                      f"extrapolated linearly; {best:.2f} s measured"}
+
+
+def run_reference(args):
+    from swd_b200 import configs  # noqa: F401  (package already loaded by caller)
+    w = sys.modules["swd_b200"].configs.c2()
+    t0 = time.perf_counter()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(w, samples=1, nsteps=args.cpu_steps)
+        if i >= args.warmup:
+            vals.append(1.0 / cb["value"])
+    mean = float(np.mean(vals))
+    value = 1.0 / mean
+    cb["value"] = value
+    return {"metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "parallelism": "host OpenMP"},
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-steps", type=int, default=300, help="time steps per CPU-baseline sample")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    load_pkg()
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = td
+    out = run_ours(args, rank, world, dist)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

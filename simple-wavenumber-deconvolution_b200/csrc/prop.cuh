@@ -229,8 +229,13 @@ __global__ void __launch_bounds__(256) k_fwd_p(FwdArgs a)
                     if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = to_store<__half>(pn[0] * sc);
                     else ((__nv_bfloat16 *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = to_store<__nv_bfloat16>(pn[0] * sc);
                 }
-            } else if (threadIdx.x == 0 && threadIdx.y == 0) {
-                a.strips.scale[(size_t)a.it * a.strips.nscale + slot] = 0.f;
+            } else {
+                // an all-zero block: store zeros so the restore never reads stale halves
+                if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)a.it * a.strips.nscale + slot] = 0.f;
+                if (si >= 0) {
+                    if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = __float2half_rn(0.f);
+                    else ((__nv_bfloat16 *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = __float2bfloat16_rn(0.f);
+                }
             }
         }
     }
@@ -298,8 +303,9 @@ __global__ void __launch_bounds__(256) k_bwd_1(BwdArgs a)
                 const int slot = (x / 8) * ((g.ntz + 31) / 32) + (z / 32);
                 const float mx = a.strips.scale[(size_t)a.it * a.strips.nscale + slot];
                 const float inv = mx / (a.strips.prec == 1 ? 32768.f : 1.f);
-                p = a.strips.prec == 1 ? strip_load<__half>(a.strips, a.it, si, inv)
-                                       : strip_load<__nv_bfloat16>(a.strips, a.it, si, inv);
+                p = mx == 0.f ? 0.f
+                              : (a.strips.prec == 1 ? strip_load<__half>(a.strips, a.it, si, inv)
+                                                    : strip_load<__nv_bfloat16>(a.strips, a.it, si, inv));
             }
         }
         a.s.p[ip] = p;
