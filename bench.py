@@ -287,6 +287,30 @@ def cpu_baseline(w, samples=1, nsteps=24):
                       f"extrapolated linearly; {best:.2f} s measured"}
 
 
+def run_profile_kernels(args):
+    """One RTM shot on the benchmark grid with a short record (--nt) and seeded random data,
+    no warm-up shots and no data generation: the command the ncu captures run, so that few
+    launches precede the captured ones.  Prints per-kernel event timings."""
+    import ctypes as C
+    swd = load_pkg()
+    from swd_b200 import configs
+    w = configs.c2()
+    w.nt = args.nt
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt)
+    vmig = swd.pad_model(w.vp_mig, w.pmlc)
+    E.setup_default(vmig, np.full_like(vmig, 1000.0))
+    rick = swd.ricker_wave(w.nt, w.f0, w.dt)
+    rx, rz = w.receivers_padded()
+    sx, sz = w.source_padded()
+    shot = swd.ShotSpec(sx, sz, rx, rz, w.nt)
+    data = np.random.default_rng(0).standard_normal((len(rx), w.nt)).astype(np.float32) * 1e-6
+    E.profile(1)
+    E.rtm_shot(shot, rick, data, want=())
+    prof = E.profile_read()
+    print(json.dumps({"mode": "profile-kernels", "grid": [w.ntx, w.ntz], "nt": w.nt, "launches": E.launch_count(),
+                      "kernels_us": {k: ms / n * 1e3 for k, (ms, n) in prof.items() if n}}))
+
+
 def run_reference(args):
     from swd_b200 import configs  # noqa: F401  (package already loaded by caller)
     w = sys.modules["swd_b200"].configs.c2()
@@ -314,10 +338,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=300, help="time steps per CPU-baseline sample")
+    ap.add_argument("--profile-kernels", action="store_true", help="one short shot for ncu captures")
+    ap.add_argument("--nt", type=int, default=30, help="record length of --profile-kernels")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     load_pkg()
+    if args.profile_kernels:
+        run_profile_kernels(args)
+        return
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)

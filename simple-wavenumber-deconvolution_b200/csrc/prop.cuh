@@ -223,11 +223,13 @@ __global__ void __launch_bounds__(256) k_fwd_p(FwdArgs a)
             const float mx = smax;
             const int slot = blockIdx.y * gridDim.x + blockIdx.x;
             if (mx > 0.f) {
-                const float sc = (a.strips.prec == 1 ? 32768.f : 1.f) / mx;
+                // normalise first (|p|/mx <= 1 even when mx is denormal), then scale into the
+                // half range; the restore undoes it in the same order
                 if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)a.it * a.strips.nscale + slot] = mx;
                 if (si >= 0) {
-                    if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = to_store<__half>(pn[0] * sc);
-                    else ((__nv_bfloat16 *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = to_store<__nv_bfloat16>(pn[0] * sc);
+                    const float q = pn[0] / mx;
+                    if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = to_store<__half>(q * 32768.f);
+                    else ((__nv_bfloat16 *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = to_store<__nv_bfloat16>(q);
                 }
             } else {
                 // an all-zero block: store zeros so the restore never reads stale halves
@@ -262,10 +264,12 @@ struct BwdArgs {
     double *I, *S, *R;   // FP64 imaging accumulators (R nullable)
 };
 
+// restore: value = (stored / unit) * mx, unit = 32768 for half, 1 for bf16
 template <typename S>
-__device__ __forceinline__ float strip_load(const Strips &st, int it, int si, float scale)
+__device__ __forceinline__ float strip_load(const Strips &st, int it, int si, float mx)
 {
-    return (float)((const S *)st.buf)[(size_t)it * st.slen + si] * scale;
+    const float unit = sizeof(S) == 2 && st.prec == 1 ? 32768.f : 1.f;
+    return ((float)((const S *)st.buf)[(size_t)it * st.slen + si] / unit) * mx;
 }
 template <>
 __device__ __forceinline__ float strip_load<float>(const Strips &st, int it, int si, float)
@@ -302,10 +306,9 @@ __global__ void __launch_bounds__(256) k_bwd_1(BwdArgs a)
                 // the forward kernel's scale slot for this cell: same block tiling
                 const int slot = (x / 8) * ((g.ntz + 31) / 32) + (z / 32);
                 const float mx = a.strips.scale[(size_t)a.it * a.strips.nscale + slot];
-                const float inv = mx / (a.strips.prec == 1 ? 32768.f : 1.f);
                 p = mx == 0.f ? 0.f
-                              : (a.strips.prec == 1 ? strip_load<__half>(a.strips, a.it, si, inv)
-                                                    : strip_load<__nv_bfloat16>(a.strips, a.it, si, inv));
+                              : (a.strips.prec == 1 ? strip_load<__half>(a.strips, a.it, si, mx)
+                                                    : strip_load<__nv_bfloat16>(a.strips, a.it, si, mx));
             }
         }
         a.s.p[ip] = p;

@@ -161,7 +161,7 @@ def test_rtm_receiver_illumination_and_stack_of_two(case, swd, orc):
     assert rel_l2(st, f1.astype(np.float64) + f2) < 1e-6
 
 
-@pytest.mark.parametrize("prec,tol", [(1, 2e-3), (2, 1e-2)])
+@pytest.mark.parametrize("prec,tol", [(1, 5e-3), (2, 5e-2)])
 def test_compressed_strips(case, swd, orc, prec, tol):
     data = orc.forward(case.M, case.G, case.rick)["seis"]
     case.E.set_strip_precision(0)
