@@ -159,6 +159,28 @@ int swd_profile(swd_ctx *ctx, int every);
 int swd_profile_read(swd_ctx *ctx, double *ms, long long *launches);
 long long swd_launch_count(const swd_ctx *ctx);
 
+/* ---- deconvolution without allocation ------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory while
+ * they run: plug-in hosts that own the whole device memory pool and hand their plug-ins only
+ * the buffers they pass in, and latency-bound services that reserve memory up front because
+ * cudaFree synchronises the whole device and would stall their other streams.
+ * Same algorithm and kernels as swd_decon, but all scratch (the per-window result slots and
+ * the output taper) lives in one static device array of SWD_DECON_STATIC_SCRATCH_FLOATS
+ * floats (16 MiB) that every GPU which loads libswd holds until the process exits.  The call
+ * allocates nothing: migreal/migpsf (nx*nz) and mig_dec/mig_coef (nx*nz) must be device
+ * memory on the current device, already allocated by the caller.  Work is enqueued on
+ * `cuda_stream` (NULL = the default stream); results are ready when that stream reaches it.
+ * Returns SWD_ERR_CAPACITY when windows*outwinx*outwinz + outwinx*outwinz exceeds the array,
+ * SWD_ERR_ARG for invalid geometry or non-device pointers.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Every call reuses the same array and leaves its contents behind; each
+ * call writes every scratch word it reads, so nothing needs clearing, but calls that overlap
+ * on the GPU (other streams or host threads) race on the shared array. */
+#define SWD_ERR_CAPACITY 6
+#define SWD_DECON_STATIC_SCRATCH_FLOATS (4u << 20)
+int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const float *migpsf,
+                      float *mig_dec, float *mig_coef, void *cuda_stream);
+
 /* ---- host preparation (the reference's host functions, restated) ------------------- */
 /* cal_xishu, acoustic_HLVSPRTMC.cpp:1858-1878 */
 void swd_prep_xishu(int Lc, float *rc);

@@ -653,6 +653,32 @@ static int decon_geo(const swd_decon_params *p, DeconGeo &g)
 }
 
 // ------------------------------------------------------------------------------------
+// Static scratch of swd_decon_noalloc: the per-window result slots and the output taper of
+// one deconvolution, so that entry point never allocates.  Every device that loads this
+// library holds the 16 MiB array until the process exits; all calls share it.
+// ------------------------------------------------------------------------------------
+static __device__ __align__(256) float g_decon_scratch[SWD_DECON_STATIC_SCRATCH_FLOATS];
+
+// Hann-edged output taper on the device (same expression as the host taper of swd_decon,
+// kk_decon_interp_psf_minewindow.cpp:355-383), written into the static scratch.
+__global__ void k_decon_taper(float *coefr, int outwinx, int outwinz, int snapwinx, int snapwinz)
+{
+    const double PI = 3.1415926;
+    const int n = outwinx * outwinz;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int ix = j / outwinz, iz = j % outwinz;
+        float cx, cz;
+        if (ix <= snapwinx - 1) cx = 0.5000 - 0.5 * cos(PI * ix / (snapwinx - 1));
+        else if (ix >= outwinx - snapwinx) cx = 0.5000 + 0.5 * cos(PI * (ix - outwinx + snapwinx) / (snapwinx - 1));
+        else cx = 1.0;
+        if (iz <= snapwinz - 1) cz = 0.5000 - 0.5 * cos(PI * iz / (snapwinz - 1));
+        else if (iz >= outwinz - snapwinz) cz = 0.5000 + 0.5 * cos(PI * (iz - outwinz + snapwinz) / (snapwinz - 1));
+        else cz = 1.0;
+        coefr[j] = cx * cz;
+    }
+}
+
+// ------------------------------------------------------------------------------------
 // C ABI
 // ------------------------------------------------------------------------------------
 extern "C" {
@@ -1169,6 +1195,40 @@ int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, 
     } while (0);
     if (!ctx_in) cudaStreamDestroy(tmp.stream);
     return rc;
+}
+
+int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const float *migpsf, float *mig_dec,
+                      float *mig_coef, void *cuda_stream)
+{
+    // device address of the static scratch, looked up once per device with that device
+    // current; the lookup allocates nothing
+    static float *scratch_addr[64] = {nullptr};
+    DeconGeo g;
+    if (!p || decon_geo(p, g) != SWD_OK) return SWD_ERR_ARG;
+    const size_t nout = (size_t)g.outwinx * g.outwinz;
+    if ((size_t)g.totalnum * nout + nout > SWD_DECON_STATIC_SCRATCH_FLOATS) return SWD_ERR_CAPACITY;
+    const void *ptrs[4] = {migreal, migpsf, mig_dec, mig_coef};
+    for (const void *q : ptrs)
+        if (!is_device_ptr(q)) return SWD_ERR_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWD_ERR_CUDA;
+    if (!scratch_addr[dev]) {
+        void *a = nullptr;
+        if (cudaGetSymbolAddress(&a, g_decon_scratch) != cudaSuccess || !a) {
+            cudaGetLastError();
+            return SWD_ERR_CUDA;
+        }
+        scratch_addr[dev] = (float *)a;
+    }
+    float *coefr = scratch_addr[dev], *winout = coefr + nout;
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + g.n0 + g.n1);
+    if (cudaFuncSetAttribute(k_decon_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+        return SWD_ERR_CUDA;
+    k_decon_taper<<<(int)((nout + 255) / 256), 256, 0, st>>>(coefr, g.outwinx, g.outwinz, p->snapwinx, p->snapwinz);
+    k_decon_window<<<g.totalnum, 512, sm, st>>>(g, migreal, migpsf, coefr, winout);
+    k_decon_gather<<<592, 256, 0, st>>>(g, winout, coefr, mig_dec, mig_coef);
+    return cudaGetLastError() == cudaSuccess ? SWD_OK : SWD_ERR_CUDA;
 }
 
 }  // extern "C"
