@@ -1,0 +1,114 @@
+"""The drop-in programs AFor, AVSPRTM and decon2d_mine run in a project tree laid out like the
+reference's (parameter.txt, input/, output/, forward/, kkdecon_acoustic/) and must write the
+reference's files with the reference's results.  GPU tests compare against the outputs of
+the reference's own programs (tests/golden/*.npz); CPU tests cover the error paths, which
+return before any device work."""
+import importlib.util
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, PKG_DIR, rel_l2
+
+TOL = 1e-4
+
+
+def _mkg(name):
+    spec = importlib.util.spec_from_file_location(name, GOLDEN / f"{name}.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _tree(d):
+    for sub in ("input", "output", "forward"):
+        (d / sub).mkdir(exist_ok=True)
+    return d
+
+
+def test_missing_parameter_file_is_an_error():
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        r = subprocess.run([str(PKG_DIR / "AVSPRTM")], cwd=d, capture_output=True, text=True)
+        assert r.returncode != 0 and "Cannot open the parameters" in r.stdout
+        r = subprocess.run([str(PKG_DIR / "AFor")], cwd=d / "forward", capture_output=True, text=True)
+        assert r.returncode != 0
+
+
+def test_truncated_parameter_file_is_an_error():
+    mk = _mkg("make_golden_ref_gpu")
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        mk.write_params(d / "parameter.txt", mk.CASE, 0)
+        lines = (d / "parameter.txt").read_text().splitlines()[:20]
+        (d / "parameter.txt").write_text("\n".join(lines) + "\n")
+        r = subprocess.run([str(PKG_DIR / "AVSPRTM")], cwd=d, capture_output=True, text=True)
+        assert r.returncode != 0
+
+
+def test_decon_rejects_even_windows():
+    mk = _mkg("make_golden")
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        (d / "output").mkdir()
+        mk.write_decon_params(d / "parameter.txt", 100, 90, (10, 11), (21, 21), (5, 5), 1e-3)
+        r = subprocess.run([str(PKG_DIR / "decon2d_mine")], cwd=d, capture_output=True, text=True)
+        assert "Should Be Odd" in r.stdout
+
+
+@pytest.mark.gpu
+def test_afor_and_avsprtm_reproduce_the_reference_programs():
+    g = np.load(GOLDEN / "ref_gpu_small.npz")
+    mk = _mkg("make_golden_ref_gpu")
+    nx, nz, pml, Lc, nt, swin, window = [int(v) for v in g["case"]]
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        g["acc_vp"].tofile(d / "input" / "acc_vp.bin")
+        rd = lambda name, shape: np.fromfile(d / "output" / name, np.float32).reshape(shape)
+        for flag in (0, 1):
+            mk.write_params(d / "parameter.txt", mk.CASE, flag)
+            subprocess.run([str(PKG_DIR / "AFor")], cwd=d / "forward", check=True, capture_output=True)
+            subprocess.run([str(PKG_DIR / "AVSPRTM")], cwd=d, check=True, capture_output=True)
+        r_n = g["obs"].shape[0]
+        assert rel_l2(rd("1source_seismogram_obs.bin", (r_n, nt)), g["obs"]) < TOL
+        assert rel_l2(rd("1source_seismogram_obsup.bin", (r_n, nt)), g["obsup"]) < TOL
+        assert rel_l2(rd("1source_seismogram_obsdown.bin", (r_n, nt)), g["obsdown"]) < TOL
+        assert rel_l2(rd("rick_hilbert.bin", (nt,)), g["rick_hilbert"]) < 1e-5
+        assert np.array_equal(rd("ini_vp.bin", (nx, nz)), g["ini_vp"])
+        assert np.array_equal(rd("rho_scatter.bin", (nx, nz)), g["rho_scatter"])
+        assert rel_l2(rd("image_pp1.bin", (nx, nz)), g["image_pp"]) < TOL
+        assert rel_l2(rd("fimage_pp1.bin", (nx, nz)), g["fimage_pp"]) < TOL
+        assert rel_l2(rd("migration_pp.bin", (nx, nz)), g["migration_pp"]) < TOL
+        # PSF data are differences of two records; compare them on their own scale
+        assert rel_l2(rd("1source_seismogram_scatterup.bin", (r_n, nt)), g["scatterup"]) < 1e-2
+        assert rel_l2(rd("image_psf1.bin", (nx, nz)), g["image_psf"]) < 1e-2
+        assert rel_l2(rd("migration_psf.bin", (nx, nz)), g["migration_psf"]) < 1e-2
+
+
+@pytest.mark.gpu
+def test_decon2d_mine_reproduces_the_reference_program():
+    mk = _mkg("make_golden")
+    g = np.load(GOLDEN / "decon_ref.npz")
+    for k, (nx, nz, psf, flt, snap, eps, seed) in enumerate(mk.DECON_CASES):
+        _, _, vp = mk.synthetic_decon_inputs(nx, nz, psf, seed)
+        with tempfile.TemporaryDirectory() as d:
+            d = Path(d)
+            (d / "input").mkdir()
+            (d / "output").mkdir()
+            mk.write_decon_params(d / "parameter.txt", nx, nz, psf, flt, snap, eps)
+            vp.tofile(d / "input" / "acc_vp.bin")
+            vp.tofile(d / "input" / "ini_vp.bin")
+            g[f"mig{k}"].tofile(d / "input" / "mig.bin")
+            g[f"psf{k}"].tofile(d / "input" / "psf.bin")
+            subprocess.run([str(PKG_DIR / "decon2d_mine")], cwd=d, check=True, capture_output=True)
+            dec = np.fromfile(d / "output" / "dec.bin", np.float32).reshape(nx, nz)
+            coef = np.fromfile(d / "output" / "migration_coef.bin", np.float32).reshape(nx, nz)
+            assert (d / "output" / "start.flag").exists() and (d / "output" / "end.flag").exists()
+            txt = (d / "output" / "migration_coef.txt").read_bytes().split(b"\r\t\n")
+            assert len(txt) == nz + 1
+        assert np.array_equal(coef, g[f"coef{k}"])
+        assert rel_l2(dec, g[f"dec{k}"]) < 1e-3
