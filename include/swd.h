@@ -15,7 +15,9 @@
  *    complete when the call returns.
  *  - Every call returns an int status (SWD_OK = 0); swd_last_error() describes the last
  *    failure on a context.  A context is used by one host thread at a time and owns one
- *    CUDA stream (swd_set_stream() may substitute the caller's).
+ *    CUDA stream (swd_set_stream() may substitute the caller's).  Time loops run as
+ *    replayed CUDA graphs of 64 steps; on the legacy default stream (handle 0), which cannot
+ *    be captured, they are launched step by step instead.
  *  - Seismograms are trace-major [r_n][nt]; images nx*nz unless stated otherwise.
  */
 #ifndef SWD_H
@@ -86,6 +88,13 @@ int swd_set_cpml(swd_ctx *ctx, const float *a_x, const float *a_x_half,
                  const float *b_z, const float *b_z_half);
 int swd_set_model(swd_ctx *ctx, const float *vp, const float *rho);   /* padded ntx*ntz */
 int swd_set_strip_precision(swd_ctx *ctx, int strip_precision);       /* SWD_STRIP_* */
+/* kernel path: SWD_PATH_PLAIN (default) runs four cells of a column per thread with 128-bit
+ * loads and two launches per time step (the velocity and pressure halves, like the
+ * reference's vx/vz/p kernels); SWD_PATH_FUSED (Lc <= 6) runs one launch per time step on
+ * shared-memory tiles with the velocity halo recomputed. */
+#define SWD_PATH_PLAIN 0
+#define SWD_PATH_FUSED 1
+int swd_set_kernel_path(swd_ctx *ctx, int path);
 
 /* ---- forward modelling --------------------------------------------------------------
  * Replaces fdtd_2d_GPU_forward of AFor (forward/headrtm.h:159-171,
@@ -151,10 +160,12 @@ int swd_decon(swd_ctx *ctx, const swd_decon_params *p, const float *migreal,
 /* ---- instrumentation (no reference counterpart; the reference only prints clock()) ---
  * swd_profile(ctx, every): bracket each kernel launch of every `every`-th time step with
  * CUDA events on the context stream (0 disables).  swd_profile_read fills, per kernel id
- * (0 forward-v, 1 forward-p, 2 backward-1, 3 backward-2), the summed milliseconds and the
+ * (0 forward-v, 1 forward-p, 2 backward-1, 3 backward-2 of the plain path; 4 forward step,
+ * 5 backward step of the fused path; 6 / 7 whole forward / backward time steps, i.e. a pass
+ * divided by its steps), the summed milliseconds and the
  * number of timed launches, and clears them.  swd_launch_count is the number of kernels the
  * context has launched since it was created. */
-#define SWD_NKERNELS 4
+#define SWD_NKERNELS 8
 int swd_profile(swd_ctx *ctx, int every);
 int swd_profile_read(swd_ctx *ctx, double *ms, long long *launches);
 long long swd_launch_count(const swd_ctx *ctx);

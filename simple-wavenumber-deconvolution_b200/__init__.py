@@ -26,6 +26,7 @@ LIB_PATH = PKG_DIR / "libswd.so"
 
 SWD_OK, SWD_ERR_ARG, SWD_ERR_CUDA, SWD_ERR_ALLOC, SWD_ERR_STATE, SWD_ERR_DEVICE = range(6)
 STRIP_F32, STRIP_F16, STRIP_BF16 = 0, 1, 2
+PATH_PLAIN, PATH_FUSED = 0, 1
 RTM_PREPROCESS, RTM_ILLUM_RCV, RTM_NO_STACK = 1, 2, 4
 
 
@@ -82,6 +83,7 @@ def lib():
         L.swd_set_cpml.argtypes = [vp] + [vp] * 8
         L.swd_set_model.argtypes = [vp, vp, vp]
         L.swd_set_strip_precision.argtypes = [vp, C.c_int]
+        L.swd_set_kernel_path.argtypes = [vp, C.c_int]
         L.swd_forward.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, vp, vp]
         L.swd_rtm_shot.argtypes = [vp, C.POINTER(Shot), vp, vp, C.c_uint, vp, vp, vp, vp]
         L.swd_rtm_raw.argtypes = [vp, vp, vp, vp]
@@ -239,6 +241,10 @@ class Engine:
     def set_strip_precision(self, prec: int):
         self._ck(lib().swd_set_strip_precision(self._h, prec))
 
+    def set_kernel_path(self, path: int):
+        """PATH_PLAIN: one cell per thread, two launches per step; PATH_FUSED: one launch per step."""
+        self._ck(lib().swd_set_kernel_path(self._h, path))
+
     def set_stream(self, stream_handle: int):
         self._ck(lib().swd_set_stream(self._h, C.c_void_p(stream_handle)))
 
@@ -254,10 +260,11 @@ class Engine:
 
     def profile_read(self):
         """{kernel: (summed ms, timed launches)} for forward-v, forward-p, backward-1, backward-2."""
-        ms = np.zeros(4, np.float64)
-        n = np.zeros(4, np.int64)
+        ms = np.zeros(8, np.float64)
+        n = np.zeros(8, np.int64)
         self._ck(lib().swd_profile_read(self._h, _ptr(ms), _ptr(n)))
-        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(["fwd_v", "fwd_p", "bwd_1", "bwd_2"])}
+        names = ["fwd_v", "fwd_p", "bwd_1", "bwd_2", "fwd_step", "bwd_step", "fwd_pass_step", "bwd_pass_step"]
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(names)}
 
     def launch_count(self) -> int:
         return int(lib().swd_launch_count(self._h))

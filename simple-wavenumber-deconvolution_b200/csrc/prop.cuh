@@ -69,90 +69,209 @@ __device__ __forceinline__ int strip_index(int x, int z, int ntx, int ntz, int p
 }
 
 // ------------------------------------------------------------------------------------
-// velocity half step:  vx, vz from p (reference kernels _vx/_vz, :24-118; receiver
-// variants with the wider guards and -dx/-dz, :623-715).  WIDE selects the receiver
-// back-propagation guards.
+// Plain path: two launches per time step, fields updated in place.  Each thread owns four
+// consecutive cells of one column (z0 .. z0+3, z0 a multiple of 4) and moves them with
+// 128-bit loads: an x-direction tap is one float4 of the neighbouring column, the
+// z-direction taps come from the float4 chunks just above and below, already in
+// registers.  Every field array carries a guard band (GUARD floats on both sides) so the
+// chunks next to the grid edge are readable; their values only feed cells that fail the
+// update guards.  Per-cell arithmetic is that of the reference kernels, element by element.
 // ------------------------------------------------------------------------------------
+constexpr int GUARD = 64;
+
+__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ float &el(float4 &v, int k) { return (&v.x)[k]; }
+__device__ __forceinline__ float elc(const float4 &v, int k) { return (&v.x)[k]; }
+
+// z-window of a column around z0: w[NB*4 + k] holds z0 + k for k in [-NB*4, 4 + NB*4)
+template <int LC>
+struct ZWin {
+    static constexpr int NB = (LC + 3) / 4;
+    float v[4 * (2 * NB + 1)];
+    __device__ __forceinline__ void load(const float *col, int z0)
+    {
+#pragma unroll
+        for (int b = -NB; b <= NB; b++) {
+            const float4 q = ld4(col + z0 + 4 * b);
+            v[4 * (b + NB) + 0] = q.x; v[4 * (b + NB) + 1] = q.y;
+            v[4 * (b + NB) + 2] = q.z; v[4 * (b + NB) + 3] = q.w;
+        }
+    }
+    __device__ __forceinline__ float at(int k) const { return v[4 * NB + k]; }   // z0 + k
+};
+
+// velocity half step (reference kernels _vx/_vz, acoustic_HLVSPRTMLc.cu:24-118; receiver
+// variants with the wider guards and -dx/-dz, :623-715)
 template <int LC, bool WIDE>
-__device__ __forceinline__ void v_update(const Geo &g, const Cpml &c, const float *__restrict__ rho,
-                                         Wave w, float odx, float odz, int x, int z)
+__device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const float *__restrict__ rho, Wave w,
+                                          float odx, float odz, int x, int z0)
 {
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
-    const size_t ip = cidx(x, z, ldz);
-    const bool gx = WIDE ? (z >= 0 && z <= ntz - 1 && x >= LC - 1 && x <= ntx - LC - 1)
-                         : (z >= LC && z <= ntz - LC && x >= LC - 1 && x <= ntx - LC - 1);
-    if (gx) {
-        float d = 0.f;
+    const size_t ip = (size_t)x * ldz + z0;
+    // ---- vx: x taps from the neighbouring columns
+    const bool colx = x >= LC - 1 && x <= ntx - LC - 1;
+    if (colx) {
+        bool gx[4];
+        bool any = false;
 #pragma unroll
-        for (int ic = 0; ic < LC; ic++) d += g.rc[ic] * (w.p[ip + (ic + 1) * ldz] - w.p[ip - ic * ldz]) * odx;
-        const float a = __ldg(c.axh + x);
-        float phi = 0.f;
-        if (a != 0.f) {
-            phi = __ldg(c.bxh + x) * w.ppx[ip] + a * d;
-            w.ppx[ip] = phi;
+        for (int k = 0; k < 4; k++) {
+            const int z = z0 + k;
+            gx[k] = WIDE ? (z <= ntz - 1) : (z >= LC && z <= ntz - LC);
+            any |= gx[k];
         }
-        const float orho = __frcp_rn(0.5f * (__ldg(rho + ip) + __ldg(rho + ip + ldz)));
-        w.vx[ip] = g.dt * orho * (d + phi) + w.vx[ip];
+        if (any) {
+            float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int ic = 0; ic < LC; ic++) {
+                const float4 a = ld4(w.p + ip + (size_t)(ic + 1) * ldz), b = ld4(w.p + ip - (size_t)ic * ldz);
+#pragma unroll
+                for (int k = 0; k < 4; k++) el(d, k) += g.rc[ic] * (elc(a, k) - elc(b, k)) * odx;
+            }
+            const float ax = __ldg(c.axh + x);
+            float4 phi = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ax != 0.f) {
+                const float bx = __ldg(c.bxh + x);
+                float4 po = ld4(w.ppx + ip);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    el(phi, k) = bx * elc(po, k) + ax * elc(d, k);
+                    if (gx[k]) el(po, k) = elc(phi, k);
+                }
+                st4(w.ppx + ip, po);
+            }
+            const float4 r0 = ldg4(rho + ip), r1 = ldg4(rho + ip + ldz);
+            float4 v = ld4(w.vx + ip);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float orho = __frcp_rn(0.5f * (elc(r0, k) + elc(r1, k)));
+                if (gx[k]) el(v, k) = g.dt * orho * (elc(d, k) + elc(phi, k)) + elc(v, k);
+            }
+            st4(w.vx + ip, v);
+        }
     }
-    const bool gz = WIDE ? (z >= LC - 1 && z <= ntz - LC - 1 && x >= 0 && x <= ntx - 1)
-                         : (z >= LC - 1 && z <= ntz - LC - 1 && x >= LC && x <= ntx - LC);
-    if (gz) {
-        float d = 0.f;
+    // ---- vz: z taps from the column's own window
+    const bool colz = WIDE ? (x >= 0 && x <= ntx - 1) : (x >= LC && x <= ntx - LC);
+    if (colz) {
+        bool gz[4];
+        bool any = false;
 #pragma unroll
-        for (int ic = 0; ic < LC; ic++) d += g.rc[ic] * (w.p[ip + (ic + 1)] - w.p[ip - ic]) * odz;
-        const float a = __ldg(c.azh + z);
-        float phi = 0.f;
-        if (a != 0.f) {
-            phi = __ldg(c.bzh + z) * w.ppz[ip] + a * d;
-            w.ppz[ip] = phi;
+        for (int k = 0; k < 4; k++) {
+            const int z = z0 + k;
+            gz[k] = z >= LC - 1 && z <= ntz - LC - 1;
+            any |= gz[k];
         }
-        const float orho = __frcp_rn(0.5f * (__ldg(rho + ip) + __ldg(rho + ip + 1)));
-        w.vz[ip] = g.dt * orho * (d + phi) + w.vz[ip];
+        if (any) {
+            ZWin<LC> pw;
+            pw.load(w.p + (size_t)x * ldz, z0);
+            float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+#pragma unroll
+                for (int ic = 0; ic < LC; ic++) el(d, k) += g.rc[ic] * (pw.at(k + ic + 1) - pw.at(k - ic)) * odz;
+            float4 phi = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 az = ldg4(c.azh + z0);
+            if (az.x != 0.f || az.y != 0.f || az.z != 0.f || az.w != 0.f) {
+                const float4 bz = ldg4(c.bzh + z0);
+                float4 po = ld4(w.ppz + ip);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    el(phi, k) = elc(bz, k) * elc(po, k) + elc(az, k) * elc(d, k);
+                    if (gz[k] && elc(az, k) != 0.f) el(po, k) = elc(phi, k);
+                    else el(phi, k) = 0.f;
+                }
+                st4(w.ppz + ip, po);
+            }
+            const float4 r0 = ldg4(rho + ip);
+            const float r4 = __ldg(rho + ip + 4);
+            float4 v = ld4(w.vz + ip);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float rn = k < 3 ? elc(r0, k + 1) : r4;
+                const float orho = __frcp_rn(0.5f * (elc(r0, k) + rn));
+                if (gz[k]) el(v, k) = g.dt * orho * (elc(d, k) + elc(phi, k)) + elc(v, k);
+            }
+            st4(w.vz + ip, v);
+        }
     }
 }
 
-// pressure step with CPML (reference kernel _p, :121-173).  Returns true if p was updated.
+// pressure step with CPML (reference kernel _p, :121-173) on the four cells; returns the
+// new values in pn (old values where not updated) and the per-cell update flags.
 template <int LC>
-__device__ __forceinline__ bool p_update(const Geo &g, const Cpml &c, const float *__restrict__ vp,
-                                         const float *__restrict__ rho, Wave w, float odx, float odz,
-                                         int x, int z, float &pnew)
+__device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const float *__restrict__ vp,
+                                          const float *__restrict__ rho, Wave w, float odx, float odz, int x, int z0,
+                                          float4 &pn, bool upd[4])
 {
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
-    const size_t ip = cidx(x, z, ldz);
-    pnew = w.p[ip];
-    if (!(z >= LC && z <= ntz - LC && x >= LC && x <= ntx - LC)) return false;
-    float dvx = 0.f, dvz = 0.f;
+    const size_t ip = (size_t)x * ldz + z0;
+    pn = ld4(w.p + ip);
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int z = z0 + k;
+        upd[k] = z >= LC && z <= ntz - LC && x >= LC && x <= ntx - LC;
+        any |= upd[k];
+    }
+    if (!any) return;
+    float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
+    ZWin<LC> vw;
+    vw.load(w.vz + (size_t)x * ldz, z0);
 #pragma unroll
     for (int ic = 0; ic < LC; ic++) {
-        dvx += g.rc[ic] * (w.vx[ip + ic * ldz] - w.vx[ip - (ic + 1) * ldz]) * odx;
-        dvz += g.rc[ic] * (w.vz[ip + ic] - w.vz[ip - (ic + 1)]) * odz;
+        const float4 a = ld4(w.vx + ip + (size_t)ic * ldz), b = ld4(w.vx + ip - (size_t)(ic + 1) * ldz);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            el(dvx, k) += g.rc[ic] * (elc(a, k) - elc(b, k)) * odx;
+            el(dvz, k) += g.rc[ic] * (vw.at(k + ic) - vw.at(k - ic - 1)) * odz;
+        }
     }
-    float phx = 0.f, phz = 0.f;
+    float4 phx = make_float4(0.f, 0.f, 0.f, 0.f), phz = make_float4(0.f, 0.f, 0.f, 0.f);
     const float ax = __ldg(c.ax + x);
     if (ax != 0.f) {
-        phx = __ldg(c.bx + x) * w.pvx[ip] + ax * dvx;
-        w.pvx[ip] = phx;
+        const float bx = __ldg(c.bx + x);
+        float4 po = ld4(w.pvx + ip);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            el(phx, k) = bx * elc(po, k) + ax * elc(dvx, k);
+            if (upd[k]) el(po, k) = elc(phx, k);
+        }
+        st4(w.pvx + ip, po);
     }
-    const float az = __ldg(c.az + z);
-    if (az != 0.f) {
-        phz = __ldg(c.bz + z) * w.pvz[ip] + az * dvz;
-        w.pvz[ip] = phz;
+    const float4 az = ldg4(c.az + z0);
+    if (az.x != 0.f || az.y != 0.f || az.z != 0.f || az.w != 0.f) {
+        const float4 bz = ldg4(c.bz + z0);
+        float4 po = ld4(w.pvz + ip);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            el(phz, k) = elc(bz, k) * elc(po, k) + elc(az, k) * elc(dvz, k);
+            if (upd[k] && elc(az, k) != 0.f) el(po, k) = elc(phz, k);
+            else el(phz, k) = 0.f;
+        }
+        st4(w.pvz + ip, po);
     }
-    const float v = __ldg(vp + ip);
-    pnew = g.dt * __ldg(rho + ip) * v * v * (dvx + phx + dvz + phz) + pnew;
-    return true;
+    const float4 v = ldg4(vp + ip), r = ldg4(rho + ip);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (upd[k])
+            el(pn, k) = g.dt * elc(r, k) * elc(v, k) * elc(v, k) * (elc(dvx, k) + elc(phx, k) + elc(dvz, k) + elc(phz, k)) + elc(pn, k);
 }
 
 // ------------------------------------------------------------------------------------
-// Forward modelling, two launches per time step (all fields in place).
+// Forward modelling
 // ------------------------------------------------------------------------------------
 struct FwdArgs {
     Geo g;
     Cpml c;
     const float *vp, *rho;
     Wave w[2];           // w[1] is the Hilbert twin when NW == 2
-    float amp[2];        // wavelet samples added at the source after the p update
-    int sx, sz, it, nt;
+    // time index = *itp + itoff (a device counter, so one captured graph serves every
+    // chunk of steps); wavelet samples come from the device arrays wav0 / wav1
+    const int *itp;
+    int itoff;
+    const float *wav0, *wav1;
+    int sx, sz, nt;
     Wells wells;
     float *seis;         // [r_n][nt]
     Strips strips;       // save (forward pass of RTM), buf == nullptr to skip
@@ -160,84 +279,93 @@ struct FwdArgs {
     float2 *colbuf;      // [ncol][nt][ldz] (p, twin p)
 };
 
+// block (32, 8): lane -> four rows, warp -> one column; a block covers 128 rows x 8 columns
+__device__ __forceinline__ void cell4(int &x, int &z0)
+{
+    z0 = (blockIdx.x * 32 + threadIdx.x) * 4;
+    x = blockIdx.y * 8 + threadIdx.y;
+}
+
 template <int LC, int NW>
 __global__ void __launch_bounds__(256) k_fwd_v(FwdArgs a)
 {
-    const int z = blockIdx.x * 32 + threadIdx.x;
-    const int x = blockIdx.y * 8 + threadIdx.y;
-    if (x >= a.g.ntx || z >= a.g.ntz) return;
+    int x, z0;
+    cell4(x, z0);
+    if (x >= a.g.ntx || z0 >= a.g.ntz) return;
 #pragma unroll
-    for (int k = 0; k < NW; k++) v_update<LC, false>(a.g, a.c, a.rho, a.w[k], a.g.odx, a.g.odz, x, z);
+    for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.rho, a.w[k], a.g.odx, a.g.odz, x, z0);
 }
-
-template <typename S> __device__ __forceinline__ S to_store(float v);
-template <> __device__ __forceinline__ float to_store<float>(float v) { return v; }
-template <> __device__ __forceinline__ __half to_store<__half>(float v) { return __float2half_rn(v); }
-template <> __device__ __forceinline__ __nv_bfloat16 to_store<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
 template <int LC, int NW>
 __global__ void __launch_bounds__(256) k_fwd_p(FwdArgs a)
 {
-    const int z = blockIdx.x * 32 + threadIdx.x;
-    const int x = blockIdx.y * 8 + threadIdx.y;
+    const int it = *a.itp + a.itoff;
+    int x, z0;
+    cell4(x, z0);
     const Geo &g = a.g;
-    const bool in = (x < g.ntx && z < g.ntz);
-    float pn[NW];
+    const bool in = x < g.ntx && z0 < g.ntz;
+    float4 pn[NW];
 #pragma unroll
-    for (int k = 0; k < NW; k++) pn[k] = 0.f;
+    for (int k = 0; k < NW; k++) pn[k] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (in) {
-        const size_t ip = cidx(x, z, g.ldz);
+        const size_t ip = (size_t)x * g.ldz + z0;
 #pragma unroll
-        for (int k = 0; k < NW; k++) {
-            bool upd = p_update<LC>(g, a.c, a.vp, a.rho, a.w[k], g.odx, g.odz, x, z, pn[k]);
-            if (x == a.sx && z == a.sz) { pn[k] += a.amp[k]; upd = true; }
-            if (upd) a.w[k].p[ip] = pn[k];
+        for (int w = 0; w < NW; w++) {
+            bool upd[4];
+            p_update4<LC>(g, a.c, a.vp, a.rho, a.w[w], g.odx, g.odz, x, z0, pn[w], upd);
+            bool any = upd[0] || upd[1] || upd[2] || upd[3];
+            if (x == a.sx) {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (a.sz == z0 + k) { el(pn[w], k) += (w == 0 ? a.wav0[it] : a.wav1[it]); any = true; }
+            }
+            if (any) st4(a.w[w].p + ip, pn[w]);
         }
-        // receivers
         const int wc = __ldg(a.wells.wcol + x);
         if (wc >= 0) {
-            const int tr = __ldg(a.wells.wmap + (size_t)wc * g.ldz + z);
-            if (tr >= 0) a.seis[(size_t)tr * a.nt + a.it] = pn[0];
-        }
-        if (a.colmap) {
-            const int cs = __ldg(a.colmap + x);
-            if (cs >= 0) a.colbuf[((size_t)cs * a.nt + a.it) * g.ldz + z] = make_float2(pn[0], NW > 1 ? pn[NW - 1] : 0.f);
+            const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * g.ldz + z0));
+            const int t[4] = {tr.x, tr.y, tr.z, tr.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (t[k] >= 0 && z0 + k < g.ntz) a.seis[(size_t)t[k] * a.nt + it] = elc(pn[0], k);
+            if (a.colmap) {
+                float2 *cb = a.colbuf + ((size_t)wc * a.nt + it) * g.ldz + z0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) cb[k] = make_float2(elc(pn[0], k), elc(pn[NW - 1], k));
+            }
         }
     }
-    // strips (field 0): uncompressed store, or per-(step, x-block) scaled half/bf16
+    // strips (field 0): uncompressed store, or per-(step, block) scaled half/bf16
     if (a.strips.buf) {
-        const int si = in ? strip_index(x, z, g.ntx, g.ntz, g.pmlc, LC) : -1;
+        int si[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) si[k] = (in && z0 + k < g.ntz) ? strip_index(x, z0 + k, g.ntx, g.ntz, g.pmlc, LC) : -1;
         if (a.strips.prec == 0) {
-            if (si >= 0) ((float *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = pn[0];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (si[k] >= 0) ((float *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = elc(pn[0], k);
         } else {
-            // scale = max |p| over this block's strip cells; the block owns whole columns of
-            // its x-range inside one 32-row z-band, so the scale slot is (step, blockIdx).
             __shared__ float smax;
             if (threadIdx.x == 0 && threadIdx.y == 0) smax = 0.f;
             __syncthreads();
-            float v = si >= 0 ? fabsf(pn[0]) : 0.f;
+            float v = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (si[k] >= 0) v = fmaxf(v, fabsf(elc(pn[0], k)));
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
             if (threadIdx.x == 0 && v > 0.f) atomicMax((int *)&smax, __float_as_int(v));
             __syncthreads();
             const float mx = smax;
             const int slot = blockIdx.y * gridDim.x + blockIdx.x;
-            if (mx > 0.f) {
-                // normalise first (|p|/mx <= 1 even when mx is denormal), then scale into the
-                // half range; the restore undoes it in the same order
-                if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)a.it * a.strips.nscale + slot] = mx;
-                if (si >= 0) {
-                    const float q = pn[0] / mx;
-                    if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = to_store<__half>(q * 32768.f);
-                    else ((__nv_bfloat16 *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = to_store<__nv_bfloat16>(q);
-                }
-            } else {
-                // an all-zero block: store zeros so the restore never reads stale halves
-                if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)a.it * a.strips.nscale + slot] = 0.f;
-                if (si >= 0) {
-                    if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = __float2half_rn(0.f);
-                    else ((__nv_bfloat16 *)a.strips.buf)[(size_t)a.it * a.strips.slen + si] = __float2bfloat16_rn(0.f);
-                }
+            if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)it * a.strips.nscale + slot] = mx;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (si[k] < 0) continue;
+                // normalise first (|p|/mx <= 1 even for denormal mx), then scale to the type
+                const float q = mx > 0.f ? elc(pn[0], k) / mx : 0.f;
+                if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = __float2half_rn(q * 32768.f);
+                else ((__nv_bfloat16 *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = __float2bfloat16_rn(q);
             }
         }
     }
@@ -256,107 +384,174 @@ struct BwdArgs {
     Wave s;              // source wavefield (p, vx, vz only)
     Wave r;              // receiver wavefield
     float *dpdt;
-    float sub;           // rick[it+1]
-    int sx, sz, it, nt;
+    const int *itp;      // time index = *itp + itoff
+    int itoff;
+    const float *wavsub; // wavelet; rick[it+1] is subtracted at the source
+    int sx, sz, nt;
     Strips strips;       // restore
     Wells wells;
     const float *rdata;  // [r_n][nt] preprocessed data injected at the receivers
     double *I, *S, *R;   // FP64 imaging accumulators (R nullable)
 };
 
-// restore: value = (stored / unit) * mx, unit = 32768 for half, 1 for bf16
-template <typename S>
-__device__ __forceinline__ float strip_load(const Strips &st, int it, int si, float mx)
+// one restored strip value; the scale slot is the forward block that saved the cell
+__device__ __forceinline__ float strip_restore(const Strips &st, int it, int si, int x, int z, int nz_blocks)
 {
-    const float unit = sizeof(S) == 2 && st.prec == 1 ? 32768.f : 1.f;
-    return ((float)((const S *)st.buf)[(size_t)it * st.slen + si] / unit) * mx;
+    if (st.prec == 0) return ((const float *)st.buf)[(size_t)it * st.slen + si];
+    const int slot = (x / 8) * nz_blocks + (z / 128);
+    const float mx = st.scale[(size_t)it * st.nscale + slot];
+    if (mx == 0.f) return 0.f;
+    if (st.prec == 1) return ((float)((const __half *)st.buf)[(size_t)it * st.slen + si] / 32768.f) * mx;
+    return (float)((const __nv_bfloat16 *)st.buf)[(size_t)it * st.slen + si] * mx;
 }
-template <>
-__device__ __forceinline__ float strip_load<float>(const Strips &st, int it, int si, float)
+
+__device__ __forceinline__ bool interior(int x, int z, const Geo &g)
 {
-    return ((const float *)st.buf)[(size_t)it * st.slen + si];
+    return z >= g.pmlc && z <= g.ntz - g.pmlc - 1 && x >= g.pmlc && x <= g.ntx - g.pmlc - 1;
 }
 
 template <int LC>
 __global__ void __launch_bounds__(256) k_bwd_1(BwdArgs a)
 {
-    const int z = blockIdx.x * 32 + threadIdx.x;
-    const int x = blockIdx.y * 8 + threadIdx.y;
+    const int it = *a.itp + a.itoff;
+    int x, z0;
+    cell4(x, z0);
     const Geo &g = a.g;
-    if (x >= g.ntx || z >= g.ntz) return;
-    const int ldz = g.ldz, pmlc = g.pmlc;
-    const size_t ip = cidx(x, z, ldz);
+    if (x >= g.ntx || z0 >= g.ntz) return;
+    const int ldz = g.ldz;
+    const size_t ip = (size_t)x * ldz + z0;
     // source wavefield pressure, interior only (fdtd_2d_GPU_kernel_p_backward :434-485)
-    if (z >= pmlc && z <= g.ntz - pmlc - 1 && x >= pmlc && x <= g.ntx - pmlc - 1) {
-        float dvx = 0.f, dvz = 0.f;
+    bool in[4];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
+    const bool src_here = x == a.sx && a.sz >= z0 && a.sz < z0 + 4;
+    if (any) {
+        float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
+        ZWin<LC> vw;
+        vw.load(a.s.vz + (size_t)x * ldz, z0);
 #pragma unroll
         for (int ic = 0; ic < LC; ic++) {
-            dvx += g.rc[ic] * (a.s.vx[ip + ic * ldz] - a.s.vx[ip - (ic + 1) * ldz]) * g.odx;
-            dvz += g.rc[ic] * (a.s.vz[ip + ic] - a.s.vz[ip - (ic + 1)]) * g.odz;
-        }
-        const float v = __ldg(a.vp + ip), rh = __ldg(a.rho + ip);
-        float p = (-g.dt) * rh * v * v * (dvx + dvz) + a.s.p[ip];
-        a.dpdt[ip] = rh * v * v * (dvx + dvz);
-        if (x == a.sx && z == a.sz) p -= a.sub;
-        // boundary strips overwrite (fdtd_2d_GPU_kernel_borders_backward :575-620)
-        const int si = strip_index(x, z, g.ntx, g.ntz, pmlc, LC);
-        if (si >= 0) {
-            if (a.strips.prec == 0) p = strip_load<float>(a.strips, a.it, si, 1.f);
-            else {
-                // the forward kernel's scale slot for this cell: same block tiling
-                const int slot = (x / 8) * ((g.ntz + 31) / 32) + (z / 32);
-                const float mx = a.strips.scale[(size_t)a.it * a.strips.nscale + slot];
-                p = mx == 0.f ? 0.f
-                              : (a.strips.prec == 1 ? strip_load<__half>(a.strips, a.it, si, mx)
-                                                    : strip_load<__nv_bfloat16>(a.strips, a.it, si, mx));
+            const float4 p1 = ld4(a.s.vx + ip + (size_t)ic * ldz), p2 = ld4(a.s.vx + ip - (size_t)(ic + 1) * ldz);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                el(dvx, k) += g.rc[ic] * (elc(p1, k) - elc(p2, k)) * g.odx;
+                el(dvz, k) += g.rc[ic] * (vw.at(k + ic) - vw.at(k - ic - 1)) * g.odz;
             }
         }
-        a.s.p[ip] = p;
-    } else if (x == a.sx && z == a.sz) {
-        a.s.p[ip] -= a.sub;
+        const float4 v = ldg4(a.vp + ip), r = ldg4(a.rho + ip);
+        float4 p = ld4(a.s.p + ip), dp = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int nzb = (g.ntz + 127) / 128;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!in[k]) continue;
+            const float rv = elc(r, k) * elc(v, k) * elc(v, k);
+            el(p, k) = (-g.dt) * elc(r, k) * elc(v, k) * elc(v, k) * (elc(dvx, k) + elc(dvz, k)) + elc(p, k);
+            el(dp, k) = rv * (elc(dvx, k) + elc(dvz, k));
+            if (src_here && a.sz == z0 + k) el(p, k) -= a.wavsub[it + 1];
+            // boundary strips overwrite (fdtd_2d_GPU_kernel_borders_backward :575-620)
+            const int si = strip_index(x, z0 + k, g.ntx, g.ntz, g.pmlc, LC);
+            if (si >= 0) el(p, k) = strip_restore(a.strips, it, si, x, z0 + k, nzb);
+        }
+        if (src_here) {
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (a.sz == z0 + k && !in[k]) el(p, k) -= a.wavsub[it + 1];
+        }
+        st4(a.s.p + ip, p);
+        st4(a.dpdt + ip, dp);
+    } else if (src_here) {
+        a.s.p[ip + (a.sz - z0)] -= a.wavsub[it + 1];
     }
     // receiver wavefield velocities (wide guards, negative spacing)
-    v_update<LC, true>(g, a.c, a.rho, a.r, -g.odx, -g.odz, x, z);
+    v_update4<LC, true>(g, a.c, a.rho, a.r, -g.odx, -g.odz, x, z0);
 }
 
 template <int LC>
 __global__ void __launch_bounds__(256) k_bwd_2(BwdArgs a)
 {
-    const int z = blockIdx.x * 32 + threadIdx.x;
-    const int x = blockIdx.y * 8 + threadIdx.y;
+    const int it = *a.itp + a.itoff;
+    int x, z0;
+    cell4(x, z0);
     const Geo &g = a.g;
-    if (x >= g.ntx || z >= g.ntz) return;
-    const int ldz = g.ldz, pmlc = g.pmlc;
-    const size_t ip = cidx(x, z, ldz);
-    const bool interior = (z >= pmlc && z <= g.ntz - pmlc - 1 && x >= pmlc && x <= g.ntx - pmlc - 1);
+    if (x >= g.ntx || z0 >= g.ntz) return;
+    const int ldz = g.ldz;
+    const size_t ip = (size_t)x * ldz + z0;
+    bool in[4];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
     // source wavefield velocities, interior only (:488-573)
-    if (interior) {
-        float d = 0.f;
+    if (any) {
+        float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int ic = 0; ic < LC; ic++) d += g.rc[ic] * (a.s.p[ip + (ic + 1) * ldz] - a.s.p[ip - ic * ldz]) * g.odx;
-        float orho = __frcp_rn(0.5f * (__ldg(a.rho + ip) + __ldg(a.rho + ip + ldz)));
-        a.s.vx[ip] = (-g.dt) * orho * d + a.s.vx[ip];
-        d = 0.f;
+        for (int ic = 0; ic < LC; ic++) {
+            const float4 p1 = ld4(a.s.p + ip + (size_t)(ic + 1) * ldz), p2 = ld4(a.s.p + ip - (size_t)ic * ldz);
 #pragma unroll
-        for (int ic = 0; ic < LC; ic++) d += g.rc[ic] * (a.s.p[ip + (ic + 1)] - a.s.p[ip - ic]) * g.odz;
-        orho = __frcp_rn(0.5f * (__ldg(a.rho + ip) + __ldg(a.rho + ip + 1)));
-        a.s.vz[ip] = (-g.dt) * orho * d + a.s.vz[ip];
+            for (int k = 0; k < 4; k++) el(d, k) += g.rc[ic] * (elc(p1, k) - elc(p2, k)) * g.odx;
+        }
+        const float4 r0 = ldg4(a.rho + ip), r1 = ldg4(a.rho + ip + ldz);
+        float4 vx = ld4(a.s.vx + ip);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float orho = __frcp_rn(0.5f * (elc(r0, k) + elc(r1, k)));
+            if (in[k]) el(vx, k) = (-g.dt) * orho * elc(d, k) + elc(vx, k);
+        }
+        st4(a.s.vx + ip, vx);
+        ZWin<LC> pw;
+        pw.load(a.s.p + (size_t)x * ldz, z0);
+        d = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int ic = 0; ic < LC; ic++) el(d, k) += g.rc[ic] * (pw.at(k + ic + 1) - pw.at(k - ic)) * g.odz;
+        const float r4 = __ldg(a.rho + ip + 4);
+        float4 vz = ld4(a.s.vz + ip);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float rn = k < 3 ? elc(r0, k + 1) : r4;
+            const float orho = __frcp_rn(0.5f * (elc(r0, k) + rn));
+            if (in[k]) el(vz, k) = (-g.dt) * orho * elc(d, k) + elc(vz, k);
+        }
+        st4(a.s.vz + ip, vz);
     }
     // receiver pressure + hard injection (:717-782)
-    float pr;
-    bool upd = p_update<LC>(g, a.c, a.vp, a.rho, a.r, -g.odx, -g.odz, x, z, pr);
+    float4 pr;
+    bool upd[4];
+    p_update4<LC>(g, a.c, a.vp, a.rho, a.r, -g.odx, -g.odz, x, z0, pr, upd);
+    bool wr = upd[0] || upd[1] || upd[2] || upd[3];
     const int wc = __ldg(a.wells.wcol + x);
     if (wc >= 0) {
-        const int tr = __ldg(a.wells.wmap + (size_t)wc * ldz + z);
-        if (tr >= 0) { pr = a.rdata[(size_t)tr * a.nt + a.it]; upd = true; }
+        const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * ldz + z0));
+        const int t[4] = {tr.x, tr.y, tr.z, tr.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (t[k] >= 0 && z0 + k < g.ntz) { el(pr, k) = a.rdata[(size_t)t[k] * a.nt + it]; wr = true; }
     }
-    if (upd) a.r.p[ip] = pr;
+    if (wr) st4(a.r.p + ip, pr);
     // imaging condition in FP64 (sum_image_GPU_kernel_image :785-817)
-    if (interior) {
-        const double dp = (double)a.dpdt[ip];
-        a.I[ip] += dp * (double)pr;
-        a.S[ip] += dp * dp;
-        if (a.R) a.R[ip] += (double)pr * (double)pr;
+    if (any) {
+        const float4 dp4 = ld4(a.dpdt + ip);
+        double2 *I2 = reinterpret_cast<double2 *>(a.I + ip), *S2 = reinterpret_cast<double2 *>(a.S + ip);
+        double2 i0 = I2[0], i1 = I2[1], s0 = S2[0], s1 = S2[1];
+        double *iv[4] = {&i0.x, &i0.y, &i1.x, &i1.y}, *sv[4] = {&s0.x, &s0.y, &s1.x, &s1.y};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!in[k]) continue;
+            const double dp = (double)elc(dp4, k);
+            *iv[k] += dp * (double)elc(pr, k);
+            *sv[k] += dp * dp;
+        }
+        I2[0] = i0; I2[1] = i1; S2[0] = s0; S2[1] = s1;
+        if (a.R) {
+            double2 *R2 = reinterpret_cast<double2 *>(a.R + ip);
+            double2 q0 = R2[0], q1 = R2[1];
+            double *rv[4] = {&q0.x, &q0.y, &q1.x, &q1.y};
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (in[k]) *rv[k] += (double)elc(pr, k) * (double)elc(pr, k);
+            R2[0] = q0; R2[1] = q1;
+        }
     }
 }
 

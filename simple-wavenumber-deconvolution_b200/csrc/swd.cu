@@ -16,6 +16,7 @@
 
 #include "../../include/swd.h"
 #include "prop.cuh"
+#include "prop_fused.cuh"
 #include "fft.cuh"
 #include "decon.cuh"
 
@@ -25,8 +26,9 @@ using namespace swd;
 // small helpers
 // ------------------------------------------------------------------------------------
 struct DevBuf {
-    void *p = nullptr;
-    size_t n = 0;
+    void *p = nullptr;   // allocation base (what cudaFree takes)
+    size_t n = 0;        // bytes allocated
+    size_t off = 0;      // byte offset of element 0 (guard band of grid arrays)
 };
 
 struct swd_ctx {
@@ -44,6 +46,9 @@ struct swd_ctx {
     DevBuf vp, rho, cpml[8];
     // wavefields: w[0], w[1] (7 arrays each), dp/dt
     DevBuf wave[2][7], dpdt;
+    // second copies of p, vx, vz, phi_p_x, phi_p_z for the fused (double-buffered) path
+    DevBuf wave2[2][5];
+    int path = SWD_PATH_PLAIN;
     // acquisition
     DevBuf wcol, wmap, seis, seis2, rdata, colbuf, kzcoef, tw;
     // strips
@@ -52,20 +57,31 @@ struct swd_ctx {
     DevBuf I, S, R, stack, reduce;
     bool have_R = false, have_shot = false;
     DevBuf stage_in, stage_out;
+    // chunked CUDA-graph execution of the time loops
+    DevBuf ctrl, wav;
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr, probe = nullptr;
+        std::vector<char> key;
+        std::vector<cudaEvent_t> ev;   // probe events: (start, end) per kernel of the probed step
+    } gfwd, gbwd;
+    int use_graphs = 1;
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
     long long prof_n[SWD_NKERNELS] = {0};
     long long launches = 0;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+    std::vector<int> prof_count;
     std::vector<cudaEvent_t> ev_pool;
     swd_ctx()
     {
         DevBuf *all[] = {&vp, &rho, &dpdt, &wcol, &wmap, &seis, &seis2, &rdata, &colbuf, &kzcoef, &tw,
-                         &strips, &strip_scale, &I, &S, &R, &stack, &reduce, &stage_in, &stage_out};
+                         &strips, &strip_scale, &I, &S, &R, &stack, &reduce, &stage_in, &stage_out, &ctrl, &wav};
         for (DevBuf *b : all) bufs.push_back(b);
         for (auto &b : cpml) bufs.push_back(&b);
         for (auto &w : wave)
+            for (auto &b : w) bufs.push_back(&b);
+        for (auto &w : wave2)
             for (auto &b : w) bufs.push_back(&b);
     }
 };
@@ -97,6 +113,7 @@ static int fail(swd_ctx *c, int code, const char *fmt, ...)
 
 static int ensure(swd_ctx *ctx, DevBuf &b, size_t bytes)
 {
+    b.off = 0;
     if (b.n >= bytes && b.p) return SWD_OK;
     if (b.p) {
         cudaStreamSynchronize(ctx->stream);
@@ -164,8 +181,20 @@ static int grid_to_dev(swd_ctx *ctx, float *dst, const float *src)
     return SWD_OK;
 }
 
-static inline float *F(DevBuf &b) { return (float *)b.p; }
-static inline double *D(DevBuf &b) { return (double *)b.p; }
+static inline float *F(DevBuf &b) { return (float *)((char *)b.p + b.off); }
+static inline double *D(DevBuf &b) { return (double *)((char *)b.p + b.off); }
+
+// A grid-shaped array: ntx*ldz elements plus GUARD elements on both sides, zero-filled, so
+// the four-cell kernels can read the vector chunks next to the grid edges.
+static int ensure_grid(swd_ctx *ctx, DevBuf &b, size_t elem, size_t extra_cols = 0)
+{
+    const size_t n = ((size_t)(ctx->ntx + extra_cols) * ctx->ldz + 2 * GUARD) * elem;
+    const bool fresh = !(b.p && b.n >= n);
+    CKR(ensure(ctx, b, n));
+    b.off = GUARD * elem;
+    if (fresh) CK(cudaMemsetAsync(b.p, 0, b.n, ctx->stream));
+    return SWD_OK;
+}
 static inline int *I32(DevBuf &b) { return (int *)b.p; }
 
 static Geo make_geo(const swd_ctx *c)
@@ -208,18 +237,23 @@ static cudaEvent_t ev_get(swd_ctx *c)
     return e;
 }
 
-struct ProfScope {   // records a (start, end) event pair around one launch when active
+struct ProfScope {   // records a (start, end) event pair around a span of work when active
     swd_ctx *c;
     int k;
     bool on;
+    int count;
     cudaEvent_t a{}, b{};
-    ProfScope(swd_ctx *c_, int k_, bool on_) : c(c_), k(k_), on(on_)
+    ProfScope(swd_ctx *c_, int k_, bool on_, int count_ = 1) : c(c_), k(k_), on(on_), count(count_)
     {
         if (on) { a = ev_get(c); b = ev_get(c); cudaEventRecord(a, c->stream); }
     }
     ~ProfScope()
     {
-        if (on) { cudaEventRecord(b, c->stream); c->prof_pending.push_back({k, {a, b}}); }
+        if (on) {
+            cudaEventRecord(b, c->stream);
+            c->prof_pending.push_back({k, {a, b}});
+            c->prof_count.push_back(count);
+        }
     }
 };
 
@@ -227,16 +261,18 @@ static void prof_collect(swd_ctx *c)
 {
     if (c->prof_pending.empty()) return;
     cudaStreamSynchronize(c->stream);
-    for (auto &p : c->prof_pending) {
+    for (size_t i = 0; i < c->prof_pending.size(); i++) {
+        auto &p = c->prof_pending[i];
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
             c->prof_ms[p.first] += ms;
-            c->prof_n[p.first] += 1;
+            c->prof_n[p.first] += c->prof_count[i];
         }
         c->ev_pool.push_back(p.second.first);
         c->ev_pool.push_back(p.second.second);
     }
     c->prof_pending.clear();
+    c->prof_count.clear();
     cudaGetLastError();
 }
 
@@ -245,13 +281,42 @@ static size_t grid_bytes(const swd_ctx *c) { return (size_t)c->ntx * c->ldz * si
 static int zero_wave(swd_ctx *ctx, int k)
 {
     for (int i = 0; i < 7; i++) {
-        CKR(ensure(ctx, ctx->wave[k][i], grid_bytes(ctx)));
-        CK(cudaMemsetAsync(ctx->wave[k][i].p, 0, grid_bytes(ctx), ctx->stream));
+        CKR(ensure_grid(ctx, ctx->wave[k][i], sizeof(float)));
+        CK(cudaMemsetAsync(ctx->wave[k][i].p, 0, ctx->wave[k][i].n, ctx->stream));
     }
     return SWD_OK;
 }
 
-static dim3 grid_blocks(const swd_ctx *c) { return dim3((c->ntz + 31) / 32, (c->ntx + 7) / 8); }
+static dim3 grid_blocks(const swd_ctx *c) { return dim3((c->ntz + 127) / 128, (c->ntx + 7) / 8); }
+
+// ---- fused path: 32 x 32 tiles, double-buffered fields --------------------------------
+constexpr int FTX = 32, FTZ = 32;
+static bool fused(const swd_ctx *c) { return c->path == SWD_PATH_FUSED && c->Lc <= 6; }
+static dim3 fused_blocks(const swd_ctx *c) { return dim3((c->ntz + FTZ - 1) / FTZ, (c->ntx + FTX - 1) / FTX); }
+
+static int zero_wave2(swd_ctx *ctx, int k)
+{
+    for (int i = 0; i < 5; i++) {
+        CKR(ensure_grid(ctx, ctx->wave2[k][i], sizeof(float)));
+        CK(cudaMemsetAsync(ctx->wave2[k][i].p, 0, ctx->wave2[k][i].n, ctx->stream));
+    }
+    return SWD_OK;
+}
+
+// copy `par` of field k: par 0 = wave[k][0..4], par 1 = wave2[k][0..4]
+static float *fcopy(swd_ctx *c, int k, int par, int i) { return par ? F(c->wave2[k][i]) : F(c->wave[k][i]); }
+
+static Field2 make_field2(swd_ctx *c, int k, int in_par)
+{
+    Field2 f;
+    const int o = 1 - in_par;
+    f.p = fcopy(c, k, in_par, 0); f.vx = fcopy(c, k, in_par, 1); f.vz = fcopy(c, k, in_par, 2);
+    f.ppx = fcopy(c, k, in_par, 3); f.ppz = fcopy(c, k, in_par, 4);
+    f.po = fcopy(c, k, o, 0); f.vxo = fcopy(c, k, o, 1); f.vzo = fcopy(c, k, o, 2);
+    f.ppxo = fcopy(c, k, o, 3); f.ppzo = fcopy(c, k, o, 4);
+    f.pvx = F(c->wave[k][5]); f.pvz = F(c->wave[k][6]);
+    return f;
+}
 
 // ------------------------------------------------------------------------------------
 // acquisition: receivers grouped by well column
@@ -474,37 +539,49 @@ __global__ void k_pml_z(float *v, int ntx, int ntz, int pml)
 // launch dispatch on the stencil half-length
 // ------------------------------------------------------------------------------------
 template <int LC>
-static void launch_fwd(swd_ctx *c, const FwdArgs &a, int nw, dim3 grid, bool prof)
+static void launch_fwd_v(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s)
 {
-    dim3 blk(32, 8);
-    cudaStream_t s = c->stream;
-    {
-        ProfScope ps(c, 0, prof);
-        if (nw == 2) k_fwd_v<LC, 2><<<grid, blk, 0, s>>>(a);
-        else k_fwd_v<LC, 1><<<grid, blk, 0, s>>>(a);
-    }
-    {
-        ProfScope ps(c, 1, prof);
-        if (nw == 2) k_fwd_p<LC, 2><<<grid, blk, 0, s>>>(a);
-        else k_fwd_p<LC, 1><<<grid, blk, 0, s>>>(a);
-    }
-    c->launches += 2;
+    if (nw == 2) k_fwd_v<LC, 2><<<grid, dim3(32, 8), 0, s>>>(a);
+    else k_fwd_v<LC, 1><<<grid, dim3(32, 8), 0, s>>>(a);
 }
 
 template <int LC>
-static void launch_bwd(swd_ctx *c, const BwdArgs &a, dim3 grid, bool prof)
+static void launch_fwd_p(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s)
 {
-    dim3 blk(32, 8);
-    {
-        ProfScope ps(c, 2, prof);
-        k_bwd_1<LC><<<grid, blk, 0, c->stream>>>(a);
-    }
-    {
-        ProfScope ps(c, 3, prof);
-        k_bwd_2<LC><<<grid, blk, 0, c->stream>>>(a);
-    }
-    c->launches += 2;
+    if (nw == 2) k_fwd_p<LC, 2><<<grid, dim3(32, 8), 0, s>>>(a);
+    else k_fwd_p<LC, 1><<<grid, dim3(32, 8), 0, s>>>(a);
 }
+
+template <int LC>
+static void launch_bwd_1(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_1<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+
+template <int LC>
+static void launch_bwd_2(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_2<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+
+template <int LC>
+static void launch_fwd_fused(const FStepArgs &a, int nw, cudaStream_t s)
+{
+    const dim3 grid((a.g.ntz + FTZ - 1) / FTZ, (a.g.ntx + FTX - 1) / FTX);
+    if (nw == 2) k_fwd_step<LC, 2, FTX, FTZ><<<grid, 256, 0, s>>>(a);
+    else k_fwd_step<LC, 1, FTX, FTZ><<<grid, 256, 0, s>>>(a);
+}
+
+template <int LC>
+static void launch_bwd_fused(const BStepArgs &a, cudaStream_t s)
+{
+    const dim3 grid((a.g.ntz + FTZ - 1) / FTZ, (a.g.ntx + FTX - 1) / FTX);
+    k_bwd_step<LC, FTX, FTZ><<<grid, 256, 0, s>>>(a);
+}
+
+#define LC_DISPATCH6(LCV, FN, ...)                               \
+    switch (LCV) {                                               \
+        case 1: FN<1>(__VA_ARGS__); break;                       \
+        case 2: FN<2>(__VA_ARGS__); break;                       \
+        case 3: FN<3>(__VA_ARGS__); break;                       \
+        case 4: FN<4>(__VA_ARGS__); break;                       \
+        case 5: FN<5>(__VA_ARGS__); break;                       \
+        default: FN<6>(__VA_ARGS__); break;                      \
+    }
 
 #define LC_DISPATCH(LCV, FN, ...)                                \
     switch (LCV) {                                               \
@@ -550,10 +627,113 @@ struct FwdJob {
     float2 *colbuf = nullptr;
 };
 
+// device copies of the shot's wavelet(s): wav[0..nt) = rick, wav[nt..2nt) = Hilbert twin
+static int upload_wavelets(swd_ctx *ctx, const FwdJob &J, int nt)
+{
+    CKR(ensure(ctx, ctx->wav, sizeof(float) * 2 * (size_t)ctx->grid.nt_max));
+    CK(cudaMemcpyAsync(F(ctx->wav), J.rick.data(), sizeof(float) * nt, cudaMemcpyHostToDevice, ctx->stream));
+    if (J.twin) CK(cudaMemcpyAsync(F(ctx->wav) + nt, J.hrick.data(), sizeof(float) * nt, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));   // the host vectors may go away after this
+    return SWD_OK;
+}
+
 static int strip_len(const swd_ctx *c) { return 2 * c->Lc * c->nx + 2 * c->Lc * (c->nz - 2 * c->Lc); }
+
+
+// ------------------------------------------------------------------------------------
+// Chunked graph execution of a time loop.  The step kernels read their time index from a
+// device counter (it = *counter + itoff), so one captured graph of K steps followed by a
+// one-thread counter advance serves every chunk; it is replayed nsteps/K times and the
+// remaining steps are launched directly.  The graph is re-captured only when the step
+// arguments (pointers, geometry, shot) change.  When profiling is on, each chunk is replayed
+// from a probe copy whose first step is bracketed by event nodes, read after the chunk.
+// ------------------------------------------------------------------------------------
+constexpr int GRAPH_K = 64;
+
+__global__ void k_advance(int *counter, int d) { *counter += d; }
+
+static void graph_free(swd_ctx::StepGraph &G)
+{
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    if (G.probe) cudaGraphExecDestroy(G.probe);
+    for (cudaEvent_t e : G.ev) cudaEventDestroy(e);
+    G = swd_ctx::StepGraph();
+}
+
+template <class Launch>
+static int capture_chunk(swd_ctx *ctx, cudaGraphExec_t *out, int dir, int *counter, Launch launch, cudaEvent_t *ev)
+{
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < GRAPH_K; k++) launch(k, k == GRAPH_K / 2 ? ev : nullptr);
+    k_advance<<<1, 1, 0, ctx->stream>>>(counter, dir * GRAPH_K);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (e != cudaSuccess) return fail(ctx, SWD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, SWD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    return SWD_OK;
+}
+
+// Launch(k, ev): enqueue step k (itoff = dir*k) on ctx->stream; when ev != nullptr record
+// ev[2j] / ev[2j+1] around its j-th kernel.  nk kernels per step with profiling ids kid[].
+template <class Launch>
+static int run_steps(swd_ctx *ctx, swd_ctx::StepGraph &G, const void *key, size_t keylen, int start, int dir,
+                     int nsteps, int nk, const int *kid, Launch launch)
+{
+    CKR(ensure(ctx, ctx->ctrl, 64));
+    int *counter = I32(ctx->ctrl);
+    CK(cudaMemcpyAsync(counter, &start, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    // the legacy default stream (handle 0) cannot be captured: launch directly there
+    const int nchunks = (ctx->use_graphs && ctx->stream != nullptr) ? nsteps / GRAPH_K : 0;
+    const int rem = nsteps - nchunks * GRAPH_K;
+    const bool prof = ctx->prof_every > 0;
+    if (nchunks > 0) {
+        const bool same = G.exec && G.key.size() == keylen && memcmp(G.key.data(), key, keylen) == 0;
+        if (!same) {
+            graph_free(G);
+            G.key.assign((const char *)key, (const char *)key + keylen);
+            CKR(capture_chunk(ctx, &G.exec, dir, counter, launch, nullptr));
+        }
+        if (prof && !G.probe) {
+            G.ev.resize(2 * nk);
+            for (auto &e : G.ev) CK(cudaEventCreate(&e));
+            CKR(capture_chunk(ctx, &G.probe, dir, counter, launch, G.ev.data()));
+        }
+    }
+    const int pc = prof && nchunks > 0 ? nchunks / 2 : -1;   // the chunk that carries the probe events
+    {
+        // whole-pass time per step (profiling ids 6 forward, 7 backward)
+        ProfScope pass(ctx, dir > 0 ? 6 : 7, prof, nsteps);
+        for (int c = 0; c < nchunks; c++) {
+            CK(cudaGraphLaunch(c == pc ? G.probe : G.exec, ctx->stream));
+            ctx->launches += (long long)nk * GRAPH_K;
+        }
+        for (int k = 0; k < rem; k++) {
+            launch(k, nullptr);
+            ctx->launches += nk;
+        }
+    }
+    CK(cudaGetLastError());
+    if (pc >= 0) {
+        // the probe step sits mid-chunk between busy neighbours; read it once the pass drained
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (int j = 0; j < nk; j++) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, G.ev[2 * j], G.ev[2 * j + 1]) == cudaSuccess) {
+                ctx->prof_ms[kid[j]] += ms;
+                ctx->prof_n[kid[j]] += 1;
+            }
+        }
+    }
+    return SWD_OK;
+}
+
+static int run_forward_fused(swd_ctx *ctx, FwdJob &J, ShotPlan &P);
 
 static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
 {
+    if (fused(ctx)) return run_forward_fused(ctx, J, P);
     const swd_shot *s = J.shot;
     const int nt = s->nt;
     CKR(zero_wave(ctx, 0));
@@ -589,15 +769,88 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
             a.strips.scale = F(ctx->strip_scale);
         }
     }
-    for (int it = 0; it < nt; it++) {
-        a.it = it;
-        a.amp[0] = J.rick[it];
-        a.amp[1] = J.twin ? J.hrick[it] : 0.f;
-        const bool prof = ctx->prof_every > 0 && it % ctx->prof_every == 0;
-        LC_DISPATCH(ctx->Lc, launch_fwd, ctx, a, J.twin ? 2 : 1, grid, prof);
+    CKR(upload_wavelets(ctx, J, nt));
+    CKR(ensure(ctx, ctx->ctrl, 64));
+    a.itp = I32(ctx->ctrl);
+    a.wav0 = F(ctx->wav);
+    a.wav1 = J.twin ? F(ctx->wav) + nt : F(ctx->wav);
+    const int nw = J.twin ? 2 : 1;
+    auto launch = [&](int k, cudaEvent_t *ev) {
+        FwdArgs b = a;
+        b.itoff = k;
+        const dim3 blk(32, 8);
+        if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
+        LC_DISPATCH(ctx->Lc, launch_fwd_v, b, nw, grid, ctx->stream);
+        if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
+        LC_DISPATCH(ctx->Lc, launch_fwd_p, b, nw, grid, ctx->stream);
+        if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
+        (void)blk;
+    };
+    const int kid[2] = {0, 1};
+    a.itoff = 0;
+    return run_steps(ctx, ctx->gfwd, &a, sizeof a, 0, +1, nt, 2, kid, launch);
+}
+
+// Fused forward: step it reads copy it%2 and writes copy (it+1)%2 of every double-buffered
+// array; the final state ends in copy nt%2.
+static int run_forward_fused(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
+{
+    const swd_shot *s = J.shot;
+    const int nt = s->nt;
+    const int nw = J.twin ? 2 : 1;
+    for (int k = 0; k < nw; k++) {
+        CKR(zero_wave(ctx, k));
+        CKR(zero_wave2(ctx, k));
     }
-    CK(cudaGetLastError());
-    return SWD_OK;
+    FStepArgs a;
+    memset(&a, 0, sizeof a);
+    a.g = make_geo(ctx);
+    a.c = make_cpml(ctx);
+    a.vp = F(ctx->vp);
+    a.rho = F(ctx->rho);
+    a.sx = s->s_ix;
+    a.sz = s->s_iz;
+    a.nt = nt;
+    a.wells.wcol = I32(ctx->wcol);
+    a.wells.wmap = I32(ctx->wmap);
+    a.seis = J.seis_dev;
+    a.colmap = J.colbuf ? I32(ctx->wcol) : nullptr;
+    a.colbuf = J.colbuf;
+    const dim3 grid = fused_blocks(ctx);
+    if (J.save_strips) {
+        const int slen = strip_len(ctx);
+        const int nscale = grid.x * grid.y;
+        const size_t esz = ctx->strip_prec == SWD_STRIP_F32 ? 4 : 2;
+        CKR(ensure(ctx, ctx->strips, esz * (size_t)slen * nt));
+        a.strips.buf = ctx->strips.p;
+        a.strips.slen = slen;
+        a.strips.prec = ctx->strip_prec;
+        a.strips.nscale = nscale;
+        if (ctx->strip_prec != SWD_STRIP_F32) {
+            CKR(ensure(ctx, ctx->strip_scale, sizeof(float) * (size_t)nscale * nt));
+            a.strips.scale = F(ctx->strip_scale);
+        }
+    }
+    CKR(upload_wavelets(ctx, J, nt));
+    CKR(ensure(ctx, ctx->ctrl, 64));
+    a.itp = I32(ctx->ctrl);
+    a.wav0 = F(ctx->wav);
+    a.wav1 = J.twin ? F(ctx->wav) + nt : F(ctx->wav);
+    a.w[0] = make_field2(ctx, 0, 0);
+    a.w[1] = nw == 2 ? make_field2(ctx, 1, 0) : a.w[0];
+    auto launch = [&](int k, cudaEvent_t *ev) {
+        // chunks start at even steps, so step k of a chunk reads copy k%2
+        FStepArgs b = a;
+        b.itoff = k;
+        b.w[0] = make_field2(ctx, 0, k & 1);
+        b.w[1] = nw == 2 ? make_field2(ctx, 1, k & 1) : b.w[0];
+        if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
+        LC_DISPATCH6(ctx->Lc, launch_fwd_fused, b, nw, ctx->stream);
+        if (ev) cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal);
+    };
+    const int kid[1] = {4};
+    a.itoff = 0;
+    return run_steps(ctx, ctx->gfwd, &a, sizeof a, 0, +1, nt, 1, kid, launch);
 }
 
 static int check_ready(swd_ctx *ctx)
@@ -730,6 +983,8 @@ int swd_destroy(swd_ctx *ctx)
         if (b->p) cudaFree(b->p);
     prof_collect(ctx);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    graph_free(ctx->gfwd);
+    graph_free(ctx->gbwd);
     if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SWD_OK;
@@ -805,9 +1060,13 @@ int swd_set_cpml(swd_ctx *ctx, const float *a_x, const float *a_x_half, const fl
     CK(cudaSetDevice(ctx->dev));
     for (int i = 0; i < 8; i++) {
         if (!src[i]) return fail(ctx, SWD_ERR_ARG, "CPML array %d is NULL", i);
-        const int n = (i % 4) < 2 ? ctx->ntx : ctx->ntz;
-        CKR(ensure(ctx, ctx->cpml[i], sizeof(float) * n));
-        CKR(to_dev(ctx, ctx->cpml[i].p, src[i], sizeof(float) * n));
+        const bool xaxis = (i % 4) < 2;
+        const int n = xaxis ? ctx->ntx : ctx->ntz;
+        const size_t cap = (size_t)(xaxis ? ctx->ntx : ctx->ldz) + 2 * GUARD;
+        CKR(ensure(ctx, ctx->cpml[i], sizeof(float) * cap));
+        ctx->cpml[i].off = GUARD * sizeof(float);
+        CK(cudaMemsetAsync(ctx->cpml[i].p, 0, ctx->cpml[i].n, ctx->stream));
+        CKR(to_dev(ctx, F(ctx->cpml[i]), src[i], sizeof(float) * n));
     }
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_cpml = true;
@@ -818,17 +1077,24 @@ int swd_set_model(swd_ctx *ctx, const float *vp, const float *rho)
 {
     if (!ctx || !vp || !rho) return fail(ctx, SWD_ERR_ARG, "vp/rho is NULL");
     CK(cudaSetDevice(ctx->dev));
-    // one extra column and row of padding so the half-node buoyancy reads at x+1 / z+1
-    // of the last cells stay inside the allocation
-    const size_t bytes = (size_t)(ctx->ntx + 1) * ctx->ldz * sizeof(float);
-    CKR(ensure(ctx, ctx->vp, bytes));
-    CKR(ensure(ctx, ctx->rho, bytes));
-    CK(cudaMemsetAsync(ctx->vp.p, 0, bytes, ctx->stream));
-    CK(cudaMemsetAsync(ctx->rho.p, 0, bytes, ctx->stream));
+    // one extra column of padding so the half-node buoyancy reads at x+1 of the last cells
+    // stay inside the allocation; guard bands for the vector chunk reads
+    CKR(ensure_grid(ctx, ctx->vp, sizeof(float), 1));
+    CKR(ensure_grid(ctx, ctx->rho, sizeof(float), 1));
+    CK(cudaMemsetAsync(ctx->vp.p, 0, ctx->vp.n, ctx->stream));
+    CK(cudaMemsetAsync(ctx->rho.p, 0, ctx->rho.n, ctx->stream));
     CKR(grid_to_dev(ctx, F(ctx->vp), vp));
     CKR(grid_to_dev(ctx, F(ctx->rho), rho));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_model = true;
+    return SWD_OK;
+}
+
+int swd_set_kernel_path(swd_ctx *ctx, int path)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    if (path != SWD_PATH_PLAIN && path != SWD_PATH_FUSED) return fail(ctx, SWD_ERR_ARG, "unknown kernel path %d", path);
+    ctx->path = path;
     return SWD_OK;
 }
 
@@ -925,18 +1191,27 @@ int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const fl
         CK(cudaMemcpyAsync(rms, raw, sizeof(float) * ntr, cudaMemcpyDeviceToDevice, ctx->stream));
     }
     // 3. backward: reconstruction + receiver back-propagation + FP64 imaging
+    const bool fz = fused(ctx);
     CKR(zero_wave(ctx, 1));
+    if (fz) {
+        CKR(zero_wave2(ctx, 1));
+        // both copies of the source wavefield start from the final forward state (copy nt%2)
+        const int fpar = nt & 1;
+        for (int i = 0; i < 3; i++)
+            CK(cudaMemcpyAsync(fcopy(ctx, 0, 1 - fpar, i), fcopy(ctx, 0, fpar, i), grid_bytes(ctx),
+                               cudaMemcpyDeviceToDevice, ctx->stream));
+    }
     const size_t gb = (size_t)ctx->ntx * ctx->ldz;
-    CKR(ensure(ctx, ctx->dpdt, sizeof(float) * gb));
-    CK(cudaMemsetAsync(ctx->dpdt.p, 0, sizeof(float) * gb, ctx->stream));
-    CKR(ensure(ctx, ctx->I, sizeof(double) * gb));
-    CKR(ensure(ctx, ctx->S, sizeof(double) * gb));
-    CK(cudaMemsetAsync(ctx->I.p, 0, sizeof(double) * gb, ctx->stream));
-    CK(cudaMemsetAsync(ctx->S.p, 0, sizeof(double) * gb, ctx->stream));
+    CKR(ensure_grid(ctx, ctx->dpdt, sizeof(float)));
+    CK(cudaMemsetAsync(ctx->dpdt.p, 0, ctx->dpdt.n, ctx->stream));
+    CKR(ensure_grid(ctx, ctx->I, sizeof(double)));
+    CKR(ensure_grid(ctx, ctx->S, sizeof(double)));
+    CK(cudaMemsetAsync(ctx->I.p, 0, ctx->I.n, ctx->stream));
+    CK(cudaMemsetAsync(ctx->S.p, 0, ctx->S.n, ctx->stream));
     ctx->have_R = (flags & SWD_RTM_ILLUM_RCV) != 0;
     if (ctx->have_R) {
-        CKR(ensure(ctx, ctx->R, sizeof(double) * gb));
-        CK(cudaMemsetAsync(ctx->R.p, 0, sizeof(double) * gb, ctx->stream));
+        CKR(ensure_grid(ctx, ctx->R, sizeof(double)));
+        CK(cudaMemsetAsync(ctx->R.p, 0, ctx->R.n, ctx->stream));
     }
     BwdArgs b;
     memset(&b, 0, sizeof b);
@@ -962,11 +1237,50 @@ int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const fl
     b.S = D(ctx->S);
     b.R = ctx->have_R ? D(ctx->R) : nullptr;
     const dim3 grid = grid_blocks(ctx);
-    for (int it = nt - 2; it >= 0; it--) {
-        b.it = it;
-        b.sub = J.rick[it + 1];
-        const bool prof = ctx->prof_every > 0 && it % ctx->prof_every == 0;
-        LC_DISPATCH(ctx->Lc, launch_bwd, ctx, b, grid, prof);
+    CKR(ensure(ctx, ctx->ctrl, 64));
+    if (fz) {
+        BStepArgs f;
+        memset(&f, 0, sizeof f);
+        f.g = b.g; f.c = b.c; f.vp = b.vp; f.rho = b.rho;
+        f.sx = b.sx; f.sz = b.sz; f.nt = nt;
+        f.strips = b.strips;
+        f.strips.nscale = fused_blocks(ctx).x * fused_blocks(ctx).y;
+        f.wells = b.wells; f.rdata = b.rdata; f.I = b.I; f.S = b.S; f.R = b.R;
+        f.itp = I32(ctx->ctrl);
+        f.wavsub = F(ctx->wav);
+        const int fpar = nt & 1;
+        // step j of the backward loop (it = nt-2-j) reads source copy (fpar + j)%2 and receiver
+        // copy j%2; chunks start at even j, so the pattern depends on k = j % GRAPH_K only
+        f.r = make_field2(ctx, 1, 0);
+        auto launch = [&](int k, cudaEvent_t *ev) {
+            BStepArgs q = f;
+            q.itoff = -k;
+            const int spar = (fpar + k) & 1;
+            q.r = make_field2(ctx, 1, k & 1);
+            q.ps = fcopy(ctx, 0, spar, 0); q.vxs = fcopy(ctx, 0, spar, 1); q.vzs = fcopy(ctx, 0, spar, 2);
+            q.pso = fcopy(ctx, 0, 1 - spar, 0); q.vxso = fcopy(ctx, 0, 1 - spar, 1); q.vzso = fcopy(ctx, 0, 1 - spar, 2);
+            if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
+            LC_DISPATCH6(ctx->Lc, launch_bwd_fused, q, ctx->stream);
+            if (ev) cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal);
+        };
+        const int kid[1] = {5};
+        f.itoff = 0;
+        CKR(run_steps(ctx, ctx->gbwd, &f, sizeof f, nt - 2, -1, nt - 1, 1, kid, launch));
+    } else {
+        b.itp = I32(ctx->ctrl);
+        b.wavsub = F(ctx->wav);
+        auto launch = [&](int k, cudaEvent_t *ev) {
+            BwdArgs q = b;
+            q.itoff = -k;
+            if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
+            LC_DISPATCH(ctx->Lc, launch_bwd_1, q, grid, ctx->stream);
+            if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
+            LC_DISPATCH(ctx->Lc, launch_bwd_2, q, grid, ctx->stream);
+            if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
+        };
+        const int kid[2] = {2, 3};
+        b.itoff = 0;
+        CKR(run_steps(ctx, ctx->gbwd, &b, sizeof b, nt - 2, -1, nt - 1, 2, kid, launch));
     }
     CK(cudaGetLastError());
     // 4. per-shot post and stack
@@ -1004,7 +1318,7 @@ int swd_rtm_raw(swd_ctx *ctx, double *image, double *illum_src, double *illum_rc
     DevBuf *src[3] = {&ctx->I, &ctx->S, &ctx->R};
     for (int k = 0; k < 3; k++) {
         if (!dst[k]) continue;
-        CK(cudaMemcpy2DAsync(dst[k], ctx->ntz * sizeof(double), src[k]->p, ctx->ldz * sizeof(double),
+        CK(cudaMemcpy2DAsync(dst[k], ctx->ntz * sizeof(double), D(*src[k]), ctx->ldz * sizeof(double),
                              ctx->ntz * sizeof(double), ctx->ntx,
                              is_device_ptr(dst[k]) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
     }

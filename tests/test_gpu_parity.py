@@ -19,7 +19,7 @@ class Case:
     """One small model set up identically for the engine and the oracle."""
 
     def __init__(self, swd, orc, nx=100, nz=60, pml=10, Lc=4, nt=400, dx=5.0, dz=5.0, dt=5e-4, f0=25.0,
-                 seed=7, geometry="wells", smooth=0, rho_pert=False):
+                 seed=7, geometry="wells", smooth=0, rho_pert=False, path=1):
         rng = np.random.default_rng(seed)
         v = np.full((nx, nz), 1900.0, np.float32)
         v[:, nz // 3:] = 2400.0
@@ -50,12 +50,14 @@ class Case:
         self.E.set_stencil(self.rc)
         self.E.set_cpml(self.cp)
         self.E.set_model(self.vp, self.rho)
+        self.E.set_kernel_path(path)
         self.shot = swd.ShotSpec(self.sx, self.sz, self.rix, self.riz, nt)
 
 
-@pytest.fixture(scope="module")
-def case(swd, orc):
-    return Case(swd, orc)
+@pytest.fixture(scope="module", params=[1, 0], ids=["fused", "plain"])
+def case(swd, orc, request):
+    """Both kernel paths: one launch per step on shared-memory tiles, and one cell per thread."""
+    return Case(swd, orc, path=request.param)
 
 
 def test_forward_matches_oracle(case, orc):
@@ -67,17 +69,20 @@ def test_forward_matches_oracle(case, orc):
     assert rel_l2(seis, o64) < TOL
 
 
-@pytest.mark.parametrize("shape", [(37, 29, 5, 4), (64, 48, 10, 5), (97, 33, 3, 2), (130, 71, 30, 4)])
-def test_forward_odd_grids_and_orders(swd, orc, shape):
+@pytest.mark.parametrize("path", [1, 0], ids=["fused", "plain"])
+@pytest.mark.parametrize("shape", [(37, 29, 5, 4), (64, 48, 10, 5), (97, 33, 3, 2), (130, 71, 30, 4), (70, 45, 6, 6),
+                                   (41, 39, 2, 7)])
+def test_forward_odd_grids_and_orders(swd, orc, shape, path):
     nx, nz, pml, Lc = shape
-    c = Case(swd, orc, nx=nx, nz=nz, pml=pml, Lc=Lc, nt=220)
+    c = Case(swd, orc, nx=nx, nz=nz, pml=pml, Lc=Lc, nt=220, path=path)
     seis = c.E.forward(c.shot, c.rick)
     o64 = orc.forward(c.M, c.G, c.rick, dtype=np.float64)["seis"]
     assert rel_l2(seis, o64) < TOL
 
 
-def test_forward_scattered_receivers_and_duplicates(swd, orc):
-    c = Case(swd, orc, geometry="scattered", nt=260)
+@pytest.mark.parametrize("path", [1, 0], ids=["fused", "plain"])
+def test_forward_scattered_receivers_and_duplicates(swd, orc, path):
+    c = Case(swd, orc, geometry="scattered", nt=260, path=path)
     seis = c.E.forward(c.shot, c.rick)
     o64 = orc.forward(c.M, c.G, c.rick, dtype=np.float64)["seis"]
     assert rel_l2(seis, o64) < TOL
@@ -150,6 +155,19 @@ def test_rtm_shot_matches_oracle(case, swd, orc):
     assert rel_l2(stack, orc.edge_zero(fim.astype(np.float32), case.Lc)) < TOL
 
 
+@pytest.mark.parametrize("path", [1, 0], ids=["fused", "plain"])
+@pytest.mark.parametrize("shape", [(53, 41, 7, 4), (90, 37, 4, 5), (64, 64, 3, 3)])
+def test_rtm_odd_grids(swd, orc, shape, path):
+    nx, nz, pml, Lc = shape
+    c = Case(swd, orc, nx=nx, nz=nz, pml=pml, Lc=Lc, nt=240, path=path, geometry="scattered" if nx == 64 else "wells")
+    data = orc.forward(c.M, c.G, c.rick)["seis"]
+    c.E.rtm_shot(c.shot, c.rick, data, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK)
+    I, S, _ = c.E.rtm_raw()
+    sh = orc.rtm_shot(c.M, c.G, c.rick, data, dtype=np.float64)
+    assert rel_l2(I, sh["img"]) < TOL
+    assert rel_l2(S, sh["illum"]) < TOL
+
+
 def test_rtm_receiver_illumination_and_stack_of_two(case, swd, orc):
     data = orc.forward(case.M, case.G, case.rick)["seis"]
     case.E.stack_reset()
@@ -173,8 +191,9 @@ def test_compressed_strips(case, swd, orc, prec, tol):
     assert 0 < e < tol
 
 
-def test_psf_density_scatterers(swd, orc):
-    c = Case(swd, orc, rho_pert=True, nt=300, smooth=5)
+@pytest.mark.parametrize("path", [1, 0], ids=["fused", "plain"])
+def test_psf_density_scatterers(swd, orc, path):
+    c = Case(swd, orc, rho_pert=True, nt=300, smooth=5, path=path)
     seis = c.E.forward(c.shot, c.rick)
     o64 = orc.forward(c.M, c.G, c.rick, dtype=np.float64)["seis"]
     assert rel_l2(seis, o64) < TOL
