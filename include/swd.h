@@ -131,6 +131,35 @@ int swd_stack_reset(swd_ctx *ctx);
 int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *const *ricks,
                   const float *const *data, unsigned flags);
 
+/* ---- Born modelling and its exact adjoint (LSRTM / velocity gradients) --------------
+ * No reference counterpart: the reference only migrates.  The Born operator linearises the
+ * forward modelling of swd_forward in the bulk modulus kappa = rho*vp^2: the scattered field
+ * propagates beside the background and receives dt*dkappa*S0 after each pressure update (S0
+ * the background's p-update sum), and its pressure is recorded at the receivers.
+ * swd_born_adjoint applies the exact transpose of that discrete operator, CPML included,
+ * so <dseis_star, L dkappa> = <L^T dseis_star, dkappa> to rounding:
+ *   grad[c] = sum_k dt * S0^k[c] * lambda_p^k[c],  lambda the adjoint state.
+ * The adjoint needs S0 at every step in reverse order.  swd_set_checkpointing selects how:
+ *   every == 0: the background pass stores S0 for all nt steps (FP32, nt*ntx*ntz floats);
+ *   every  > 0: the background state (p, vx, vz and 4 CPML arrays) is stored every `every`
+ *               steps at `prec` (SWD_STRIP_F32 / F16 / BF16, 16-bit with one scale per
+ *               snapshot, array and 128x8-cell block) and each segment is recomputed
+ *               before its adjoint steps.  Default: every = 50, BF16.
+ * swd_born optionally leaves the background checkpoints of its pass in `ckpt` (device
+ * memory of at least swd_checkpoint_bytes bytes, caller-owned, its size in ckpt_bytes; a
+ * smaller buffer is rejected with SWD_ERR_ARG); swd_born_adjoint given the same `ckpt` for
+ * the same shot skips its own background pass.  With ckpt = NULL (or every == 0)
+ * swd_born_adjoint runs the background pass itself.
+ *   dkappa  ntx*ntz padded grid (model layout), perturbation of rho*vp^2
+ *   dseis   [r_n][nt] Born data;  resid [r_n][nt] adjoint source
+ *   grad    ntx*ntz padded grid, FP64, d<resid, L dkappa>/d dkappa (overwritten) */
+int swd_set_checkpointing(swd_ctx *ctx, int every, int prec);
+int swd_checkpoint_bytes(swd_ctx *ctx, int nt, size_t *bytes);
+int swd_born(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *dkappa, float *dseis,
+             void *ckpt, size_t ckpt_bytes);
+int swd_born_adjoint(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *resid,
+                     double *grad, const void *ckpt, size_t ckpt_bytes);
+
 /* ---- helpers that run on the GPU ----------------------------------------------------
  * swd_hilbert replaces hilbert_transform1d (forward/headrtm.h:228-229,
  * forward/acoustic_hilbert_fftkz_HLForLc.cu:1257-1324).
@@ -162,10 +191,11 @@ int swd_decon(swd_ctx *ctx, const swd_decon_params *p, const float *migreal,
  * CUDA events on the context stream (0 disables).  swd_profile_read fills, per kernel id
  * (0 forward-v, 1 forward-p, 2 backward-1, 3 backward-2 of the plain path; 4 forward step,
  * 5 backward step of the fused path; 6 / 7 whole forward / backward time steps, i.e. a pass
- * divided by its steps), the summed milliseconds and the
+ * divided by its steps; 8 / 9 the two adjoint kernels of swd_born_adjoint and 10 its whole
+ * adjoint time step), the summed milliseconds and the
  * number of timed launches, and clears them.  swd_launch_count is the number of kernels the
  * context has launched since it was created. */
-#define SWD_NKERNELS 8
+#define SWD_NKERNELS 11
 int swd_profile(swd_ctx *ctx, int every);
 int swd_profile_read(swd_ctx *ctx, double *ms, long long *launches);
 long long swd_launch_count(const swd_ctx *ctx);

@@ -101,7 +101,33 @@ static void FN(upd_vz)(const FN(orc_mdl) *M, FN(orc_fld) *f, float dz, int iz0, 
 }
 
 /* p += dt*rho*vp^2*(dvx/dx + phi_vx_x + dvz/dz + phi_vz_z).  acoustic_HLVSPRTMLc.cu:121-173
- * (guard iz in [Lc, ntz-Lc], ix in [Lc, ntx-Lc]); receiver variant :717-762. */
+ * (guard iz in [Lc, ntz-Lc], ix in [Lc, ntx-Lc]); receiver variant :717-762.
+ * Born extensions (project operator): s_out receives the p-update sum S per updated cell;
+ * with dk, p additionally receives dt*dk*s_in (the scattered field's secondary source). */
+static void FN(upd_p_born)(const FN(orc_mdl) *M, FN(orc_fld) *f, float dx, float dz, T *s_out, const T *dk,
+                           const T *s_in)
+{
+    const int ntz = M->ntz, ntx = M->ntx, Lc = M->Lc;
+    const T odx = (T)(1.0 / (double)dx), odz = (T)(1.0 / (double)dz);
+    const T dt = M->dt;
+#pragma omp parallel for schedule(static)
+    for (int ix = Lc; ix <= ntx - Lc; ix++)
+        for (int iz = Lc; iz <= ntz - Lc; iz++) {
+            size_t ip = (size_t)ix * ntz + iz;
+            T dvx = 0.0, dvz = 0.0;
+            for (int ic = 0; ic < Lc; ic++) {
+                dvx += M->rc[ic] * (f->vx[ip + ic * ntz] - f->vx[ip - (ic + 1) * ntz]) * odx;
+                dvz += M->rc[ic] * (f->vz[ip + ic] - f->vz[ip - (ic + 1)]) * odz;
+            }
+            f->pvx[ip] = M->bx[ix] * f->pvx[ip] + M->ax[ix] * dvx;
+            f->pvz[ip] = M->bz[iz] * f->pvz[ip] + M->az[iz] * dvz;
+            const T S = dvx + f->pvx[ip] + dvz + f->pvz[ip];
+            if (s_out) s_out[ip] = S;
+            f->p[ip] = dt * M->rho[ip] * M->vp[ip] * M->vp[ip] * S + f->p[ip];
+            if (dk) f->p[ip] += dt * dk[ip] * s_in[ip];
+        }
+}
+
 static void FN(upd_p)(const FN(orc_mdl) *M, FN(orc_fld) *f, float dx, float dz)
 {
     const int ntz = M->ntz, ntx = M->ntx, Lc = M->Lc;
@@ -360,6 +386,117 @@ void FN(orc_rtm_post)(const orc_model *m, const T *img, const T *illum_s, T *img
             fimage[ipp] = (T)(-((I[ip + ntz] - 2.0 * I[ip] + I[ip - ntz]) / (dx * dx) +
                                 (I[ip + 1] - 2.0 * I[ip] + I[ip - 1]) / (dz * dz)) * v * v);
         }
+}
+
+
+/* ---------------- Born modelling and its adjoint (project operators) ----------------
+ * The forward step above is linear in the state (p, vx, vz and the four CPML memories) and
+ * in kappa = rho*vp^2.  Born: the scattered field b steps beside the background f and gets
+ * dt*dkappa*S0 after its p update; the receivers record b.p after each step.  The adjoint
+ * below is the transpose written as scatters of each forward loop body, applied in reverse
+ * order (P^T then V^T per step), so its correctness rests on the dot-product identity, not
+ * on matching the device's gathers. */
+void FN(orc_born)(const orc_model *m, const orc_geom *g, const float *rick, const float *dkappa, T *dseis)
+{
+    FN(orc_mdl) M;
+    FN(mdl_init)(&M, m);
+    const int ntx = M.ntx, ntz = M.ntz, Lc = M.Lc, nt = M.nt;
+    const size_t ntp = (size_t)ntx * ntz;
+    T *dk = FN(cvt)(dkappa, ntp);
+    T *s0 = (T *)calloc(ntp, sizeof(T));
+    FN(orc_fld) f, b;
+    FN(fld_alloc)(&f, ntp);
+    FN(fld_alloc)(&b, ntp);
+    const size_t src = (size_t)g->s_ix * ntz + g->s_iz;
+    for (int it = 0; it < nt; it++) {
+        FN(upd_vx)(&M, &f, m->dx, Lc, ntz - Lc, Lc - 1, ntx - Lc - 1);
+        FN(upd_vz)(&M, &f, m->dz, Lc - 1, ntz - Lc - 1, Lc, ntx - Lc);
+        FN(upd_p_born)(&M, &f, m->dx, m->dz, s0, NULL, NULL);
+        f.p[src] += rick[it];
+        FN(upd_vx)(&M, &b, m->dx, Lc, ntz - Lc, Lc - 1, ntx - Lc - 1);
+        FN(upd_vz)(&M, &b, m->dz, Lc - 1, ntz - Lc - 1, Lc, ntx - Lc);
+        FN(upd_p_born)(&M, &b, m->dx, m->dz, NULL, dk, s0);
+        for (int r = 0; r < g->nrec; r++) dseis[(size_t)r * nt + it] = b.p[(size_t)g->r_ix[r] * ntz + g->r_iz[r]];
+    }
+    FN(fld_free)(&f);
+    FN(fld_free)(&b);
+    free(dk);
+    free(s0);
+    FN(mdl_free)(&M);
+}
+
+void FN(orc_born_adjoint)(const orc_model *m, const orc_geom *g, const float *rick, const float *resid, T *grad)
+{
+    FN(orc_mdl) M;
+    FN(mdl_init)(&M, m);
+    const int ntx = M.ntx, ntz = M.ntz, Lc = M.Lc, nt = M.nt;
+    const size_t ntp = (size_t)ntx * ntz;
+    const T odx = (T)(1.0 / (double)m->dx), odz = (T)(1.0 / (double)m->dz), dt = M.dt;
+    /* background pass, S0 of every step stored */
+    T *s0 = (T *)calloc(ntp * nt, sizeof(T));
+    FN(orc_fld) f, l;
+    FN(fld_alloc)(&f, ntp);
+    const size_t src = (size_t)g->s_ix * ntz + g->s_iz;
+    for (int it = 0; it < nt; it++) {
+        FN(upd_vx)(&M, &f, m->dx, Lc, ntz - Lc, Lc - 1, ntx - Lc - 1);
+        FN(upd_vz)(&M, &f, m->dz, Lc - 1, ntz - Lc - 1, Lc, ntx - Lc);
+        FN(upd_p_born)(&M, &f, m->dx, m->dz, s0 + (size_t)it * ntp, NULL, NULL);
+        f.p[src] += rick[it];
+    }
+    FN(fld_free)(&f);
+    /* adjoint: l.p = p^, l.vx/vz = v^, l.ppx/ppz = psi^ (velocity CPML), l.pvx/pvz = phi^ */
+    FN(fld_alloc)(&l, ntp);
+    memset(grad, 0, sizeof(T) * ntp);
+    for (int k = nt - 1; k >= 0; k--) {
+        /* P^T: p' = p + c*(Dx- vx + phi_x' + Dz- vz + phi_z'), phi' = b*phi + a*D- v on Gp */
+        for (int ix = Lc; ix <= ntx - Lc; ix++)
+            for (int iz = Lc; iz <= ntz - Lc; iz++) {
+                const size_t ip = (size_t)ix * ntz + iz;
+                const T q = dt * M.rho[ip] * M.vp[ip] * M.vp[ip] * l.p[ip];
+                const T qx = q + M.ax[ix] * (q + l.pvx[ip]);
+                const T qz = q + M.az[iz] * (q + l.pvz[ip]);
+                l.pvx[ip] = M.bx[ix] * (q + l.pvx[ip]);
+                l.pvz[ip] = M.bz[iz] * (q + l.pvz[ip]);
+                for (int ic = 0; ic < Lc; ic++) {
+                    l.vx[ip + (size_t)ic * ntz] += M.rc[ic] * odx * qx;
+                    l.vx[ip - (size_t)(ic + 1) * ntz] -= M.rc[ic] * odx * qx;
+                    l.vz[ip + ic] += M.rc[ic] * odz * qz;
+                    l.vz[ip - (ic + 1)] -= M.rc[ic] * odz * qz;
+                }
+            }
+        /* V^T: vx' = vx + dt/rho_x*(Dx+ p + psi_x'), psi_x' = b'*psi_x + a'*Dx+ p on Gx */
+        for (int ix = Lc - 1; ix <= ntx - Lc - 1; ix++)
+            for (int iz = Lc; iz <= ntz - Lc; iz++) {
+                const size_t ip = (size_t)ix * ntz + iz;
+                const T orho = (T)(1 / (0.5 * (M.rho[ip] + M.rho[ip + ntz])));
+                const T r = dt * orho * l.vx[ip];
+                const T R = r + M.axh[ix] * (r + l.ppx[ip]);
+                l.ppx[ip] = M.bxh[ix] * (r + l.ppx[ip]);
+                for (int ic = 0; ic < Lc; ic++) {
+                    l.p[ip + (size_t)(ic + 1) * ntz] += M.rc[ic] * odx * R;
+                    l.p[ip - (size_t)ic * ntz] -= M.rc[ic] * odx * R;
+                }
+            }
+        for (int ix = Lc; ix <= ntx - Lc; ix++)
+            for (int iz = Lc - 1; iz <= ntz - Lc - 1; iz++) {
+                const size_t ip = (size_t)ix * ntz + iz;
+                const T orho = (T)(1 / (0.5 * (M.rho[ip] + M.rho[ip + 1])));
+                const T r = dt * orho * l.vz[ip];
+                const T R = r + M.azh[iz] * (r + l.ppz[ip]);
+                l.ppz[ip] = M.bzh[iz] * (r + l.ppz[ip]);
+                for (int ic = 0; ic < Lc; ic++) {
+                    l.p[ip + (ic + 1)] += M.rc[ic] * odz * R;
+                    l.p[ip - ic] -= M.rc[ic] * odz * R;
+                }
+            }
+        /* R^T and the gradient of this step */
+        for (int r = 0; r < g->nrec; r++) l.p[(size_t)g->r_ix[r] * ntz + g->r_iz[r]] += (T)resid[(size_t)r * nt + k];
+        const T *s = s0 + (size_t)k * ntp;
+        for (size_t ip = 0; ip < ntp; ip++) grad[ip] += dt * s[ip] * l.p[ip];
+    }
+    FN(fld_free)(&l);
+    free(s0);
+    FN(mdl_free)(&M);
 }
 
 #undef FN

@@ -87,6 +87,8 @@ def lib():
             getattr(L, f"orc_rtm_backward_{sfx}").argtypes = [C.POINTER(OrcModel), C.POINTER(OrcGeom), _f32p, tp, tp,
                                                               tp, tp, tp, C.c_void_p]
             getattr(L, f"orc_rtm_post_{sfx}").argtypes = [C.POINTER(OrcModel), tp, tp, tp, tp]
+            getattr(L, f"orc_born_{sfx}").argtypes = [C.POINTER(OrcModel), C.POINTER(OrcGeom), _f32p, _f32p, tp]
+            getattr(L, f"orc_born_adjoint_{sfx}").argtypes = [C.POINTER(OrcModel), C.POINTER(OrcGeom), _f32p, _f32p, tp]
         _lib = L
     return _lib
 
@@ -196,6 +198,24 @@ def forward(model: Model, geom: Geom, rick, hrick=None, strips=False, final=Fals
                                          _ptr(hr), _ptr(seis), _ptr(st), _ptr(fs),
                                          0 if cix is None else len(cix), _ptr(cix), _ptr(cols))
     return dict(seis=seis, strips=st, final=fs, cols=cols)
+
+
+def born(model: Model, geom: Geom, rick, dkappa, dtype=np.float64):
+    """Born data [nrec][nt] for a bulk-modulus perturbation dkappa (ntx, ntz)."""
+    sfx = "f32" if dtype == np.float32 else "f64"
+    out = np.zeros((len(geom.r_ix), model.nt), dtype)
+    getattr(lib(), f"orc_born_{sfx}")(C.byref(model.s), C.byref(geom.s), np.ascontiguousarray(rick, np.float32),
+                                      np.ascontiguousarray(dkappa, np.float32), out)
+    return out
+
+
+def born_adjoint(model: Model, geom: Geom, rick, resid, dtype=np.float64):
+    """Adjoint of born(): gradient (ntx, ntz) of <resid, born(dkappa)> with respect to dkappa."""
+    sfx = "f32" if dtype == np.float32 else "f64"
+    out = np.zeros((model.ntx, model.ntz), dtype)
+    getattr(lib(), f"orc_born_adjoint_{sfx}")(C.byref(model.s), C.byref(geom.s), np.ascontiguousarray(rick, np.float32),
+                                              np.ascontiguousarray(resid, np.float32), out)
+    return out
 
 
 def kzsep(cols, ntz, nfftz, coef, rec_col, r_iz, dtype=np.float32):

@@ -81,7 +81,12 @@ int orc_strip_len(const orc_model *m);
                               T *img, T *illum_s, T *illum_r);                              \
     /* per-shot normalisation + -vp^2 Laplacian (acoustic_HLVSPRTMC.cpp:663-743) */          \
     void orc_rtm_post_##S(const orc_model *m, const T *img, const T *illum_s,               \
-                          T *img_norm, T *fimage);
+                          T *img_norm, T *fimage);                                          \
+    /* Born modelling in kappa = rho*vp^2 and its exact adjoint (project operators) */      \
+    void orc_born_##S(const orc_model *m, const orc_geom *g, const float *rick,              \
+                      const float *dkappa, T *dseis);                                       \
+    void orc_born_adjoint_##S(const orc_model *m, const orc_geom *g, const float *rick,     \
+                              const float *resid, T *grad);
 
 ORC_DECL(float, f32)
 ORC_DECL(double, f64)

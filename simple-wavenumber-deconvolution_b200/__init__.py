@@ -95,6 +95,10 @@ def lib():
         L.swd_preprocess.argtypes = [vp, C.c_int, C.c_int, C.c_float, vp, vp]
         L.swd_decon_geometry.argtypes = [C.POINTER(DeconParams), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.swd_decon.argtypes = [vp, C.POINTER(DeconParams), vp, vp, vp, vp]
+        L.swd_set_checkpointing.argtypes = [vp, C.c_int, C.c_int]
+        L.swd_checkpoint_bytes.argtypes = [vp, C.c_int, C.POINTER(C.c_size_t)]
+        L.swd_born.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, C.c_size_t]
+        L.swd_born_adjoint.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, C.c_size_t]
         L.swd_profile.argtypes = [vp, C.c_int]
         L.swd_profile_read.argtypes = [vp, vp, vp]
         L.swd_launch_count.argtypes = [vp]
@@ -121,6 +125,15 @@ def _ptr(a):
     if hasattr(a, "data_ptr"):
         return C.c_void_p(a.data_ptr())
     return C.c_void_p(a.ctypes.data)
+
+
+def _nbytes(a) -> int:
+    """Size in bytes of a numpy array or torch tensor (0 for None)."""
+    if a is None:
+        return 0
+    if hasattr(a, "data_ptr"):
+        return a.numel() * a.element_size()
+    return a.nbytes
 
 
 def _f32(a):
@@ -258,13 +271,15 @@ class Engine:
         """Time every kernel launch of every `every`-th step with CUDA events (0 = off)."""
         self._ck(lib().swd_profile(self._h, every))
 
+    PROFILE_NAMES = ["fwd_v", "fwd_p", "bwd_1", "bwd_2", "fwd_step", "bwd_step", "fwd_pass_step", "bwd_pass_step",
+                     "adj_v", "adj_p", "adj_pass_step"]
+
     def profile_read(self):
-        """{kernel: (summed ms, timed launches)} for forward-v, forward-p, backward-1, backward-2."""
-        ms = np.zeros(8, np.float64)
-        n = np.zeros(8, np.int64)
+        """{kernel: (summed ms, timed launches)} for every profiling id of include/swd.h."""
+        ms = np.zeros(len(self.PROFILE_NAMES), np.float64)
+        n = np.zeros(len(self.PROFILE_NAMES), np.int64)
         self._ck(lib().swd_profile_read(self._h, _ptr(ms), _ptr(n)))
-        names = ["fwd_v", "fwd_p", "bwd_1", "bwd_2", "fwd_step", "bwd_step", "fwd_pass_step", "bwd_pass_step"]
-        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(names)}
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.PROFILE_NAMES)}
 
     def launch_count(self) -> int:
         return int(lib().swd_launch_count(self._h))
@@ -334,6 +349,34 @@ class Engine:
         rp = (C.c_void_p * n)(*[_ptr(r).value for r in rk])
         dp = (C.c_void_p * n)(*[_ptr(d).value for d in dd])
         self._ck(lib().swd_rtm_batch(self._h, n, arr, rp, dp, flags))
+
+    # Born modelling and its adjoint -----------------------------------------------------
+    def set_checkpointing(self, every: int, prec: int = STRIP_BF16):
+        """every = 0: store the background p-update sums of all steps (FP32); every > 0:
+        checkpoint the background state every `every` steps at `prec` and recompute."""
+        self._ck(lib().swd_set_checkpointing(self._h, every, prec))
+
+    def checkpoint_bytes(self, nt: int) -> int:
+        b = C.c_size_t(0)
+        self._ck(lib().swd_checkpoint_bytes(self._h, nt, C.byref(b)))
+        return b.value
+
+    def born(self, shot: ShotSpec, rick, dkappa, out=None, ckpt=None):
+        """Born data (r_n, nt) of the bulk-modulus perturbation dkappa (ntx, ntz).  `ckpt`
+        (device memory of checkpoint_bytes(nt) bytes) receives the background checkpoints."""
+        sh, keep = self._shot(shot)
+        d = np.zeros((sh.r_n, sh.nt), np.float32) if out is None else out
+        rk, dk = _f32(rick), _f32(dkappa)
+        self._ck(lib().swd_born(self._h, C.byref(sh), _ptr(rk), _ptr(dk), _ptr(d), _ptr(ckpt), _nbytes(ckpt)))
+        return d
+
+    def born_adjoint(self, shot: ShotSpec, rick, resid, out=None, ckpt=None):
+        """Exact adjoint of born(): (ntx, ntz) float64 gradient of <resid, born(dkappa)>."""
+        sh, keep = self._shot(shot)
+        g = np.zeros((self.ntx, self.ntz), np.float64) if out is None else out
+        rk, r = _f32(rick), _f32(resid)
+        self._ck(lib().swd_born_adjoint(self._h, C.byref(sh), _ptr(rk), _ptr(r), _ptr(g), _ptr(ckpt), _nbytes(ckpt)))
+        return g
 
     # helpers ---------------------------------------------------------------------------
     def hilbert(self, rick):

@@ -147,6 +147,21 @@ def c3(nshots=96):
     return w
 
 
+def c4(nshots=16):
+    """Differentiable LSRTM gradient: 801x401 at 5 m, nt=4000, dt=0.4 ms, 16 surface shots
+    (25 Hz) recorded by 321 receivers in a central well; reflectivity dv/v = sparse spikes
+    N(0, 0.05) at 1% density on the interior; background = the 15-point box-smoothed
+    random-field model."""
+    rng = np.random.default_rng(SEED0 + 4)
+    nx, nz = 801, 401
+    v = random_field(nx, nz, rng)
+    w = Workload("c4_801x401_nt4000_16shots", nx, nz, 5.0, 5.0, 4000, 4.0e-4, 30, 4, 25.0, v, box_smooth(v, 15),
+                 sx=[int(round(10 + s * (nx - 20) / max(1, nshots - 1))) for s in range(nshots)], sz=0,
+                 rec_x=np.full(321, 400, np.int32), rec_z=np.arange(40, 361, dtype=np.int32))
+    w.extra["reflectivity"] = (0.05 * rng.standard_normal((nx, nz)) * (rng.random((nx, nz)) < 0.01)).astype(np.float32)
+    return w
+
+
 def small(nx=100, nz=60, nt=400, pml=10, Lc=4, dx=5.0, dz=5.0, dt=5.0e-4, f0=25.0, seed=7):
     """Small two-well parity case; nx + 2*pmlc is a multiple of 16 for nx=100, pml=10, Lc=4
     (the reference CUDA build indexes past the grid otherwise)."""
@@ -157,4 +172,4 @@ def small(nx=100, nz=60, nt=400, pml=10, Lc=4, dx=5.0, dz=5.0, dt=5.0e-4, f0=25.
                     box_smooth(v, 5), sx=[nx // 4], sz=0)
 
 
-CONFIGS = {"c1": c1, "c2": c2, "c3": c3}
+CONFIGS = {"c1": c1, "c2": c2, "c3": c3, "c4": c4}

@@ -202,7 +202,7 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const flo
 template <int LC>
 __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const float *__restrict__ vp,
                                           const float *__restrict__ rho, Wave w, float odx, float odz, int x, int z0,
-                                          float4 &pn, bool upd[4])
+                                          float4 &pn, bool upd[4], float4 *ssum = nullptr)
 {
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
@@ -253,9 +253,77 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const flo
     }
     const float4 v = ldg4(vp + ip), r = ldg4(rho + ip);
 #pragma unroll
-    for (int k = 0; k < 4; k++)
-        if (upd[k])
-            el(pn, k) = g.dt * elc(r, k) * elc(v, k) * elc(v, k) * (elc(dvx, k) + elc(phx, k) + elc(dvz, k) + elc(phz, k)) + elc(pn, k);
+    for (int k = 0; k < 4; k++) {
+        const float sk = elc(dvx, k) + elc(phx, k) + elc(dvz, k) + elc(phz, k);
+        if (ssum) el(*ssum, k) = upd[k] ? sk : 0.f;
+        if (upd[k]) el(pn, k) = g.dt * elc(r, k) * elc(v, k) * elc(v, k) * sk + elc(pn, k);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// State checkpoints of one wavefield (p, vx, vz and the four CPML memories), taken before
+// step it whenever it % every == 0, snapshot it / every.  Layout: data
+// [snapshot][array 7][ntx*ldz] elements of prec (0 f32, 1 f16, 2 bf16); 16-bit snapshots
+// carry one scale per (snapshot, array, 128 x 8 block) in scale[snapshot][array][nblocks]
+// and store value / scale (x 32768 for f16).
+// ------------------------------------------------------------------------------------
+struct Ckpt {
+    void *buf;
+    float *scale;
+    int every;           // 0: no checkpoints
+    int prec;
+    int nblocks;
+    long long fstride;   // ntx * ldz
+};
+
+__device__ __forceinline__ float *wave_array(const Wave &w, int i)
+{
+    return i == 0 ? w.p : i == 1 ? w.vx : i == 2 ? w.vz : i == 3 ? w.ppx : i == 4 ? w.ppz : i == 5 ? w.pvx : w.pvz;
+}
+
+// Called by every thread of a (32, 8) block with its four cells (valid when `in`).
+__device__ __forceinline__ void ckpt_save(const Ckpt &ck, const Wave &w, int snap, bool in, size_t ip)
+{
+    const int slot = blockIdx.y * gridDim.x + blockIdx.x;
+    if (ck.prec == 0) {
+        if (!in) return;
+#pragma unroll 1
+        for (int i = 0; i < 7; i++)
+            st4((float *)ck.buf + ((size_t)snap * 7 + i) * ck.fstride + ip, ld4(wave_array(w, i) + ip));
+        return;
+    }
+    __shared__ float smax[7];
+    if (threadIdx.x < 7 && threadIdx.y == 0) smax[threadIdx.x] = 0.f;
+    __syncthreads();
+    float4 v[7];
+#pragma unroll
+    for (int i = 0; i < 7; i++) {
+        v[i] = in ? ld4(wave_array(w, i) + ip) : make_float4(0.f, 0.f, 0.f, 0.f);
+        float m = fmaxf(fmaxf(fabsf(v[i].x), fabsf(v[i].y)), fmaxf(fabsf(v[i].z), fabsf(v[i].w)));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0 && m > 0.f) atomicMax((int *)&smax[i], __float_as_int(m));
+    }
+    __syncthreads();
+    if (threadIdx.x < 7 && threadIdx.y == 0)
+        ck.scale[((size_t)snap * 7 + threadIdx.x) * ck.nblocks + slot] = smax[threadIdx.x];
+    if (!in) return;
+#pragma unroll
+    for (int i = 0; i < 7; i++) {
+        const float mx = smax[i];
+        const size_t o = ((size_t)snap * 7 + i) * ck.fstride + ip;
+        if (ck.prec == 1) {
+            __half h[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) h[k] = __float2half_rn(mx > 0.f ? elc(v[i], k) / mx * 32768.f : 0.f);
+            *reinterpret_cast<uint2 *>((__half *)ck.buf + o) = *reinterpret_cast<uint2 *>(h);
+        } else {
+            __nv_bfloat16 h[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) h[k] = __float2bfloat16_rn(mx > 0.f ? elc(v[i], k) / mx : 0.f);
+            *reinterpret_cast<uint2 *>((__nv_bfloat16 *)ck.buf + o) = *reinterpret_cast<uint2 *>(h);
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -277,6 +345,17 @@ struct FwdArgs {
     Strips strips;       // save (forward pass of RTM), buf == nullptr to skip
     const int *colmap;   // well column -> kz column slot, or nullptr
     float2 *colbuf;      // [ncol][nt][ldz] (p, twin p)
+    // Born modelling / adjoint support, read by the BORN instantiation of k_fwd_p only:
+    //   s0_out  receives field 0's p-update sum S0 = dvx+phi_x+dvz+phi_z of step it at
+    //           s0_out[(it % s0_mod) * s0_stride + cell] (0 where p is not updated); nullable
+    //   dkappa  bulk-modulus perturbation; with NW == 2 field 1 gets the secondary source
+    //           dt * dkappa * S0 after its own update and the receivers record field 1
+    // seis == nullptr records nothing.
+    float *s0_out;
+    long long s0_stride;
+    int s0_mod;
+    const float *dkappa;
+    Ckpt ck;             // field-0 state checkpoints, taken by the CKPT instantiation of k_fwd_v
 };
 
 // block (32, 8): lane -> four rows, warp -> one column; a block covers 128 rows x 8 columns
@@ -286,17 +365,22 @@ __device__ __forceinline__ void cell4(int &x, int &z0)
     x = blockIdx.y * 8 + threadIdx.y;
 }
 
-template <int LC, int NW>
+template <int LC, int NW, bool CKPT>
 __global__ void __launch_bounds__(256) k_fwd_v(FwdArgs a)
 {
     int x, z0;
     cell4(x, z0);
+    if constexpr (CKPT) {
+        const int it = *a.itp + a.itoff;
+        if (it % a.ck.every == 0)
+            ckpt_save(a.ck, a.w[0], it / a.ck.every, x < a.g.ntx && z0 < a.g.ntz, (size_t)x * a.g.ldz + z0);
+    }
     if (x >= a.g.ntx || z0 >= a.g.ntz) return;
 #pragma unroll
     for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.rho, a.w[k], a.g.odx, a.g.odz, x, z0);
 }
 
-template <int LC, int NW>
+template <int LC, int NW, bool BORN>
 __global__ void __launch_bounds__(256) k_fwd_p(FwdArgs a)
 {
     const int it = *a.itp + a.itoff;
@@ -309,11 +393,22 @@ __global__ void __launch_bounds__(256) k_fwd_p(FwdArgs a)
     for (int k = 0; k < NW; k++) pn[k] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (in) {
         const size_t ip = (size_t)x * g.ldz + z0;
+        float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int w = 0; w < NW; w++) {
             bool upd[4];
-            p_update4<LC>(g, a.c, a.vp, a.rho, a.w[w], g.odx, g.odz, x, z0, pn[w], upd);
+            p_update4<LC>(g, a.c, a.vp, a.rho, a.w[w], g.odx, g.odz, x, z0, pn[w], upd,
+                          (BORN && w == 0) ? &s0 : nullptr);
             bool any = upd[0] || upd[1] || upd[2] || upd[3];
+            if constexpr (BORN) {
+                if (w == 0 && a.s0_out) st4(a.s0_out + (size_t)(it % a.s0_mod) * a.s0_stride + ip, s0);
+                if (w == 1 && a.dkappa) {
+                    const float4 dk = ldg4(a.dkappa + ip);
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (upd[k]) el(pn[w], k) += g.dt * elc(dk, k) * elc(s0, k);
+                }
+            }
             if (x == a.sx) {
 #pragma unroll
                 for (int k = 0; k < 4; k++)
@@ -321,13 +416,14 @@ __global__ void __launch_bounds__(256) k_fwd_p(FwdArgs a)
             }
             if (any) st4(a.w[w].p + ip, pn[w]);
         }
-        const int wc = __ldg(a.wells.wcol + x);
+        const int wc = a.seis ? __ldg(a.wells.wcol + x) : -1;
         if (wc >= 0) {
             const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * g.ldz + z0));
             const int t[4] = {tr.x, tr.y, tr.z, tr.w};
+            constexpr int rf = (BORN && NW == 2) ? 1 : 0;   // Born data: the scattered field
 #pragma unroll
             for (int k = 0; k < 4; k++)
-                if (t[k] >= 0 && z0 + k < g.ntz) a.seis[(size_t)t[k] * a.nt + it] = elc(pn[0], k);
+                if (t[k] >= 0 && z0 + k < g.ntz) a.seis[(size_t)t[k] * a.nt + it] = elc(pn[rf], k);
             if (a.colmap) {
                 float2 *cb = a.colbuf + ((size_t)wc * a.nt + it) * g.ldz + z0;
 #pragma unroll

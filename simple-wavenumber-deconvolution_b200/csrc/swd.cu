@@ -17,6 +17,7 @@
 #include "../../include/swd.h"
 #include "prop.cuh"
 #include "prop_fused.cuh"
+#include "born.cuh"
 #include "fft.cuh"
 #include "decon.cuh"
 
@@ -57,13 +58,17 @@ struct swd_ctx {
     DevBuf I, S, R, stack, reduce;
     bool have_R = false, have_shot = false;
     DevBuf stage_in, stage_out;
+    // Born modelling and its adjoint: perturbation, gradient, background p-update sums,
+    // context-owned checkpoints, adjoint scratch (Qx, Qz, Rx, Rz), adjoint source, aliases
+    DevBuf dk, gk, s0, ckpt, adj[4], rbuf, alias;
+    int ckpt_every = 50, ckpt_prec = SWD_STRIP_BF16;
     // chunked CUDA-graph execution of the time loops
     DevBuf ctrl, wav;
     struct StepGraph {
         cudaGraphExec_t exec = nullptr, probe = nullptr;
         std::vector<char> key;
         std::vector<cudaEvent_t> ev;   // probe events: (start, end) per kernel of the probed step
-    } gfwd, gbwd;
+    } gfwd, gbwd, gseg, gadj;
     int use_graphs = 1;
     // instrumentation
     int prof_every = 0;
@@ -76,8 +81,10 @@ struct swd_ctx {
     swd_ctx()
     {
         DevBuf *all[] = {&vp, &rho, &dpdt, &wcol, &wmap, &seis, &seis2, &rdata, &colbuf, &kzcoef, &tw,
-                         &strips, &strip_scale, &I, &S, &R, &stack, &reduce, &stage_in, &stage_out, &ctrl, &wav};
+                         &strips, &strip_scale, &I, &S, &R, &stack, &reduce, &stage_in, &stage_out, &ctrl, &wav,
+                         &dk, &gk, &s0, &ckpt, &rbuf, &alias};
         for (DevBuf *b : all) bufs.push_back(b);
+        for (auto &b : adj) bufs.push_back(&b);
         for (auto &b : cpml) bufs.push_back(&b);
         for (auto &w : wave)
             for (auto &b : w) bufs.push_back(&b);
@@ -538,18 +545,32 @@ __global__ void k_pml_z(float *v, int ntx, int ntz, int pml)
 // ------------------------------------------------------------------------------------
 // launch dispatch on the stencil half-length
 // ------------------------------------------------------------------------------------
+// the checkpointing and Born variants are separate instantiations, so the plain modelling
+// and RTM kernels keep their register budget
 template <int LC>
 static void launch_fwd_v(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s)
 {
-    if (nw == 2) k_fwd_v<LC, 2><<<grid, dim3(32, 8), 0, s>>>(a);
-    else k_fwd_v<LC, 1><<<grid, dim3(32, 8), 0, s>>>(a);
+    const bool ck = a.ck.every > 0;
+    if (nw == 2) {
+        if (ck) k_fwd_v<LC, 2, true><<<grid, dim3(32, 8), 0, s>>>(a);
+        else k_fwd_v<LC, 2, false><<<grid, dim3(32, 8), 0, s>>>(a);
+    } else {
+        if (ck) k_fwd_v<LC, 1, true><<<grid, dim3(32, 8), 0, s>>>(a);
+        else k_fwd_v<LC, 1, false><<<grid, dim3(32, 8), 0, s>>>(a);
+    }
 }
 
 template <int LC>
 static void launch_fwd_p(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s)
 {
-    if (nw == 2) k_fwd_p<LC, 2><<<grid, dim3(32, 8), 0, s>>>(a);
-    else k_fwd_p<LC, 1><<<grid, dim3(32, 8), 0, s>>>(a);
+    const bool born = a.s0_out || a.dkappa;
+    if (nw == 2) {
+        if (born) k_fwd_p<LC, 2, true><<<grid, dim3(32, 8), 0, s>>>(a);
+        else k_fwd_p<LC, 2, false><<<grid, dim3(32, 8), 0, s>>>(a);
+    } else {
+        if (born) k_fwd_p<LC, 1, true><<<grid, dim3(32, 8), 0, s>>>(a);
+        else k_fwd_p<LC, 1, false><<<grid, dim3(32, 8), 0, s>>>(a);
+    }
 }
 
 template <int LC>
@@ -625,6 +646,11 @@ struct FwdJob {
     bool twin = false, save_strips = false;
     float *seis_dev = nullptr;
     float2 *colbuf = nullptr;
+    // Born: field 1 is the scattered field (no wavelet, secondary source dt*dkappa*S0)
+    const float *dkappa = nullptr;
+    float *s0 = nullptr;     // background p-update sums, slot it % s0_mod
+    int s0_mod = 1;
+    Ckpt ck{};               // background checkpoints (ck.every == 0: none)
 };
 
 // device copies of the shot's wavelet(s): wav[0..nt) = rick, wav[nt..2nt) = Hilbert twin
@@ -632,7 +658,8 @@ static int upload_wavelets(swd_ctx *ctx, const FwdJob &J, int nt)
 {
     CKR(ensure(ctx, ctx->wav, sizeof(float) * 2 * (size_t)ctx->grid.nt_max));
     CK(cudaMemcpyAsync(F(ctx->wav), J.rick.data(), sizeof(float) * nt, cudaMemcpyHostToDevice, ctx->stream));
-    if (J.twin) CK(cudaMemcpyAsync(F(ctx->wav) + nt, J.hrick.data(), sizeof(float) * nt, cudaMemcpyHostToDevice, ctx->stream));
+    if (J.twin && J.dkappa) CK(cudaMemsetAsync(F(ctx->wav) + nt, 0, sizeof(float) * nt, ctx->stream));
+    else if (J.twin) CK(cudaMemcpyAsync(F(ctx->wav) + nt, J.hrick.data(), sizeof(float) * nt, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));   // the host vectors may go away after this
     return SWD_OK;
 }
@@ -661,12 +688,13 @@ static void graph_free(swd_ctx::StepGraph &G)
 }
 
 template <class Launch>
-static int capture_chunk(swd_ctx *ctx, cudaGraphExec_t *out, int dir, int *counter, Launch launch, cudaEvent_t *ev)
+static int capture_chunk(swd_ctx *ctx, cudaGraphExec_t *out, int dir, int *counter, Launch launch, cudaEvent_t *ev,
+                         int klen)
 {
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < GRAPH_K; k++) launch(k, k == GRAPH_K / 2 ? ev : nullptr);
-    k_advance<<<1, 1, 0, ctx->stream>>>(counter, dir * GRAPH_K);
+    for (int k = 0; k < klen; k++) launch(k, k == klen / 2 ? ev : nullptr);
+    k_advance<<<1, 1, 0, ctx->stream>>>(counter, dir * klen);
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
     if (e != cudaSuccess) return fail(ctx, SWD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
     e = cudaGraphInstantiate(out, graph, 0);
@@ -677,37 +705,40 @@ static int capture_chunk(swd_ctx *ctx, cudaGraphExec_t *out, int dir, int *count
 
 // Launch(k, ev): enqueue step k (itoff = dir*k) on ctx->stream; when ev != nullptr record
 // ev[2j] / ev[2j+1] around its j-th kernel.  nk kernels per step with profiling ids kid[].
+// Chunks hold klen steps (the key of the captured graph includes it).
 template <class Launch>
 static int run_steps(swd_ctx *ctx, swd_ctx::StepGraph &G, const void *key, size_t keylen, int start, int dir,
-                     int nsteps, int nk, const int *kid, Launch launch)
+                     int nsteps, int nk, const int *kid, Launch launch, int klen = GRAPH_K, int pass_id = -1)
 {
     CKR(ensure(ctx, ctx->ctrl, 64));
     int *counter = I32(ctx->ctrl);
     CK(cudaMemcpyAsync(counter, &start, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     // the legacy default stream (handle 0) cannot be captured: launch directly there
-    const int nchunks = (ctx->use_graphs && ctx->stream != nullptr) ? nsteps / GRAPH_K : 0;
-    const int rem = nsteps - nchunks * GRAPH_K;
+    const int nchunks = (ctx->use_graphs && ctx->stream != nullptr) ? nsteps / klen : 0;
+    const int rem = nsteps - nchunks * klen;
     const bool prof = ctx->prof_every > 0;
     if (nchunks > 0) {
-        const bool same = G.exec && G.key.size() == keylen && memcmp(G.key.data(), key, keylen) == 0;
+        std::vector<char> k2((const char *)key, (const char *)key + keylen);
+        k2.insert(k2.end(), (const char *)&klen, (const char *)&klen + sizeof klen);
+        const bool same = G.exec && G.key == k2;
         if (!same) {
             graph_free(G);
-            G.key.assign((const char *)key, (const char *)key + keylen);
-            CKR(capture_chunk(ctx, &G.exec, dir, counter, launch, nullptr));
+            G.key = k2;
+            CKR(capture_chunk(ctx, &G.exec, dir, counter, launch, nullptr, klen));
         }
         if (prof && !G.probe) {
             G.ev.resize(2 * nk);
             for (auto &e : G.ev) CK(cudaEventCreate(&e));
-            CKR(capture_chunk(ctx, &G.probe, dir, counter, launch, G.ev.data()));
+            CKR(capture_chunk(ctx, &G.probe, dir, counter, launch, G.ev.data(), klen));
         }
     }
     const int pc = prof && nchunks > 0 ? nchunks / 2 : -1;   // the chunk that carries the probe events
     {
         // whole-pass time per step (profiling ids 6 forward, 7 backward)
-        ProfScope pass(ctx, dir > 0 ? 6 : 7, prof, nsteps);
+        ProfScope pass(ctx, pass_id >= 0 ? pass_id : (dir > 0 ? 6 : 7), prof, nsteps);
         for (int c = 0; c < nchunks; c++) {
             CK(cudaGraphLaunch(c == pc ? G.probe : G.exec, ctx->stream));
-            ctx->launches += (long long)nk * GRAPH_K;
+            ctx->launches += (long long)nk * klen;
         }
         for (int k = 0; k < rem; k++) {
             launch(k, nullptr);
@@ -733,7 +764,8 @@ static int run_forward_fused(swd_ctx *ctx, FwdJob &J, ShotPlan &P);
 
 static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
 {
-    if (fused(ctx)) return run_forward_fused(ctx, J, P);
+    // Born fields, S0 output and checkpoints exist on the plain kernels only
+    if (fused(ctx) && !J.dkappa && !J.s0 && !J.ck.every) return run_forward_fused(ctx, J, P);
     const swd_shot *s = J.shot;
     const int nt = s->nt;
     CKR(zero_wave(ctx, 0));
@@ -754,6 +786,11 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     a.seis = J.seis_dev;
     a.colmap = J.colbuf ? I32(ctx->wcol) : nullptr;
     a.colbuf = J.colbuf;
+    a.s0_out = J.s0;
+    a.s0_stride = (long long)ctx->ntx * ctx->ldz;
+    a.s0_mod = J.s0_mod;
+    a.dkappa = J.dkappa;
+    a.ck = J.ck;
     const dim3 grid = grid_blocks(ctx);
     if (J.save_strips) {
         const int slen = strip_len(ctx);
@@ -985,6 +1022,8 @@ int swd_destroy(swd_ctx *ctx)
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     graph_free(ctx->gfwd);
     graph_free(ctx->gbwd);
+    graph_free(ctx->gseg);
+    graph_free(ctx->gadj);
     if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SWD_OK;
@@ -1546,3 +1585,5 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
 }
 
 }  // extern "C"
+
+#include "born_host.inl"

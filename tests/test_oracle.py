@@ -168,3 +168,39 @@ def test_oracle_matches_reference_cuda_build(orc):
     assert rel_l2(fim, g["fimage_pp"]) < 1e-4
     mig = orc.edge_zero(fim.astype(np.float32), Lc)
     assert rel_l2(mig, g["migration_pp"]) < 1e-4
+
+
+def test_oracle_born_adjoint_dot_product(orc):
+    """The oracle's adjoint (written as scatters of each forward loop body, in reverse) is the
+    exact transpose of its Born operator: <r, L dk> = <L^T r, dk> to FP64 rounding."""
+    M, G, rick = _small_model(orc, nt=300)
+    rng = np.random.default_rng(1)
+    for trial in range(2):
+        dk = (rng.standard_normal((M.ntx, M.ntz)) * 1e7).astype(np.float32)
+        d = orc.born(M, G, rick, dk)
+        r = rng.standard_normal(d.shape).astype(np.float32)
+        g = orc.born_adjoint(M, G, rick, r)
+        lhs = float(np.dot(r.astype(np.float64).ravel(), d.ravel()))
+        rhs = float(np.dot(g.ravel(), dk.astype(np.float64).ravel()))
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+def test_oracle_born_is_the_linearised_forward(orc):
+    """Born data of dkappa = 2 kappa dv/v equal the central difference of the nonlinear
+    forward modelling in vp; the mismatch falls as eps^2."""
+    M, G, rick = _small_model(orc, nt=300)
+    rng = np.random.default_rng(2)
+    kap = M.rho.astype(np.float64) * M.vp.astype(np.float64) ** 2
+    dv_rel = np.zeros_like(kap)
+    p = M.pmlc
+    dv_rel[p:-p, p:-p] = rng.standard_normal((M.ntx - 2 * p, M.ntz - 2 * p))
+    d_born = orc.born(M, G, rick, (2 * kap * dv_rel).astype(np.float32))
+    errs = []
+    for eps in (1e-2, 1e-3):
+        outs = []
+        for s in (1, -1):
+            vp2 = (M.vp.astype(np.float64) * (1 + s * eps * dv_rel)).astype(np.float32)
+            M2 = orc.Model(vp2, M.rho, M.cp, M.rc, M.pmlc, M.Lc, M.nt, M.dx, M.dz, M.dt)
+            outs.append(orc.forward(M2, G, rick, dtype=np.float64)["seis"])
+        errs.append(rel_l2((outs[0] - outs[1]) / (2 * eps), d_born))
+    assert errs[1] < 1e-4 and errs[0] / errs[1] > 30
