@@ -19,6 +19,11 @@ step, no collective in the data path): value = all ranks' shots / the slowest ra
 reference has no CPU propagator, so this is the project's OpenMP restatement of the
 reference's stencil, imaging and preprocessing loops (oracle/, kind "port"), run for a
 bounded number of time steps per sample and extrapolated to the full record.
+
+--workload lsrtm measures the differentiable LSRTM gradient instead (801 x 401, nt = 4000,
+16 shots, reflectivity spikes at 1 % density): a step is one evaluation of
+J(r) = 1/2 sum_s ||L_s r - d_s||^2 and its gradient through the torch autograd path (Born
+forward with background checkpoints every 50 steps, checkpointed exact adjoint per shot).
 """
 from __future__ import annotations
 
@@ -314,6 +319,164 @@ def cpu_baseline(w, samples=1, nsteps=24):
                       f"extrapolated linearly; {best:.2f} s measured"}
 
 
+LSRTM_WORKLOAD = ("c4 LSRTM gradient: 801x401 @5 m, nt=4000, dt=0.4 ms, 16 shots, 321 well receivers, "
+                  "reflectivity spikes N(0,0.05) at 1% density, pml 30, 8th order")
+
+
+def adjoint_bytes(kernel, w, cp, r_n):
+    """Minimum bytes of one launch of each adjoint kernel (each array touched once)."""
+    N = w.ntx * w.ntz
+    nzc = lambda a: int(np.count_nonzero(a))
+    x_v = nzc(cp["a_x_half"]) * w.ntz + nzc(cp["a_z_half"]) * w.ntx
+    x_p = nzc(cp["a_x"]) * w.ntz + nzc(cp["a_z"]) * w.ntx
+    if kernel == "adj_v":   # Qx, Qz in; v^x, v^z r/w; rho; Rx, Rz out; psi^ r/w in the frame
+        return 36 * N + 8 * x_v
+    if kernel == "adj_p":   # Rx, Rz in; p^ r/w; S0; FP64 grad r/w; vp, rho; Qx, Qz out; phi^ in the frame; traces
+        return 52 * N + 8 * x_p + 4 * r_n
+    raise KeyError(kernel)
+
+
+def run_lsrtm(args, rank, world, dist):
+    import torch
+    swd = load_pkg()
+    from swd_b200 import configs, lsrtm
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    w = configs.c4()
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt, device=dev)
+    pmlc = w.pmlc
+    vmig = swd.pad_model(w.vp_mig, pmlc)
+    rho = np.full_like(vmig, 1000.0)
+    E.setup_default(vmig, rho)
+    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
+    rick = swd.ricker_wave(w.nt, w.f0, w.dt)
+    rx, rz = w.receivers_padded()
+    ops = [lsrtm.BornOperator(E, swd.ShotSpec(sx + pmlc, pmlc, rx, rz, w.nt), rick, vmig, rho, device=f"cuda:{dev}")
+           for sx in w.sx]
+    nshots, r_n = len(ops), len(rx)
+    prec = {"f32": swd.STRIP_F32, "f16": swd.STRIP_F16, "bf16": swd.STRIP_BF16, "i16": swd.STRIP_I16}[args.ckpt_prec]
+    r_true = torch.tensor(w.extra["reflectivity"], device="cuda")
+    with torch.no_grad():
+        data = [lsrtm.born(r_true, op) for op in ops]       # observed data: Born data of the true reflectivity
+    r0 = 0.5 * r_true                                        # current model: residual = data of 0.5 r_true
+    h_data = [d.cpu().pin_memory() for d in data]
+    h_grad = torch.empty((w.nx, w.nz), dtype=torch.float32).pin_memory()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def gradient(dd):
+        r = r0.clone().requires_grad_(True)
+        lsrtm.lsrtm_objective(r, ops, dd).backward()
+        return r.grad
+
+    def timed(K, W, e2e=False, profile=False):
+        for _ in range(W):
+            gradient(data)
+        if profile:
+            E.profile(8)
+            E.profile_read()
+        n0 = E.launch_count()
+        torch.cuda.synchronize()
+        total = 0.0
+        for _ in range(K):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            if e2e:
+                dd = [hd.to("cuda", non_blocking=True) for hd in h_data]
+                h_grad.copy_(gradient(dd), non_blocking=True)
+            else:
+                g = gradient(data)
+            b.record()
+            b.synchronize()
+            total += a.elapsed_time(b)
+        launches = E.launch_count() - n0
+        prof = E.profile_read() if profile else None
+        E.profile(0)
+        return total, launches, prof
+
+    # accuracy of the checkpointed gradient against FP32 full storage (outside the timing)
+    E.set_checkpointing(0)
+    g_full = gradient(data).double()
+    t0 = time.perf_counter()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    gradient(data)
+    b.record()
+    b.synchronize()
+    t_full = a.elapsed_time(b)
+    E.set_checkpointing(50, prec)
+    g_ck = gradient(data).double()
+    err = float((g_ck - g_full).norm() / g_full.norm())
+    ck_bytes = E.checkpoint_bytes(w.nt)
+    full_bytes = w.nt * w.ntx * ((w.ntz + 31) // 32 * 32) * 4
+    with ClockSampler(dev) as clk:
+        t_val, launches, prof = timed(args.steps, args.warmup, profile=True)
+        t_e2e, _, _ = timed(args.steps, 1, e2e=True)
+    value = nshots * args.steps / (t_val / 1e3)
+    e2e = nshots * args.steps / (t_e2e / 1e3)
+    per_launch = {k: ms / n for k, (ms, n) in prof.items() if n}
+    live = {}
+    if all(k in per_launch for k in ("adj_pass_step", "adj_v", "adj_p")):
+        t, a1, a2 = per_launch["adj_pass_step"], per_launch["adj_v"], per_launch["adj_p"]
+        live = {"adj_v": t * a1 / (a1 + a2), "adj_p": t * a2 / (a1 + a2)}
+    dom = max(live, key=live.get)
+    peak, src = peaks()
+    ab = adjoint_bytes(dom, w, cp, r_n)
+    achieved = ab / (live[dom] * 1e-3) / 1e9
+    N, Ni = w.ntx * w.ntz, w.nx * w.nz
+    cpu = lsrtm_cpu_baseline(w, nsteps=args.cpu_steps // 3)
+    return {
+        "metric": "LSRTM gradient shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": f"f32 (FP64 gradient accumulation, {args.ckpt_prec} checkpoints)",
+        "data": "synthetic (seeded random-field model, Born data of seeded reflectivity spikes)",
+        "config": {"workload": LSRTM_WORKLOAD, "parallelism": f"replicas x{world}", "shots_per_step": nshots,
+                   "checkpoints": f"every 50 steps, {args.ckpt_prec}", "l2": "flushed (256 MiB write) before every timed step"},
+        "gcell_updates_per_s": value * w.nt * 2 * N / 1e9,
+        "executed_gcell_updates_per_s": value * w.nt * 4 * N / 1e9,
+        "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(nshots * r_n * w.nt * 4),
+                "d2h_bytes_per_step": int(w.nx * w.nz * 4)},
+        "gradient_vs_fp32_full_storage": {"rel_l2": err, "full_storage_ms_per_step": t_full,
+                                          "checkpoint_bytes_per_shot": ck_bytes, "full_storage_bytes_per_shot": full_bytes},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": src, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": ab,
+                     "avg_launch_us": live[dom] * 1e3, "kernels_us": {k: v * 1e3 for k, v in live.items()},
+                     "step_us": {k: per_launch[k] * 1e3 for k in ("fwd_pass_step", "adj_pass_step") if k in per_launch}},
+        "gpu_launches": launches,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "wall_s": time.perf_counter() - t0,
+    }
+
+
+def lsrtm_cpu_baseline(w, nsteps=100):
+    """The oracle's Born modelling + adjoint (FP32, OpenMP stencils, serial adjoint scatters)
+    for one shot over nsteps steps on the full grid, extrapolated to nt."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as orc
+    swd = sys.modules.get("swd_b200") or load_pkg()
+    pmlc = w.pmlc
+    vp = swd.pad_model(w.vp_mig, pmlc)
+    rho = np.full_like(vp, 1000.0)
+    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
+    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt)
+    rx, rz = w.receivers_padded()
+    G = orc.Geom(w.sx[0] + pmlc, pmlc, rx, rz)
+    rick = swd.ricker_wave(nsteps, w.f0, w.dt)
+    dk = np.zeros_like(vp)
+    dk[pmlc:-pmlc, pmlc:-pmlc] = 2 * 1000.0 * w.vp_mig ** 2 * w.extra["reflectivity"]
+    t = time.perf_counter()
+    d = orc.born(M, G, rick, dk.astype(np.float32), np.float32)
+    orc.born_adjoint(M, G, rick, d.astype(np.float32), np.float32)
+    dt = time.perf_counter() - t
+    per_shot = dt * w.nt / nsteps
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": 1.0 / per_shot, "unit": "shots/s", "cores": cores, "kind": "port",
+            "sample": f"Born + adjoint of 1 shot, {nsteps} of {w.nt} steps on the full grid, extrapolated; "
+                      f"{dt:.2f} s measured"}
+
+
 def run_profile_kernels(args):
     """One RTM shot on the benchmark grid with a short record (--nt) and seeded random data,
     no warm-up shots and no data generation: the command the ncu captures run, so that few
@@ -370,6 +533,9 @@ def main():
     ap.add_argument("--profile-kernels", action="store_true", help="one short shot for ncu captures")
     ap.add_argument("--nt", type=int, default=30, help="record length of --profile-kernels")
     ap.add_argument("--path", type=int, default=None, help="kernel path: 0 plain (two launches per step), 1 fused")
+    ap.add_argument("--workload", choices=["rtm", "lsrtm"], default="rtm")
+    ap.add_argument("--ckpt-prec", choices=["f32", "f16", "bf16", "i16"], default="bf16",
+                    help="checkpoint precision of --workload lsrtm")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -389,7 +555,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = td
-    out = run_ours(args, rank, world, dist)
+    out = run_lsrtm(args, rank, world, dist) if args.workload == "lsrtm" else run_ours(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

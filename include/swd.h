@@ -39,6 +39,7 @@ extern "C" {
 #define SWD_STRIP_F32 0
 #define SWD_STRIP_F16 1      /* IEEE half with a per-(step, tile) scale */
 #define SWD_STRIP_BF16 2     /* bfloat16 with a per-(step, tile) scale */
+#define SWD_STRIP_I16 3      /* int16 fixed point of value / per-(step, tile) max |value| */
 
 /* flags of swd_rtm_shot */
 #define SWD_RTM_PREPROCESS 1u     /* apply rms = -int int d dt dt to the data first (reference default) */
@@ -142,7 +143,7 @@ int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *
  * The adjoint needs S0 at every step in reverse order.  swd_set_checkpointing selects how:
  *   every == 0: the background pass stores S0 for all nt steps (FP32, nt*ntx*ntz floats);
  *   every  > 0: the background state (p, vx, vz and 4 CPML arrays) is stored every `every`
- *               steps at `prec` (SWD_STRIP_F32 / F16 / BF16, 16-bit with one scale per
+ *               steps at `prec` (SWD_STRIP_F32 / F16 / BF16 / I16, 16-bit with one scale per
  *               snapshot, array and 128x8-cell block) and each segment is recomputed
  *               before its adjoint steps.  Default: every = 50, BF16.
  * swd_born optionally leaves the background checkpoints of its pass in `ckpt` (device

@@ -25,7 +25,7 @@ PKG_DIR = Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "libswd.so"
 
 SWD_OK, SWD_ERR_ARG, SWD_ERR_CUDA, SWD_ERR_ALLOC, SWD_ERR_STATE, SWD_ERR_DEVICE = range(6)
-STRIP_F32, STRIP_F16, STRIP_BF16 = 0, 1, 2
+STRIP_F32, STRIP_F16, STRIP_BF16, STRIP_I16 = 0, 1, 2, 3
 PATH_PLAIN, PATH_FUSED = 0, 1
 RTM_PREPROCESS, RTM_ILLUM_RCV, RTM_NO_STACK = 1, 2, 4
 

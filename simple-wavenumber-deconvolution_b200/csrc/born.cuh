@@ -237,16 +237,9 @@ __global__ void __launch_bounds__(256) k_ckpt_restore(Ckpt ck, Wave w, int snap,
             v = ld4((const float *)ck.buf + o);
         } else {
             const float mx = ck.scale[((size_t)snap * 7 + i) * ck.nblocks + slot];
-            const uint2 raw = *reinterpret_cast<const uint2 *>((const char *)ck.buf + 2 * o);
-            if (ck.prec == 1) {
-                const __half *h = reinterpret_cast<const __half *>(&raw);
-#pragma unroll
-                for (int k = 0; k < 4; k++) el(v, k) = __half2float(h[k]) / 32768.f * mx;
-            } else {
-                const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&raw);
-#pragma unroll
-                for (int k = 0; k < 4; k++) el(v, k) = __bfloat162float(h[k]) * mx;
-            }
+            const ushort4 h = *reinterpret_cast<const ushort4 *>((const unsigned short *)ck.buf + o);
+            v = make_float4(dec16(h.x, mx, ck.prec), dec16(h.y, mx, ck.prec), dec16(h.z, mx, ck.prec),
+                            dec16(h.w, mx, ck.prec));
         }
         st4(wave_array(w, i) + ip, v);
     }

@@ -34,7 +34,7 @@ static size_t ckpt_layout(swd_ctx *c, int nt, void *base, Ckpt *ck)
         ck->buf = base;
         ck->scale = scales ? (float *)((char *)base + data) : nullptr;
         ck->every = c->ckpt_every;
-        ck->prec = c->ckpt_prec == SWD_STRIP_F32 ? 0 : c->ckpt_prec == SWD_STRIP_F16 ? 1 : 2;
+        ck->prec = c->ckpt_prec;   // SWD_STRIP_* values are the device codes
         ck->nblocks = (int)nblocks;
         ck->fstride = (long long)fstride;
     }
@@ -112,8 +112,7 @@ int swd_set_checkpointing(swd_ctx *ctx, int every, int prec)
 {
     if (!ctx) return SWD_ERR_ARG;
     if (every < 0) return fail(ctx, SWD_ERR_ARG, "checkpoint interval %d < 0", every);
-    if (prec != SWD_STRIP_F32 && prec != SWD_STRIP_F16 && prec != SWD_STRIP_BF16)
-        return fail(ctx, SWD_ERR_ARG, "unknown checkpoint precision %d", prec);
+    if (prec < SWD_STRIP_F32 || prec > SWD_STRIP_I16) return fail(ctx, SWD_ERR_ARG, "unknown checkpoint precision %d", prec);
     ctx->ckpt_every = every;
     ctx->ckpt_prec = prec;
     return SWD_OK;

@@ -56,6 +56,24 @@ struct Strips {
 
 __device__ __forceinline__ size_t cidx(int x, int z, int ldz) { return (size_t)x * ldz + z; }
 
+// 16-bit codes of a value v relative to its block's max |v| (mx >= |v|): prec 1 IEEE half of
+// v/mx * 32768, prec 2 bfloat16 of v/mx, prec 3 int16 fixed point round(v/mx * 32767).
+// Normalising first keeps |v|/mx <= 1 even for denormal mx.
+__device__ __forceinline__ unsigned short enc16(float v, float mx, int prec)
+{
+    const float q = mx > 0.f ? v / mx : 0.f;
+    if (prec == 1) return __half_as_ushort(__float2half_rn(q * 32768.f));
+    if (prec == 2) return __bfloat16_as_ushort(__float2bfloat16_rn(q));
+    return (unsigned short)(short)__float2int_rn(q * 32767.f);
+}
+
+__device__ __forceinline__ float dec16(unsigned short u, float mx, int prec)
+{
+    if (prec == 1) return (__half2float(__ushort_as_half(u)) / 32768.f) * mx;
+    if (prec == 2) return __bfloat162float(__ushort_as_bfloat16(u)) * mx;
+    return ((float)(short)u / 32767.f) * mx;
+}
+
 // Index of cell (x, z) in the per-step strip vector, or -1.
 __device__ __forceinline__ int strip_index(int x, int z, int ntx, int ntz, int pmlc, int Lc)
 {
@@ -263,9 +281,9 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const flo
 // ------------------------------------------------------------------------------------
 // State checkpoints of one wavefield (p, vx, vz and the four CPML memories), taken before
 // step it whenever it % every == 0, snapshot it / every.  Layout: data
-// [snapshot][array 7][ntx*ldz] elements of prec (0 f32, 1 f16, 2 bf16); 16-bit snapshots
-// carry one scale per (snapshot, array, 128 x 8 block) in scale[snapshot][array][nblocks]
-// and store value / scale (x 32768 for f16).
+// [snapshot][array 7][ntx*ldz] elements of prec (0 f32, or a 16-bit code of enc16); 16-bit
+// snapshots carry one scale (the max |value|) per (snapshot, array, 128 x 8 block) in
+// scale[snapshot][array][nblocks].
 // ------------------------------------------------------------------------------------
 struct Ckpt {
     void *buf;
@@ -312,17 +330,10 @@ __device__ __forceinline__ void ckpt_save(const Ckpt &ck, const Wave &w, int sna
     for (int i = 0; i < 7; i++) {
         const float mx = smax[i];
         const size_t o = ((size_t)snap * 7 + i) * ck.fstride + ip;
-        if (ck.prec == 1) {
-            __half h[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) h[k] = __float2half_rn(mx > 0.f ? elc(v[i], k) / mx * 32768.f : 0.f);
-            *reinterpret_cast<uint2 *>((__half *)ck.buf + o) = *reinterpret_cast<uint2 *>(h);
-        } else {
-            __nv_bfloat16 h[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) h[k] = __float2bfloat16_rn(mx > 0.f ? elc(v[i], k) / mx : 0.f);
-            *reinterpret_cast<uint2 *>((__nv_bfloat16 *)ck.buf + o) = *reinterpret_cast<uint2 *>(h);
-        }
+        ushort4 h;
+        h.x = enc16(v[i].x, mx, ck.prec); h.y = enc16(v[i].y, mx, ck.prec);
+        h.z = enc16(v[i].z, mx, ck.prec); h.w = enc16(v[i].w, mx, ck.prec);
+        *reinterpret_cast<ushort4 *>((unsigned short *)ck.buf + o) = h;
     }
 }
 
@@ -456,13 +467,9 @@ __global__ void __launch_bounds__(256) k_fwd_p(FwdArgs a)
             const int slot = blockIdx.y * gridDim.x + blockIdx.x;
             if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)it * a.strips.nscale + slot] = mx;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                if (si[k] < 0) continue;
-                // normalise first (|p|/mx <= 1 even for denormal mx), then scale to the type
-                const float q = mx > 0.f ? elc(pn[0], k) / mx : 0.f;
-                if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = __float2half_rn(q * 32768.f);
-                else ((__nv_bfloat16 *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = __float2bfloat16_rn(q);
-            }
+            for (int k = 0; k < 4; k++)
+                if (si[k] >= 0)
+                    ((unsigned short *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = enc16(elc(pn[0], k), mx, a.strips.prec);
         }
     }
 }
@@ -497,8 +504,7 @@ __device__ __forceinline__ float strip_restore(const Strips &st, int it, int si,
     const int slot = (x / 8) * nz_blocks + (z / 128);
     const float mx = st.scale[(size_t)it * st.nscale + slot];
     if (mx == 0.f) return 0.f;
-    if (st.prec == 1) return ((float)((const __half *)st.buf)[(size_t)it * st.slen + si] / 32768.f) * mx;
-    return (float)((const __nv_bfloat16 *)st.buf)[(size_t)it * st.slen + si] * mx;
+    return dec16(((const unsigned short *)st.buf)[(size_t)it * st.slen + si], mx, st.prec);
 }
 
 __device__ __forceinline__ bool interior(int x, int z, const Geo &g)

@@ -288,9 +288,7 @@ __global__ void __launch_bounds__(256) k_fwd_step(FStepArgs a)
             if (x >= g.ntx || z >= g.ntz) continue;
             const int si = strip_index(x, z, g.ntx, g.ntz, g.pmlc, LC);
             if (si < 0) continue;
-            const float q = mx > 0.f ? sPn[0][cc * TZ + rr] / mx : 0.f;
-            if (a.strips.prec == 1) ((__half *)a.strips.buf)[(size_t)it * a.strips.slen + si] = __float2half_rn(q * 32768.f);
-            else ((__nv_bfloat16 *)a.strips.buf)[(size_t)it * a.strips.slen + si] = __float2bfloat16_rn(q);
+            ((unsigned short *)a.strips.buf)[(size_t)it * a.strips.slen + si] = enc16(sPn[0][cc * TZ + rr], mx, a.strips.prec);
         }
     }
 }
@@ -305,8 +303,7 @@ __device__ __forceinline__ float strip_value(const Strips &st, int it, int si, i
     const int slot = (x / TX) * nscale_z + (z / TZ);
     const float mx = st.scale[(size_t)it * st.nscale + slot];
     if (mx == 0.f) return 0.f;
-    if (st.prec == 1) return ((float)((const __half *)st.buf)[(size_t)it * st.slen + si] / 32768.f) * mx;
-    return (float)((const __nv_bfloat16 *)st.buf)[(size_t)it * st.slen + si] * mx;
+    return dec16(((const unsigned short *)st.buf)[(size_t)it * st.slen + si], mx, st.prec);
 }
 
 template <int LC, int TX, int TZ>

@@ -1140,8 +1140,7 @@ int swd_set_kernel_path(swd_ctx *ctx, int path)
 int swd_set_strip_precision(swd_ctx *ctx, int prec)
 {
     if (!ctx) return SWD_ERR_ARG;
-    if (prec != SWD_STRIP_F32 && prec != SWD_STRIP_F16 && prec != SWD_STRIP_BF16)
-        return fail(ctx, SWD_ERR_ARG, "unknown strip precision %d", prec);
+    if (prec < SWD_STRIP_F32 || prec > SWD_STRIP_I16) return fail(ctx, SWD_ERR_ARG, "unknown strip precision %d", prec);
     ctx->strip_prec = prec;
     return SWD_OK;
 }

@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-4
 TOL_DOT = 1e-5
-CKPT_TOL = {"f16": 2e-3, "bf16": 2e-2}   # gradient rel-L2 vs FP32 full storage
+CKPT_TOL = {"f16": 2e-3, "bf16": 2e-2, "i16": 1e-3}   # gradient rel-L2 vs FP32 full storage
 
 
 def _dk(case, seed=3, density=None):
@@ -95,13 +95,13 @@ def test_fp32_checkpoints_equal_full_storage(bcase, swd, every):
     c.E.set_checkpointing(50, swd.STRIP_BF16)
 
 
-@pytest.mark.parametrize("prec", ["f16", "bf16"])
+@pytest.mark.parametrize("prec", ["f16", "bf16", "i16"])
 def test_16bit_checkpoints_error(bcase, swd, prec):
     c = bcase
     resid = np.random.default_rng(4).standard_normal((len(c.rix), c.nt)).astype(np.float32)
     c.E.set_checkpointing(0)
     full = c.E.born_adjoint(c.shot, c.rick, resid)
-    c.E.set_checkpointing(50, swd.STRIP_F16 if prec == "f16" else swd.STRIP_BF16)
+    c.E.set_checkpointing(50, {"f16": swd.STRIP_F16, "bf16": swd.STRIP_BF16, "i16": swd.STRIP_I16}[prec])
     ck = c.E.born_adjoint(c.shot, c.rick, resid)
     err = rel_l2(ck, full)
     print(f"{prec} checkpoint gradient rel-L2 vs FP32 full storage: {err:.3e}")
