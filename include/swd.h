@@ -128,9 +128,27 @@ int swd_rtm_raw(swd_ctx *ctx, double *image, double *illum_src, double *illum_rc
 int swd_stack_get(swd_ctx *ctx, int edge_zero, float *migration);
 int swd_stack_reset(swd_ctx *ctx);
 
-/* ---- batched RTM: many shots of uneven nt and aperture, stacked --------------------- */
+/* ---- batched RTM: many shots of uneven nt and aperture, stacked ---------------------
+ * Replaces the per-rank shot loop of AVSPRTM (acoustic_HLVSPRTMC.cpp:546-748) on one GPU.
+ * Shots are sorted by nt and run B at a time in batched launches (one launch per half step
+ * for the whole batch, time loops as CUDA graphs); each shot's -vp^2-filtered image is added
+ * to the FP64 stack exactly as swd_rtm_shot adds it.  B = swd_set_option(SWD_OPT_BATCH), or
+ * chosen by timing probes of B = 1, 2, 4, 8 on the first call (SWD_OPT_BATCH_TUNED reads the
+ * choice).  flags: SWD_RTM_PREPROCESS only (the batch always stacks).  The context's current
+ * strip precision applies. */
 int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *const *ricks,
                   const float *const *data, unsigned flags);
+
+/* ---- engine options (no reference counterpart) ---------------------------------------
+ * SWD_OPT_GRAPHS  1 (default): time loops replay captured CUDA graphs of 64 steps;
+ *                 0: every kernel is launched from the host (the plain engine)
+ * SWD_OPT_BATCH   shots per batched launch in swd_rtm_batch, 0 (default) = autotune
+ * SWD_OPT_BATCH_TUNED  (read only) the autotuner's batch size, 0 before the first batch */
+#define SWD_OPT_GRAPHS 1
+#define SWD_OPT_BATCH 2
+#define SWD_OPT_BATCH_TUNED 3
+int swd_set_option(swd_ctx *ctx, int option, int value);
+int swd_get_option(swd_ctx *ctx, int option, int *value);
 
 /* ---- Born modelling and its exact adjoint (LSRTM / velocity gradients) --------------
  * No reference counterpart: the reference only migrates.  The Born operator linearises the

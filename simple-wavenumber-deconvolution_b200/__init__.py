@@ -28,6 +28,7 @@ SWD_OK, SWD_ERR_ARG, SWD_ERR_CUDA, SWD_ERR_ALLOC, SWD_ERR_STATE, SWD_ERR_DEVICE 
 STRIP_F32, STRIP_F16, STRIP_BF16, STRIP_I16 = 0, 1, 2, 3
 PATH_PLAIN, PATH_FUSED = 0, 1
 RTM_PREPROCESS, RTM_ILLUM_RCV, RTM_NO_STACK = 1, 2, 4
+OPT_GRAPHS, OPT_BATCH, OPT_BATCH_TUNED = 1, 2, 3
 
 
 class SwdError(RuntimeError):
@@ -95,6 +96,8 @@ def lib():
         L.swd_preprocess.argtypes = [vp, C.c_int, C.c_int, C.c_float, vp, vp]
         L.swd_decon_geometry.argtypes = [C.POINTER(DeconParams), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.swd_decon.argtypes = [vp, C.POINTER(DeconParams), vp, vp, vp, vp]
+        L.swd_set_option.argtypes = [vp, C.c_int, C.c_int]
+        L.swd_get_option.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.swd_set_checkpointing.argtypes = [vp, C.c_int, C.c_int]
         L.swd_checkpoint_bytes.argtypes = [vp, C.c_int, C.POINTER(C.c_size_t)]
         L.swd_born.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, C.c_size_t]
@@ -257,6 +260,16 @@ class Engine:
     def set_kernel_path(self, path: int):
         """PATH_PLAIN: one cell per thread, two launches per step; PATH_FUSED: one launch per step."""
         self._ck(lib().swd_set_kernel_path(self._h, path))
+
+    def set_option(self, option: int, value: int):
+        """OPT_GRAPHS (1: time loops as CUDA graphs, 0: host launches), OPT_BATCH (shots per
+        batched launch of rtm_batch, 0 = autotune)."""
+        self._ck(lib().swd_set_option(self._h, option, int(value)))
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int(0)
+        self._ck(lib().swd_get_option(self._h, option, C.byref(v)))
+        return v.value
 
     def set_stream(self, stream_handle: int):
         self._ck(lib().swd_set_stream(self._h, C.c_void_p(stream_handle)))

@@ -54,6 +54,40 @@ struct Strips {
     int slen, prec, nscale;
 };
 
+// Batched launches (blockIdx.z = shot of the batch): per-shot scalars and offsets.  Every
+// per-shot grid array of a batch is one allocation with a fixed per-shot stride (bstride
+// elements, guard bands included); traces, wavelets and well maps are concatenated.
+struct ShotDesc {
+    int sx, sz, nt;
+    int tshift;          // nt - (longest nt of the batch): backward time index offset
+    int wav_off;         // first wavelet sample of the shot
+    int wmap_off;        // first well row of the shot in the batch's wmap
+    long long seis_off;  // first trace sample of the shot in seis / rdata
+};
+
+struct Batch {
+    const ShotDesc *desc;   // nullptr: not batched
+    long long bstride;      // elements between consecutive shots' grid arrays
+    long long strip_bytes;  // bytes between consecutive shots' strip stores
+    long long scale_stride; // floats between consecutive shots' strip scales
+    int nshots;
+};
+
+__device__ __forceinline__ Wave shift_wave(Wave w, long long o)
+{
+    w.p += o; w.vx += o; w.vz += o; w.ppx += o; w.ppz += o; w.pvx += o; w.pvz += o;
+    return w;
+}
+
+__device__ __forceinline__ Strips shift_strips(Strips s, const Batch &bt, int b)
+{
+    if (s.buf) {
+        s.buf = (char *)s.buf + (size_t)b * bt.strip_bytes;
+        if (s.scale) s.scale += (size_t)b * bt.scale_stride;
+    }
+    return s;
+}
+
 __device__ __forceinline__ size_t cidx(int x, int z, int ldz) { return (size_t)x * ldz + z; }
 
 // 16-bit codes of a value v relative to its block's max |v| (mx >= |v|): prec 1 IEEE half of
@@ -367,7 +401,24 @@ struct FwdArgs {
     int s0_mod;
     const float *dkappa;
     Ckpt ck;             // field-0 state checkpoints, taken by the CKPT instantiation of k_fwd_v
+    Batch bt;            // the BATCH instantiations (NW == 1): shot = blockIdx.z
 };
+
+// The shot's view of a batched forward launch; false when the shot's record has ended.
+__device__ __forceinline__ bool fwd_view(FwdArgs &a, int it)
+{
+    const int b = blockIdx.z;
+    const ShotDesc d = a.bt.desc[b];
+    if (it >= d.nt) return false;
+    a.w[0] = shift_wave(a.w[0], (long long)b * a.bt.bstride);
+    a.sx = d.sx; a.sz = d.sz; a.nt = d.nt;
+    a.wav0 += d.wav_off;
+    a.wells.wcol += (size_t)b * a.g.ntx;
+    a.wells.wmap += (size_t)d.wmap_off * a.g.ldz;
+    if (a.seis) a.seis += d.seis_off;
+    a.strips = shift_strips(a.strips, a.bt, b);
+    return true;
+}
 
 // block (32, 8): lane -> four rows, warp -> one column; a block covers 128 rows x 8 columns
 __device__ __forceinline__ void cell4(int &x, int &z0)
@@ -376,9 +427,13 @@ __device__ __forceinline__ void cell4(int &x, int &z0)
     x = blockIdx.y * 8 + threadIdx.y;
 }
 
-template <int LC, int NW, bool CKPT>
-__global__ void __launch_bounds__(256) k_fwd_v(FwdArgs a)
+template <int LC, int NW, bool CKPT, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
 {
+    FwdArgs a = a0;
+    if constexpr (BATCH) {
+        if (!fwd_view(a, *a.itp + a.itoff)) return;
+    }
     int x, z0;
     cell4(x, z0);
     if constexpr (CKPT) {
@@ -391,10 +446,14 @@ __global__ void __launch_bounds__(256) k_fwd_v(FwdArgs a)
     for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.rho, a.w[k], a.g.odx, a.g.odz, x, z0);
 }
 
-template <int LC, int NW, bool BORN>
-__global__ void __launch_bounds__(256) k_fwd_p(FwdArgs a)
+template <int LC, int NW, bool BORN, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_fwd_p(const FwdArgs a0)
 {
+    FwdArgs a = a0;
     const int it = *a.itp + a.itoff;
+    if constexpr (BATCH) {
+        if (!fwd_view(a, it)) return;
+    }
     int x, z0;
     cell4(x, z0);
     const Geo &g = a.g;
@@ -495,7 +554,33 @@ struct BwdArgs {
     Wells wells;
     const float *rdata;  // [r_n][nt] preprocessed data injected at the receivers
     double *I, *S, *R;   // FP64 imaging accumulators (R nullable)
+    Batch bt;            // the BATCH instantiations: shot = blockIdx.z
 };
+
+// The shot's view of a batched backward launch: its own time index (every shot of a batch
+// starts the backward pass at its own nt - 2, so shorter records finish early); false once
+// the shot is done.
+__device__ __forceinline__ bool bwd_view(BwdArgs &a, int &it)
+{
+    const int b = blockIdx.z;
+    const ShotDesc d = a.bt.desc[b];
+    it += d.tshift;
+    if (it < 0) return false;
+    const long long o = (long long)b * a.bt.bstride;
+    a.s = shift_wave(a.s, o);
+    a.r = shift_wave(a.r, o);
+    a.dpdt += o;
+    a.I += o;
+    a.S += o;
+    if (a.R) a.R += o;
+    a.sx = d.sx; a.sz = d.sz; a.nt = d.nt;
+    a.wavsub += d.wav_off;
+    a.wells.wcol += (size_t)b * a.g.ntx;
+    a.wells.wmap += (size_t)d.wmap_off * a.g.ldz;
+    a.rdata += d.seis_off;
+    a.strips = shift_strips(a.strips, a.bt, b);
+    return true;
+}
 
 // one restored strip value; the scale slot is the forward block that saved the cell
 __device__ __forceinline__ float strip_restore(const Strips &st, int it, int si, int x, int z, int nz_blocks)
@@ -512,10 +597,14 @@ __device__ __forceinline__ bool interior(int x, int z, const Geo &g)
     return z >= g.pmlc && z <= g.ntz - g.pmlc - 1 && x >= g.pmlc && x <= g.ntx - g.pmlc - 1;
 }
 
-template <int LC>
-__global__ void __launch_bounds__(256) k_bwd_1(BwdArgs a)
+template <int LC, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
 {
-    const int it = *a.itp + a.itoff;
+    BwdArgs a = a0;
+    int it = *a.itp + a.itoff;
+    if constexpr (BATCH) {
+        if (!bwd_view(a, it)) return;
+    }
     int x, z0;
     cell4(x, z0);
     const Geo &g = a.g;
@@ -569,10 +658,14 @@ __global__ void __launch_bounds__(256) k_bwd_1(BwdArgs a)
     v_update4<LC, true>(g, a.c, a.rho, a.r, -g.odx, -g.odz, x, z0);
 }
 
-template <int LC>
-__global__ void __launch_bounds__(256) k_bwd_2(BwdArgs a)
+template <int LC, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_bwd_2(const BwdArgs a0)
 {
-    const int it = *a.itp + a.itoff;
+    BwdArgs a = a0;
+    int it = *a.itp + a.itoff;
+    if constexpr (BATCH) {
+        if (!bwd_view(a, it)) return;
+    }
     int x, z0;
     cell4(x, z0);
     const Geo &g = a.g;

@@ -62,13 +62,19 @@ struct swd_ctx {
     // context-owned checkpoints, adjoint scratch (Qx, Qz, Rx, Rz), adjoint source, aliases
     DevBuf dk, gk, s0, ckpt, adj[4], rbuf, alias;
     int ckpt_every = 50, ckpt_prec = SWD_STRIP_BF16;
+    // batched RTM (swd_rtm_batch): every per-shot grid array is one allocation of per-shot slices
+    struct BatchBufs {
+        DevBuf w[2][7], dpdt, I, S, strips, scale, rdata, wcol, wmap, desc, wav, reduce;
+    } bat;
+    int batch_opt = 0;      // shots per batched launch; 0 = autotune on first use
+    int batch_tuned = 0;    // the autotuner's choice (0 = not tuned yet)
     // chunked CUDA-graph execution of the time loops
     DevBuf ctrl, wav;
     struct StepGraph {
         cudaGraphExec_t exec = nullptr, probe = nullptr;
         std::vector<char> key;
         std::vector<cudaEvent_t> ev;   // probe events: (start, end) per kernel of the probed step
-    } gfwd, gbwd, gseg, gadj;
+    } gfwd, gbwd, gseg, gadj, gbf, gbb;
     int use_graphs = 1;
     // instrumentation
     int prof_every = 0;
@@ -85,6 +91,11 @@ struct swd_ctx {
                          &dk, &gk, &s0, &ckpt, &rbuf, &alias};
         for (DevBuf *b : all) bufs.push_back(b);
         for (auto &b : adj) bufs.push_back(&b);
+        DevBuf *ball[] = {&bat.dpdt, &bat.I, &bat.S, &bat.strips, &bat.scale, &bat.rdata, &bat.wcol, &bat.wmap,
+                          &bat.desc, &bat.wav, &bat.reduce};
+        for (DevBuf *b : ball) bufs.push_back(b);
+        for (auto &w : bat.w)
+            for (auto &b : w) bufs.push_back(&b);
         for (auto &b : cpml) bufs.push_back(&b);
         for (auto &w : wave)
             for (auto &b : w) bufs.push_back(&b);
@@ -336,7 +347,8 @@ struct ShotPlan {
     std::vector<int> well_x;
 };
 
-static int plan_shot(swd_ctx *ctx, const swd_shot *s, ShotPlan &P)
+// validation and the host-side well maps of one shot (no device work)
+static int plan_shot_host(swd_ctx *ctx, const swd_shot *s, ShotPlan &P)
 {
     if (!s) return fail(ctx, SWD_ERR_ARG, "shot is NULL");
     if (s->nt < 2 || s->nt > ctx->grid.nt_max) return fail(ctx, SWD_ERR_ARG, "shot nt=%d outside [2, nt_max=%d]", s->nt, ctx->grid.nt_max);
@@ -365,6 +377,12 @@ static int plan_shot(swd_ctx *ctx, const swd_shot *s, ShotPlan &P)
         int keep = P.wmap[(size_t)P.wcol[rx[a.first]] * ctx->ldz + rz[a.first]];
         a.second = keep;
     }
+    return SWD_OK;
+}
+
+static int plan_shot(swd_ctx *ctx, const swd_shot *s, ShotPlan &P)
+{
+    CKR(plan_shot_host(ctx, s, P));
     CKR(ensure(ctx, ctx->wcol, sizeof(int) * ctx->ntx));
     CKR(ensure(ctx, ctx->wmap, sizeof(int) * P.wmap.size()));
     CK(cudaMemcpyAsync(ctx->wcol.p, P.wcol.data(), sizeof(int) * ctx->ntx, cudaMemcpyHostToDevice, ctx->stream));
@@ -1024,6 +1042,8 @@ int swd_destroy(swd_ctx *ctx)
     graph_free(ctx->gbwd);
     graph_free(ctx->gseg);
     graph_free(ctx->gadj);
+    graph_free(ctx->gbf);
+    graph_free(ctx->gbb);
     if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SWD_OK;
@@ -1390,15 +1410,6 @@ int swd_stack_reset(swd_ctx *ctx)
     return SWD_OK;
 }
 
-int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *const *ricks, const float *const *data,
-                  unsigned flags)
-{
-    if (!ctx || nshots < 0 || (nshots > 0 && (!shots || !ricks || !data))) return fail(ctx, SWD_ERR_ARG, "bad batch");
-    for (int i = 0; i < nshots; i++)
-        CKR(swd_rtm_shot(ctx, &shots[i], ricks[i], data[i], flags, nullptr, nullptr, nullptr, nullptr));
-    return SWD_OK;
-}
-
 int swd_hilbert(swd_ctx *ctx, int nt, const float *rick, float *hrick)
 {
     if (!ctx || !rick || !hrick || nt < 2) return fail(ctx, SWD_ERR_ARG, "bad hilbert arguments");
@@ -1586,3 +1597,4 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
 }  // extern "C"
 
 #include "born_host.inl"
+#include "batch_host.inl"
