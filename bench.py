@@ -20,6 +20,12 @@ reference has no CPU propagator, so this is the project's OpenMP restatement of 
 reference's stencil, imaging and preprocessing loops (oracle/, kind "port"), run for a
 bounded number of time steps per sample and extrapolated to the full record.
 
+--workload batch measures batched multi-shot RTM on the 96-shot walkaway survey (1201 x 601,
+nt ~ U[3000, 6000], 200-600 receivers, 20-35 Hz): a step is the whole survey migrated and
+stacked by swd_rtm_batch (autotuned batch size, CUDA graphs, FP32 strips); the same survey
+through the plain engine (one shot per launch sequence, host launches, FP32 strips) is timed
+beside it, and the stacks are compared (also for int16 strips, which halve the strip memory).
+
 --workload lsrtm measures the differentiable LSRTM gradient instead (801 x 401, nt = 4000,
 16 shots, reflectivity spikes at 1 % density): a step is one evaluation of
 J(r) = 1/2 sum_s ||L_s r - d_s||^2 and its gradient through the torch autograd path (Born
@@ -450,6 +456,98 @@ def run_lsrtm(args, rank, world, dist):
     }
 
 
+BATCH_WORKLOAD = ("c3 batched RTM: 96 walkaway-VSP shots, 1201x601 @5 m, nt ~ U[3000,6000], dt=0.4 ms, "
+                  "200-600 well receivers, 20-35 Hz, pml 30, 8th order")
+
+
+def run_batch(args, rank, world, dist):
+    import torch
+    swd = load_pkg()
+    from swd_b200 import configs
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    w = configs.c3()
+    shots_cfg = w.extra["shots"]
+    ntmax = max(s["nt"] for s in shots_cfg)
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, ntmax, device=dev)
+    pmlc = w.pmlc
+    vtrue, vmig = swd.pad_model(w.vp, pmlc), swd.pad_model(w.vp_mig, pmlc)
+    rho = np.full_like(vmig, 1000.0)
+    E.setup_default(vtrue, rho)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    E.set_stream(stream.cuda_stream)
+    shots, ricks, data = [], [], []
+    for s in shots_cfg:
+        sh = swd.ShotSpec(s["sx"] + pmlc, s["sz"] + pmlc, s["rec_x"] + pmlc, s["rec_z"] + pmlc, s["nt"])
+        rk = swd.ricker_wave(s["nt"], s["f0"], w.dt)
+        shots.append(sh)
+        ricks.append(rk)
+        data.append(E.forward(sh, rk))           # observed data in the true model
+    E.set_model(vmig, rho)
+    cells = sum(s["nt"] * (2 * w.ntx * w.ntz + w.nx * w.nz) for s in shots_cfg)
+
+    def timed(fn, K, W):
+        for _ in range(W):
+            fn()
+        torch.cuda.synchronize()
+        n0 = E.launch_count()
+        total = 0.0
+        for _ in range(K):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total, E.launch_count() - n0
+
+    def plain():
+        E.stack_reset()
+        for sh, rk, d in zip(shots, ricks, data):
+            E.rtm_shot(sh, rk, d, want=())
+
+    def batched():
+        E.stack_reset()
+        E.rtm_batch(shots, ricks, data)
+
+    # plain engine: one shot per launch sequence, host launches, FP32 strips
+    E.set_option(swd.OPT_GRAPHS, 0)
+    E.set_strip_precision(swd.STRIP_F32)
+    t_plain, _ = timed(plain, args.steps, 1)
+    st_plain = E.stack(edge_zero=False).astype(np.float64)
+    # batched engine: autotuned batch, CUDA graphs, FP32 strips
+    E.set_option(swd.OPT_GRAPHS, 1)
+    E.set_option(swd.OPT_BATCH, 0)
+    with ClockSampler(dev) as clk:
+        t_bat, launches = timed(batched, args.steps, args.warmup)
+    st_bat = E.stack(edge_zero=False).astype(np.float64)
+    # int16 strips: the image error of halving the strip memory
+    E.set_strip_precision(swd.STRIP_I16)
+    batched()
+    st_bat16 = E.stack(edge_zero=False).astype(np.float64)
+    E.set_strip_precision(swd.STRIP_F32)
+    nshot = len(shots) * args.steps
+    value = nshot / (t_bat / 1e3)
+    plain_v = nshot / (t_plain / 1e3)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return {
+        "metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_bat / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (FP64 imaging)", "data": "synthetic (seeded random-field model)",
+        "config": {"workload": BATCH_WORKLOAD, "parallelism": f"replicas x{world}", "shots_per_step": len(shots),
+                   "batch_size": E.get_option(swd.OPT_BATCH_TUNED), "l2": "inputs of one batch exceed L2"},
+        "gcell_updates_per_s": cells * args.steps / (t_bat / 1e3) / 1e9,
+        "plain_engine": {"value": plain_v, "unit": "shots/s", "ms_per_step": t_plain / args.steps,
+                         "what": "swd_rtm_shot per shot, host launches (no graphs), FP32 strips"},
+        "speedup_vs_plain": value / plain_v,
+        "stack_rel_l2_vs_plain": rel(st_bat, st_plain),
+        "stack_rel_l2_int16_strips_vs_plain": rel(st_bat16, st_plain),
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+
+
 def lsrtm_cpu_baseline(w, nsteps=100):
     """The oracle's Born modelling + adjoint (FP32, OpenMP stencils, serial adjoint scatters)
     for one shot over nsteps steps on the full grid, extrapolated to nt."""
@@ -533,7 +631,7 @@ def main():
     ap.add_argument("--profile-kernels", action="store_true", help="one short shot for ncu captures")
     ap.add_argument("--nt", type=int, default=30, help="record length of --profile-kernels")
     ap.add_argument("--path", type=int, default=None, help="kernel path: 0 plain (two launches per step), 1 fused")
-    ap.add_argument("--workload", choices=["rtm", "lsrtm"], default="rtm")
+    ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch"], default="rtm")
     ap.add_argument("--ckpt-prec", choices=["f32", "f16", "bf16", "i16"], default="bf16",
                     help="checkpoint precision of --workload lsrtm")
     args = ap.parse_args()
@@ -555,7 +653,8 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = td
-    out = run_lsrtm(args, rank, world, dist) if args.workload == "lsrtm" else run_ours(args, rank, world, dist)
+    runner = {"rtm": run_ours, "lsrtm": run_lsrtm, "batch": run_batch}[args.workload]
+    out = runner(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:
