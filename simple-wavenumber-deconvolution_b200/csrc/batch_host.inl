@@ -148,6 +148,7 @@ static int rtm_batch_run(swd_ctx *ctx, const swd_shot *shots, const float *const
     a.c = make_cpml(ctx);
     a.vp = F(ctx->vp);
     a.rho = F(ctx->rho);
+    a.m = make_mat(ctx);
     a.w[0] = a.w[1] = batch_wave(ctx, 0);
     a.itp = I32(ctx->ctrl);
     a.wav0 = a.wav1 = F(ctx->bat.wav);
@@ -173,6 +174,7 @@ static int rtm_batch_run(swd_ctx *ctx, const swd_shot *shots, const float *const
     bb.c = a.c;
     bb.vp = a.vp;
     bb.rho = a.rho;
+    bb.m = a.m;
     bb.s = batch_wave(ctx, 0);
     bb.r = batch_wave(ctx, 1);
     bb.dpdt = F(ctx->bat.dpdt);

@@ -50,6 +50,7 @@ static FwdArgs born_fwd_args(swd_ctx *ctx, const swd_shot *s, bool twin)
     a.c = make_cpml(ctx);
     a.vp = F(ctx->vp);
     a.rho = F(ctx->rho);
+    a.m = make_mat(ctx);
     a.w[0] = make_wave(ctx, 0);
     a.w[1] = twin ? make_wave(ctx, 1) : make_wave(ctx, 0);
     a.sx = s->s_ix;

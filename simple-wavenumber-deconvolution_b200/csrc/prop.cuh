@@ -2,8 +2,8 @@
 //
 // Layout in HBM: every field is x-major with z fastest and a leading dimension ldz that is
 // ntz rounded up to 32, so a warp (32 lanes along z) reads one aligned 128-byte line.
-// Material is read as vp and rho (8 B/cell); dt*rho*vp^2 and the half-node buoyancy
-// 1/(0.5*(rho_i + rho_i+1)) are formed in registers.  CPML memory variables are only
+// Material is read as three precomputed coefficient arrays (struct Mat: dt times the
+// half-node buoyancies and dt*rho*vp^2, formed once per model).  CPML memory variables are only
 // read and written where the profile coefficient a is non-zero (the PML frame).
 //
 // Arithmetic follows the reference kernels term by term (acoustic_HLVSPRTMLc.cu:24-221,
@@ -29,6 +29,14 @@ struct Geo {
 
 struct Cpml {
     const float *ax, *axh, *az, *azh, *bx, *bxh, *bz, *bzh;
+};
+
+// Material coefficients of the updates, formed once per model (k_material) with the same
+// operations and order the per-cell expressions use, so the updates are unchanged bit for
+// bit:  cbx = dt * rcp(0.5*(rho[x] + rho[x+1])),  cbz = dt * rcp(0.5*(rho[z] + rho[z+1])),
+// ck = ((dt*rho)*vp)*vp.  vx += cbx*(d + phi), vz += cbz*(d + phi), p += ck*(sum).
+struct Mat {
+    const float *cbx, *cbz, *ck;
 };
 
 // One wavefield updated in place.
@@ -157,8 +165,8 @@ struct ZWin {
 // velocity half step (reference kernels _vx/_vz, acoustic_HLVSPRTMLc.cu:24-118; receiver
 // variants with the wider guards and -dx/-dz, :623-715)
 template <int LC, bool WIDE>
-__device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const float *__restrict__ rho, Wave w,
-                                          float odx, float odz, int x, int z0)
+__device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
+                                          int x, int z0)
 {
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
@@ -193,13 +201,11 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const flo
                 }
                 st4(w.ppx + ip, po);
             }
-            const float4 r0 = ldg4(rho + ip), r1 = ldg4(rho + ip + ldz);
+            const float4 cb = ldg4(m.cbx + ip);
             float4 v = ld4(w.vx + ip);
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float orho = __frcp_rn(0.5f * (elc(r0, k) + elc(r1, k)));
-                if (gx[k]) el(v, k) = g.dt * orho * (elc(d, k) + elc(phi, k)) + elc(v, k);
-            }
+            for (int k = 0; k < 4; k++)
+                if (gx[k]) el(v, k) = elc(cb, k) * (elc(d, k) + elc(phi, k)) + elc(v, k);
             st4(w.vx + ip, v);
         }
     }
@@ -235,15 +241,11 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const flo
                 }
                 st4(w.ppz + ip, po);
             }
-            const float4 r0 = ldg4(rho + ip);
-            const float r4 = __ldg(rho + ip + 4);
+            const float4 cb = ldg4(m.cbz + ip);
             float4 v = ld4(w.vz + ip);
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float rn = k < 3 ? elc(r0, k + 1) : r4;
-                const float orho = __frcp_rn(0.5f * (elc(r0, k) + rn));
-                if (gz[k]) el(v, k) = g.dt * orho * (elc(d, k) + elc(phi, k)) + elc(v, k);
-            }
+            for (int k = 0; k < 4; k++)
+                if (gz[k]) el(v, k) = elc(cb, k) * (elc(d, k) + elc(phi, k)) + elc(v, k);
             st4(w.vz + ip, v);
         }
     }
@@ -252,9 +254,8 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const flo
 // pressure step with CPML (reference kernel _p, :121-173) on the four cells; returns the
 // new values in pn (old values where not updated) and the per-cell update flags.
 template <int LC>
-__device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const float *__restrict__ vp,
-                                          const float *__restrict__ rho, Wave w, float odx, float odz, int x, int z0,
-                                          float4 &pn, bool upd[4], float4 *ssum = nullptr)
+__device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
+                                          int x, int z0, float4 &pn, bool upd[4], float4 *ssum = nullptr)
 {
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
@@ -303,12 +304,12 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const flo
         }
         st4(w.pvz + ip, po);
     }
-    const float4 v = ldg4(vp + ip), r = ldg4(rho + ip);
+    const float4 kc = ldg4(m.ck + ip);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const float sk = elc(dvx, k) + elc(phx, k) + elc(dvz, k) + elc(phz, k);
         if (ssum) el(*ssum, k) = upd[k] ? sk : 0.f;
-        if (upd[k]) el(pn, k) = g.dt * elc(r, k) * elc(v, k) * elc(v, k) * sk + elc(pn, k);
+        if (upd[k]) el(pn, k) = elc(kc, k) * sk + elc(pn, k);
     }
 }
 
@@ -378,6 +379,7 @@ struct FwdArgs {
     Geo g;
     Cpml c;
     const float *vp, *rho;
+    Mat m;
     Wave w[2];           // w[1] is the Hilbert twin when NW == 2
     // time index = *itp + itoff (a device counter, so one captured graph serves every
     // chunk of steps); wavelet samples come from the device arrays wav0 / wav1
@@ -443,11 +445,11 @@ __global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
     }
     if (x >= a.g.ntx || z0 >= a.g.ntz) return;
 #pragma unroll
-    for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.rho, a.w[k], a.g.odx, a.g.odz, x, z0);
+    for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.m, a.w[k], a.g.odx, a.g.odz, x, z0);
 }
 
 template <int LC, int NW, bool BORN, bool BATCH = false>
-__global__ void __launch_bounds__(256) k_fwd_p(const FwdArgs a0)
+__global__ void __launch_bounds__(256, (NW == 1 && !BORN && !BATCH && LC <= 4) ? 5 : 1) k_fwd_p(const FwdArgs a0)
 {
     FwdArgs a = a0;
     const int it = *a.itp + a.itoff;
@@ -467,7 +469,7 @@ __global__ void __launch_bounds__(256) k_fwd_p(const FwdArgs a0)
 #pragma unroll
         for (int w = 0; w < NW; w++) {
             bool upd[4];
-            p_update4<LC>(g, a.c, a.vp, a.rho, a.w[w], g.odx, g.odz, x, z0, pn[w], upd,
+            p_update4<LC>(g, a.c, a.m, a.w[w], g.odx, g.odz, x, z0, pn[w], upd,
                           (BORN && w == 0) ? &s0 : nullptr);
             bool any = upd[0] || upd[1] || upd[2] || upd[3];
             if constexpr (BORN) {
@@ -543,6 +545,7 @@ struct BwdArgs {
     Geo g;
     Cpml c;
     const float *vp, *rho;
+    Mat m;
     Wave s;              // source wavefield (p, vx, vz only)
     Wave r;              // receiver wavefield
     float *dpdt;
@@ -655,7 +658,7 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
         a.s.p[ip + (a.sz - z0)] -= a.wavsub[it + 1];
     }
     // receiver wavefield velocities (wide guards, negative spacing)
-    v_update4<LC, true>(g, a.c, a.rho, a.r, -g.odx, -g.odz, x, z0);
+    v_update4<LC, true>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0);
 }
 
 template <int LC, bool BATCH = false>
@@ -685,13 +688,12 @@ __global__ void __launch_bounds__(256) k_bwd_2(const BwdArgs a0)
 #pragma unroll
             for (int k = 0; k < 4; k++) el(d, k) += g.rc[ic] * (elc(p1, k) - elc(p2, k)) * g.odx;
         }
-        const float4 r0 = ldg4(a.rho + ip), r1 = ldg4(a.rho + ip + ldz);
+        // (-dt)*rcp(...) = -cbx exactly
+        const float4 cbx = ldg4(a.m.cbx + ip);
         float4 vx = ld4(a.s.vx + ip);
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const float orho = __frcp_rn(0.5f * (elc(r0, k) + elc(r1, k)));
-            if (in[k]) el(vx, k) = (-g.dt) * orho * elc(d, k) + elc(vx, k);
-        }
+        for (int k = 0; k < 4; k++)
+            if (in[k]) el(vx, k) = (-elc(cbx, k)) * elc(d, k) + elc(vx, k);
         st4(a.s.vx + ip, vx);
         ZWin<LC> pw;
         pw.load(a.s.p + (size_t)x * ldz, z0);
@@ -700,20 +702,17 @@ __global__ void __launch_bounds__(256) k_bwd_2(const BwdArgs a0)
         for (int k = 0; k < 4; k++)
 #pragma unroll
             for (int ic = 0; ic < LC; ic++) el(d, k) += g.rc[ic] * (pw.at(k + ic + 1) - pw.at(k - ic)) * g.odz;
-        const float r4 = __ldg(a.rho + ip + 4);
+        const float4 cbz = ldg4(a.m.cbz + ip);
         float4 vz = ld4(a.s.vz + ip);
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const float rn = k < 3 ? elc(r0, k + 1) : r4;
-            const float orho = __frcp_rn(0.5f * (elc(r0, k) + rn));
-            if (in[k]) el(vz, k) = (-g.dt) * orho * elc(d, k) + elc(vz, k);
-        }
+        for (int k = 0; k < 4; k++)
+            if (in[k]) el(vz, k) = (-elc(cbz, k)) * elc(d, k) + elc(vz, k);
         st4(a.s.vz + ip, vz);
     }
     // receiver pressure + hard injection (:717-782)
     float4 pr;
     bool upd[4];
-    p_update4<LC>(g, a.c, a.vp, a.rho, a.r, -g.odx, -g.odz, x, z0, pr, upd);
+    p_update4<LC>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0, pr, upd);
     bool wr = upd[0] || upd[1] || upd[2] || upd[3];
     const int wc = __ldg(a.wells.wcol + x);
     if (wc >= 0) {

@@ -43,8 +43,8 @@ struct swd_ctx {
     int strip_prec = SWD_STRIP_F32;
     std::string err;
     std::vector<DevBuf *> bufs;
-    // model / operator
-    DevBuf vp, rho, cpml[8];
+    // model / operator; mat = the update coefficients cbx, cbz, ck (struct Mat)
+    DevBuf vp, rho, cpml[8], mat[3];
     // wavefields: w[0], w[1] (7 arrays each), dp/dt
     DevBuf wave[2][7], dpdt;
     // second copies of p, vx, vz, phi_p_x, phi_p_z for the fused (double-buffered) path
@@ -97,6 +97,7 @@ struct swd_ctx {
         for (auto &w : bat.w)
             for (auto &b : w) bufs.push_back(&b);
         for (auto &b : cpml) bufs.push_back(&b);
+        for (auto &b : mat) bufs.push_back(&b);
         for (auto &w : wave)
             for (auto &b : w) bufs.push_back(&b);
         for (auto &w : wave2)
@@ -232,6 +233,13 @@ static Cpml make_cpml(swd_ctx *c)
     p.ax = F(c->cpml[0]); p.axh = F(c->cpml[1]); p.az = F(c->cpml[2]); p.azh = F(c->cpml[3]);
     p.bx = F(c->cpml[4]); p.bxh = F(c->cpml[5]); p.bz = F(c->cpml[6]); p.bzh = F(c->cpml[7]);
     return p;
+}
+
+static Mat make_mat(swd_ctx *c)
+{
+    Mat m;
+    m.cbx = F(c->mat[0]); m.cbz = F(c->mat[1]); m.ck = F(c->mat[2]);
+    return m;
 }
 
 static Wave make_wave(swd_ctx *c, int k)
@@ -544,6 +552,31 @@ __global__ void k_smooth(const float *__restrict__ vin, float *vout, const doubl
     vout[ip] = iz < pml + 8 ? vin[ip] : (float)s;
 }
 
+// Update coefficients of struct Mat on the padded grid (same operations and order as the
+// per-cell expressions of the reference kernels): cbx = dt*rcp(0.5*(rho[x]+rho[x+1])),
+// cbz = dt*rcp(0.5*(rho[z]+rho[z+1])), ck = ((dt*rho)*vp)*vp.  Neighbours past the grid read
+// the zeroed padding; coefficients whose denominator is zero are stored as 0 (the updates
+// never use those cells).
+__global__ void k_material(const float *__restrict__ vp, const float *__restrict__ rho, float dt, int ntx, int ntz,
+                           int ldz, float *cbx, float *cbz, float *ck)
+{
+    const size_t n = (size_t)ntx * ldz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int z = (int)(i % ldz);
+        float bx = 0.f, bz = 0.f, kc = 0.f;
+        if (z < ntz) {
+            const float r0 = rho[i], r1 = rho[i + ldz], r2 = rho[i + 1], v = vp[i];
+            const float sx = 0.5f * (r0 + r1), sz = 0.5f * (r0 + r2);
+            if (sx != 0.f) bx = dt * __frcp_rn(sx);
+            if (sz != 0.f) bz = dt * __frcp_rn(sz);
+            kc = dt * r0 * v * v;
+        }
+        cbx[i] = bx;
+        cbz[i] = bz;
+        ck[i] = kc;
+    }
+}
+
 // model_in_pml (acoustic_HLVSPRTMC.cpp:1428-1468): x-edges for interior rows, then z-edges
 __global__ void k_pml_x(float *v, int ntx, int ntz, int pml)
 {
@@ -794,6 +827,7 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     a.c = make_cpml(ctx);
     a.vp = F(ctx->vp);
     a.rho = F(ctx->rho);
+    a.m = make_mat(ctx);
     a.w[0] = make_wave(ctx, 0);
     a.w[1] = J.twin ? make_wave(ctx, 1) : make_wave(ctx, 0);
     a.sx = s->s_ix;
@@ -1144,6 +1178,11 @@ int swd_set_model(swd_ctx *ctx, const float *vp, const float *rho)
     CK(cudaMemsetAsync(ctx->rho.p, 0, ctx->rho.n, ctx->stream));
     CKR(grid_to_dev(ctx, F(ctx->vp), vp));
     CKR(grid_to_dev(ctx, F(ctx->rho), rho));
+    for (auto &b : ctx->mat) CKR(ensure_grid(ctx, b, sizeof(float)));
+    k_material<<<592, 256, 0, ctx->stream>>>(F(ctx->vp), F(ctx->rho), ctx->grid.dt, ctx->ntx, ctx->ntz, ctx->ldz,
+                                             F(ctx->mat[0]), F(ctx->mat[1]), F(ctx->mat[2]));
+    ctx->launches++;
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_model = true;
     return SWD_OK;
@@ -1277,6 +1316,7 @@ int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const fl
     b.c = make_cpml(ctx);
     b.vp = F(ctx->vp);
     b.rho = F(ctx->rho);
+    b.m = make_mat(ctx);
     b.s = make_wave(ctx, 0);
     b.r = make_wave(ctx, 1);
     b.dpdt = F(ctx->dpdt);
