@@ -57,6 +57,22 @@ def load_pkg():
     return mod
 
 
+def max_over_ranks(dist, values, device):
+    """Element-wise max over ranks of per-rank device timings: the slowest rank sets the job
+    time of a replica run.  dist is torch.distributed (or None for one process)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_throughput(units_per_rank, world, t_ms):
+    """Whole-job units per second: every rank processed units_per_rank units in at most t_ms."""
+    return units_per_rank * world / (t_ms / 1e3)
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -232,16 +248,11 @@ def run_ours(args, rank, world, dist):
     with ClockSampler(dev) as clk:
         t_val, launches, prof = timed(d_data, d_rick, d_img, d_fim, args.steps, args.warmup, profile=True)
         t_e2e, _, _ = timed(h_data, h_rick, h_img, h_fim, args.steps, max(1, args.warmup // 3))
-    if dist:
-        import torch.distributed as td
-        t = torch.tensor([t_val, t_e2e], dtype=torch.float64, device="cuda")
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        t_val, t_e2e = float(t[0]), float(t[1])
+    t_val, t_e2e = max_over_ranks(dist, [t_val, t_e2e], "cuda")
     if rank != 0:
         return None
-    shots = args.steps * world
-    value = shots / (t_val / 1e3)
-    e2e = shots / (t_e2e / 1e3)
+    value = replica_throughput(args.steps, world, t_val)
+    e2e = replica_throughput(args.steps, world, t_e2e)
     N, Ni = w.ntx * w.ntz, w.nx * w.nz
     cells_per_shot = nt * (N + Ni + N)
     slen = 2 * w.Lc * w.nx + 2 * w.Lc * (w.nz - 2 * w.Lc)
@@ -419,8 +430,9 @@ def run_lsrtm(args, rank, world, dist):
     with ClockSampler(dev) as clk:
         t_val, launches, prof = timed(args.steps, args.warmup, profile=True)
         t_e2e, _, _ = timed(args.steps, 1, e2e=True)
-    value = nshots * args.steps / (t_val / 1e3)
-    e2e = nshots * args.steps / (t_e2e / 1e3)
+    t_val, t_e2e = max_over_ranks(dist, [t_val, t_e2e], "cuda")
+    value = replica_throughput(nshots * args.steps, world, t_val)
+    e2e = replica_throughput(nshots * args.steps, world, t_e2e)
     per_launch = {k: ms / n for k, (ms, n) in prof.items() if n}
     live = {}
     if all(k in per_launch for k in ("adj_pass_step", "adj_v", "adj_p")):
@@ -527,9 +539,9 @@ def run_batch(args, rank, world, dist):
     batched()
     st_bat16 = E.stack(edge_zero=False).astype(np.float64)
     E.set_strip_precision(swd.STRIP_F32)
-    nshot = len(shots) * args.steps
-    value = nshot / (t_bat / 1e3)
-    plain_v = nshot / (t_plain / 1e3)
+    t_bat, t_plain = max_over_ranks(dist, [t_bat, t_plain], "cuda")
+    value = replica_throughput(len(shots) * args.steps, world, t_bat)
+    plain_v = replica_throughput(len(shots) * args.steps, world, t_plain)
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     return {
         "metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
