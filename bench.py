@@ -590,7 +590,9 @@ def lsrtm_cpu_baseline(w, nsteps=100):
 def run_profile_kernels(args):
     """One RTM shot on the benchmark grid with a short record (--nt) and seeded random data,
     no warm-up shots and no data generation: the command the ncu captures run, so that few
-    launches precede the captured ones.  Prints per-kernel event timings."""
+    launches precede the captured ones.  Kernels are launched directly (no CUDA graphs; the
+    kernels are the same ones the graphs replay), which keeps ncu's per-launch handling fast.
+    Prints per-kernel event timings."""
     import ctypes as C
     swd = load_pkg()
     from swd_b200 import configs
@@ -599,6 +601,7 @@ def run_profile_kernels(args):
     E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt)
     vmig = swd.pad_model(w.vp_mig, w.pmlc)
     E.setup_default(vmig, np.full_like(vmig, 1000.0))
+    E.set_option(swd.OPT_GRAPHS, 0)
     if args.path is not None:
         E.set_kernel_path(args.path)
     rick = swd.ricker_wave(w.nt, w.f0, w.dt)
