@@ -132,11 +132,17 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 # workload
 # ------------------------------------------------------------------------------------------
-WORKLOAD = "c2 PSF-RTM shot: 1601x801 @5 m, nt=6000, dt=0.4 ms, 30 Hz, 641 well receivers, pml 30, 8th order"
+WORKLOADS = {
+    "c2": "c2 PSF-RTM shot: 1601x801 @5 m, nt=6000, dt=0.4 ms, 30 Hz, 641 well receivers, pml 30, 8th order",
+    "c5": "c5 PSF-RTM shot: 4001x1601 @4 m, nt=8000, dt=0.35 ms, 25 Hz, 1201 well receivers, pml 30, 8th order, "
+          "FP16-scaled strips",
+}
+WORKLOAD = WORKLOADS["c2"]
 
 
-def algorithmic_bytes(kernel, w, cp, strip_len, r_n):
-    """Minimum bytes one launch of each kernel must move (each array touched once)."""
+def algorithmic_bytes(kernel, w, cp, strip_len, r_n, strip_esz=4):
+    """Minimum bytes one launch of each kernel must move (each array touched once); strips
+    cost strip_esz bytes per value (4 for FP32, 2 for 16-bit)."""
     N = w.ntx * w.ntz
     Ni = w.nx * w.nz
     nzc = lambda a: int(np.count_nonzero(a))
@@ -145,9 +151,9 @@ def algorithmic_bytes(kernel, w, cp, strip_len, r_n):
     if kernel == "fwd_v":      # p, vx r/w, vz r/w, rho; phi_p_x / phi_p_z r/w in the frame
         return 24 * N + 8 * x_v
     if kernel == "fwd_p":      # vx, vz, p r/w, vp, rho; phi_v r/w in the frame; strip save; traces
-        return 24 * N + 8 * x_p + 4 * strip_len + 4 * r_n
+        return 24 * N + 8 * x_p + strip_esz * strip_len + 4 * r_n
     if kernel == "bwd_1":      # receiver p, v r/w, rho (all cells); source v, p r/w, vp, dp/dt (interior); strips
-        return 24 * N + 24 * Ni + 8 * x_v + 4 * strip_len
+        return 24 * N + 24 * Ni + 8 * x_v + strip_esz * strip_len
     if kernel == "bwd_2":      # receiver v, p r/w, vp, rho; source p, v r/w, dp/dt, FP64 I,S r/w (interior)
         return 24 * N + 56 * Ni + 8 * x_p + 4 * r_n
     if kernel == "fwd_step":   # one fused launch per forward step: p, vx, vz r/w, vp, rho, CPML, strips
@@ -188,10 +194,12 @@ def run_ours(args, rank, world, dist):
     from swd_b200 import configs
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    w = configs.c2()
+    w = configs.CONFIGS[args.config]()
     E, shot, rick, data, cp = setup(swd, w, dev)
     if args.path is not None:
         E.set_kernel_path(args.path)
+    strips = w.extra.get("strips", "f32")
+    E.set_strip_precision({"f32": swd.STRIP_F32, "f16": swd.STRIP_F16}[strips])
     # a dedicated stream: the library captures its time loops into CUDA graphs, which the
     # legacy default stream does not allow
     stream = torch.cuda.Stream()
@@ -275,7 +283,7 @@ def run_ours(args, rank, world, dist):
     launches_per_shot = {"fwd_v": nt, "fwd_p": nt, "bwd_1": nt - 1, "bwd_2": nt - 1, "fwd_step": nt, "bwd_step": nt - 1}
     dom = max(live, key=lambda k: live[k] * launches_per_shot[k])
     peak, src = peaks()
-    ab = algorithmic_bytes(dom, w, cp, slen, r_n)
+    ab = algorithmic_bytes(dom, w, cp, slen, r_n, 4 if strips == "f32" else 2)
     achieved = ab / (live[dom] * 1e-3) / 1e9
     traffic = None
     tj = ROOT / "profiles" / "traffic.json"
@@ -283,13 +291,14 @@ def run_ours(args, rank, world, dist):
         t = json.loads(tj.read_text()).get(dom)
         if t and "bytes_per_cell" in t:
             traffic = t["bytes_per_cell"] * N
-    cpu = cpu_baseline(w, samples=1, nsteps=args.cpu_steps)
+    # the CPU sample: --cpu-steps steps on the 1601x801 grid, fewer on larger grids (same work)
+    cpu = cpu_baseline(w, samples=1, nsteps=max(32, int(args.cpu_steps * 1669 * 869 / N)))
     return {
         "metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP64 imaging)", "data": "synthetic (seeded random-field model, PSF data)",
-        "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed step",
-                   "strips": "f32"},
+        "config": {"workload": WORKLOADS[args.config], "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MiB write) before every timed step", "strips": strips},
         "gcell_updates_per_s": value * cells_per_shot / 1e9,
         "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(data.nbytes + rick.nbytes),
                 "d2h_bytes_per_step": int(2 * w.nx * w.nz * 4)},
@@ -647,6 +656,7 @@ def main():
     ap.add_argument("--nt", type=int, default=30, help="record length of --profile-kernels")
     ap.add_argument("--path", type=int, default=None, help="kernel path: 0 plain (two launches per step), 1 fused")
     ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch"], default="rtm")
+    ap.add_argument("--config", choices=["c2", "c5"], default="c2", help="grid of --workload rtm")
     ap.add_argument("--ckpt-prec", choices=["f32", "f16", "bf16", "i16"], default="bf16",
                     help="checkpoint precision of --workload lsrtm")
     args = ap.parse_args()

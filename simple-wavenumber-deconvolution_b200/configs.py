@@ -162,6 +162,23 @@ def c4(nshots=16):
     return w
 
 
+def c5():
+    """Large imaging: 4001x1601 at 4 m, nt=8000, dt=0.35 ms, 25 Hz; random-field model
+    1800-4500 m/s with 3 dipping interfaces; 24 surface shots; 1201 receivers in a central
+    well (z = 200..1400 cells); scatter points on a 40x16 lattice (spacing 100 cells, offset 50);
+    FP16-scaled boundary strips."""
+    rng = np.random.default_rng(SEED0 + 5)
+    nx, nz = 4001, 1601
+    v = random_field(nx, nz, rng, corr=80.0)
+    w = Workload("c5_4001x1601_nt8000", nx, nz, 4.0, 4.0, 8000, 3.5e-4, 30, 4, 25.0, v, box_smooth(v, 15),
+                 sx=[int(round(50 + s * (nx - 100) / 23)) for s in range(24)], sz=0,
+                 rec_x=np.full(1201, 2000, np.int32), rec_z=np.arange(200, 1401, dtype=np.int32))
+    w.scatter_x = 50 + 100 * np.arange(40)
+    w.scatter_z = 50 + 100 * np.arange(16)
+    w.extra["strips"] = "f16"
+    return w
+
+
 def small(nx=100, nz=60, nt=400, pml=10, Lc=4, dx=5.0, dz=5.0, dt=5.0e-4, f0=25.0, seed=7):
     """Small two-well parity case; nx + 2*pmlc is a multiple of 16 for nx=100, pml=10, Lc=4
     (the reference CUDA build indexes past the grid otherwise)."""
@@ -172,4 +189,4 @@ def small(nx=100, nz=60, nt=400, pml=10, Lc=4, dx=5.0, dz=5.0, dt=5.0e-4, f0=25.
                     box_smooth(v, 5), sx=[nx // 4], sz=0)
 
 
-CONFIGS = {"c1": c1, "c2": c2, "c3": c3, "c4": c4}
+CONFIGS = {"c1": c1, "c2": c2, "c3": c3, "c4": c4, "c5": c5}
