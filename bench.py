@@ -148,18 +148,20 @@ def algorithmic_bytes(kernel, w, cp, strip_len, r_n, strip_esz=4):
     nzc = lambda a: int(np.count_nonzero(a))
     x_v = nzc(cp["a_x_half"]) * w.ntz + nzc(cp["a_z_half"]) * w.ntx     # CPML cells of the v update
     x_p = nzc(cp["a_x"]) * w.ntz + nzc(cp["a_z"]) * w.ntx               # CPML cells of the p update
-    if kernel == "fwd_v":      # p, vx r/w, vz r/w, rho; phi_p_x / phi_p_z r/w in the frame
-        return 24 * N + 8 * x_v
-    if kernel == "fwd_p":      # vx, vz, p r/w, vp, rho; phi_v r/w in the frame; strip save; traces
-        return 24 * N + 8 * x_p + strip_esz * strip_len + 4 * r_n
-    if kernel == "bwd_1":      # receiver p, v r/w, rho (all cells); source v, p r/w, vp, dp/dt (interior); strips
-        return 24 * N + 24 * Ni + 8 * x_v + strip_esz * strip_len
-    if kernel == "bwd_2":      # receiver v, p r/w, vp, rho; source p, v r/w, dp/dt, FP64 I,S r/w (interior)
-        return 24 * N + 56 * Ni + 8 * x_p + 4 * r_n
+    if kernel == "fwd_v":      # p; vx, vz r/w; cbx, cbz; psi r/w in the frame
+        return 28 * N + 8 * x_v
+    if kernel == "fwd_p":      # vx, vz; p r/w; ck; phi r/w in the frame; strip save; traces
+        return 20 * N + 8 * x_p + strip_esz * strip_len + 4 * r_n
+    if kernel == "bwd_1":      # receiver p, v r/w, cbx, cbz (all cells) + psi in the frame;
+        #                        source v, p r/w, vp, rho, dp/dt (interior); strips
+        return 28 * N + 28 * Ni + 8 * x_v + strip_esz * strip_len
+    if kernel == "bwd_2":      # receiver v, p r/w, ck (all cells) + phi in the frame; source p, v r/w,
+        #                        cbx, cbz (interior); dp/dt and FP64 I, S r/w (interior); traces
+        return 20 * N + 64 * Ni + 8 * x_p + 4 * r_n
     if kernel == "fwd_step":   # one fused launch per forward step: p, vx, vz r/w, vp, rho, CPML, strips
-        return 32 * N + 8 * (x_v + x_p) + 4 * strip_len + 4 * r_n
+        return 32 * N + 8 * (x_v + x_p) + strip_esz * strip_len + 4 * r_n
     if kernel == "bwd_step":   # one fused launch per backward step: receiver 24N, material 8N, source 24Ni, FP64 image 32Ni
-        return 32 * N + 56 * Ni + 8 * (x_v + x_p) + 4 * strip_len + 4 * r_n
+        return 32 * N + 56 * Ni + 8 * (x_v + x_p) + strip_esz * strip_len + 4 * r_n
     raise KeyError(kernel)
 
 
@@ -605,7 +607,7 @@ def run_profile_kernels(args):
     import ctypes as C
     swd = load_pkg()
     from swd_b200 import configs
-    w = configs.c2()
+    w = configs.CONFIGS[args.config]()
     w.nt = args.nt
     E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt)
     vmig = swd.pad_model(w.vp_mig, w.pmlc)
@@ -613,6 +615,7 @@ def run_profile_kernels(args):
     E.set_option(swd.OPT_GRAPHS, 0)
     if args.path is not None:
         E.set_kernel_path(args.path)
+    E.set_strip_precision({"f32": swd.STRIP_F32, "f16": swd.STRIP_F16}[w.extra.get("strips", "f32")])
     rick = swd.ricker_wave(w.nt, w.f0, w.dt)
     rx, rz = w.receivers_padded()
     sx, sz = w.source_padded()

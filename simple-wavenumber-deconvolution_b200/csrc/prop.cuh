@@ -98,6 +98,18 @@ __device__ __forceinline__ Strips shift_strips(Strips s, const Batch &bt, int b)
 
 __device__ __forceinline__ size_t cidx(int x, int z, int ldz) { return (size_t)x * ldz + z; }
 
+// Whether the (32, 8) block of cell4() (rows 128*bx .. +127, columns 8*by .. +7) holds a cell
+// of the strip band; uniform over the block, so blocks without strip cells skip the strip
+// code, including the block reduction of 16-bit strips.
+__device__ __forceinline__ bool block_has_strips(int ntx, int ntz, int pmlc, int Lc)
+{
+    const int x0 = blockIdx.y * 8, x1 = x0 + 7, z0 = blockIdx.x * 128, z1 = z0 + 127;
+    auto hit = [&](int xa, int xb, int za, int zb) { return x0 <= xb && x1 >= xa && z0 <= zb && z1 >= za; };
+    const int xl = pmlc, xr = ntx - pmlc - 1, zt = pmlc, zb = ntz - pmlc - 1;
+    return hit(xl, xr, zt, zt + Lc - 1) || hit(xl, xr, zb - Lc + 1, zb) || hit(xl, xl + Lc - 1, zt, zb) ||
+           hit(xr - Lc + 1, xr, zt, zb);
+}
+
 // 16-bit codes of a value v relative to its block's max |v| (mx >= |v|): prec 1 IEEE half of
 // v/mx * 32768, prec 2 bfloat16 of v/mx, prec 3 int16 fixed point round(v/mx * 32767).
 // Normalising first keeps |v|/mx <= 1 even for denormal mx.
@@ -140,6 +152,11 @@ __device__ __forceinline__ int strip_index(int x, int z, int ntx, int ntz, int p
 constexpr int GUARD = 64;
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+// bring the line of a global address into L2 (no register result)
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+    asm volatile("{\n\t.reg .u64 ga;\n\tcvta.to.global.u64 ga, %0;\n\tprefetch.global.L2 [ga];\n\t}" ::"l"(p));
+}
 __device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
 __device__ __forceinline__ float &el(float4 &v, int k) { return (&v.x)[k]; }
@@ -504,7 +521,7 @@ __global__ void __launch_bounds__(256, (NW == 1 && !BORN && !BATCH && LC <= 4) ?
         }
     }
     // strips (field 0): uncompressed store, or per-(step, block) scaled half/bf16
-    if (a.strips.buf) {
+    if (a.strips.buf && block_has_strips(g.ntx, g.ntz, g.pmlc, LC)) {
         int si[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) si[k] = (in && z0 + k < g.ntz) ? strip_index(x, z0 + k, g.ntx, g.ntz, g.pmlc, LC) : -1;
@@ -636,6 +653,7 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
         const float4 v = ldg4(a.vp + ip), r = ldg4(a.rho + ip);
         float4 p = ld4(a.s.p + ip), dp = make_float4(0.f, 0.f, 0.f, 0.f);
         const int nzb = (g.ntz + 127) / 128;
+        const bool band = block_has_strips(g.ntx, g.ntz, g.pmlc, LC);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             if (!in[k]) continue;
@@ -644,8 +662,10 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
             el(dp, k) = rv * (elc(dvx, k) + elc(dvz, k));
             if (src_here && a.sz == z0 + k) el(p, k) -= a.wavsub[it + 1];
             // boundary strips overwrite (fdtd_2d_GPU_kernel_borders_backward :575-620)
-            const int si = strip_index(x, z0 + k, g.ntx, g.ntz, g.pmlc, LC);
-            if (si >= 0) el(p, k) = strip_restore(a.strips, it, si, x, z0 + k, nzb);
+            if (band) {
+                const int si = strip_index(x, z0 + k, g.ntx, g.ntz, g.pmlc, LC);
+                if (si >= 0) el(p, k) = strip_restore(a.strips, it, si, x, z0 + k, nzb);
+            }
         }
         if (src_here) {
 #pragma unroll
@@ -679,6 +699,11 @@ __global__ void __launch_bounds__(256) k_bwd_2(const BwdArgs a0)
     bool any = false;
 #pragma unroll
     for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
+    if (any) {   // the imaging operands are read last: start their DRAM reads now
+        prefetch_l2(a.I + ip);
+        prefetch_l2(a.S + ip);
+        prefetch_l2(a.dpdt + ip);
+    }
     // source wavefield velocities, interior only (:488-573)
     if (any) {
         float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
