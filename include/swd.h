@@ -121,6 +121,15 @@ int swd_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, const flo
  * Unless SWD_RTM_NO_STACK, fimage is added to the context's FP64 stack. */
 int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *data,
                  unsigned flags, float *syn, float *image_pp, float *image_src, float *fimage);
+/* The same RTM in two calls, like the reference's fdtd_2d_GPU_forward(inv_flag=1) /
+ * fdtd_2d_GPU_backward pair (acoustic_HLVSPRTMLc.cu:239-432, 946-1215): swd_rtm_forward runs
+ * the forward pass (syn nullable) and keeps its final wavefield and boundary strips in the
+ * context instead of a disk file; swd_rtm_backward then migrates `data` for the same shot
+ * (same source cell, nt and r_n).  Any other propagation call in between discards the kept
+ * pass, and swd_rtm_backward then returns SWD_ERR_STATE. */
+int swd_rtm_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, float *syn);
+int swd_rtm_backward(swd_ctx *ctx, const swd_shot *shot, const float *data, unsigned flags,
+                     float *image_pp, float *image_src, float *fimage);
 /* raw accumulators of the last shot on the padded grid: I, S (and R if accumulated), FP64 */
 int swd_rtm_raw(swd_ctx *ctx, double *image, double *illum_src, double *illum_rcv);
 /* the stacked image nx*nz, optionally with the reference's edge zeroing

@@ -88,6 +88,8 @@ def lib():
         L.swd_forward.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, vp, vp]
         L.swd_rtm_shot.argtypes = [vp, C.POINTER(Shot), vp, vp, C.c_uint, vp, vp, vp, vp]
         L.swd_rtm_raw.argtypes = [vp, vp, vp, vp]
+        L.swd_rtm_forward.argtypes = [vp, C.POINTER(Shot), vp, vp]
+        L.swd_rtm_backward.argtypes = [vp, C.POINTER(Shot), vp, C.c_uint, vp, vp, vp]
         L.swd_stack_get.argtypes = [vp, C.c_int, vp]
         L.swd_stack_reset.argtypes = [vp]
         L.swd_rtm_batch.argtypes = [vp, C.c_int, C.POINTER(Shot), C.POINTER(vp), C.POINTER(vp), C.c_uint]
@@ -332,6 +334,23 @@ class Engine:
                                     _ptr(outs.get("image_pp")), _ptr(outs.get("image_src")), _ptr(outs.get("fimage"))))
         if syn is not None:
             outs["syn"] = syn
+        return outs
+
+    def rtm_forward(self, shot: ShotSpec, rick, syn=False):
+        """Forward pass of an RTM shot; its final wavefield and strips stay for rtm_backward."""
+        sh, keep = self._shot(shot)
+        out = np.zeros((sh.r_n, sh.nt), np.float32) if syn else None
+        rk = _f32(rick)
+        self._ck(lib().swd_rtm_forward(self._h, C.byref(sh), _ptr(rk), _ptr(out)))
+        return out
+
+    def rtm_backward(self, shot: ShotSpec, data, flags=RTM_PREPROCESS, want=("image_pp", "image_src", "fimage")):
+        """Backward pass of the shot whose rtm_forward ran just before."""
+        sh, keep = self._shot(shot)
+        outs = {k: np.zeros((self.nx, self.nz), np.float32) for k in want}
+        d = _f32(data)
+        self._ck(lib().swd_rtm_backward(self._h, C.byref(sh), _ptr(d), flags, _ptr(outs.get("image_pp")),
+                                        _ptr(outs.get("image_src")), _ptr(outs.get("fimage"))))
         return outs
 
     def rtm_raw(self, rcv=False):

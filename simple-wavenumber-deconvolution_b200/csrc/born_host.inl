@@ -177,6 +177,7 @@ int swd_born_adjoint(swd_ctx *ctx, const swd_shot *shot, const float *rick, cons
     const size_t ntr = (size_t)r_n * nt;
     const size_t fstride = (size_t)ctx->ntx * ctx->ldz;
     const int every = ctx->ckpt_every;
+    ctx->kept.valid = false;   // wave[0] and wave[1] are reused below
     // adjoint source: residual traces, duplicates of a cell summed into the injected trace
     CKR(ensure(ctx, ctx->rbuf, sizeof(float) * ntr));
     CKR(to_dev(ctx, ctx->rbuf.p, resid, sizeof(float) * ntr));

@@ -66,6 +66,13 @@ struct swd_ctx {
     struct BatchBufs {
         DevBuf w[2][7], dpdt, I, S, strips, scale, rdata, wcol, wmap, desc, wav, reduce;
     } bat;
+    // the RTM forward pass whose final wavefield and strips are kept for swd_rtm_backward;
+    // every other pass that reuses those buffers clears it
+    struct KeptShotState {
+        bool valid;
+        int s_ix, s_iz, nt, r_n, path;
+    };
+    KeptShotState kept{false, 0, 0, 0, 0, 0};
     int batch_opt = 0;      // shots per batched launch; 0 = autotune on first use
     int batch_tuned = 0;    // the autotuner's choice (0 = not tuned yet)
     // chunked CUDA-graph execution of the time loops
@@ -815,6 +822,7 @@ static int run_forward_fused(swd_ctx *ctx, FwdJob &J, ShotPlan &P);
 
 static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
 {
+    ctx->kept.valid = false;   // wave[0], strips and the wavelet buffer are overwritten
     // Born fields, S0 output and checkpoints exist on the plain kernels only
     if (fused(ctx) && !J.dkappa && !J.s0 && !J.ck.every) return run_forward_fused(ctx, J, P);
     const swd_shot *s = J.shot;
@@ -1254,11 +1262,10 @@ int swd_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, const flo
     return SWD_OK;
 }
 
-int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *data, unsigned flags, float *syn,
-                 float *image_pp, float *image_src, float *fimage)
+// RTM forward pass: boundary strips saved, the final state stays in wave[0] (and in the
+// second copies for the fused path) for rtm_backward_part; the shot it ran is remembered.
+static int rtm_forward_part(swd_ctx *ctx, const swd_shot *shot, const float *rick, float *syn)
 {
-    CKR(check_ready(ctx));
-    if (!rick || !data) return fail(ctx, SWD_ERR_ARG, "rick and data are required");
     ShotPlan P;
     CKR(plan_shot(ctx, shot, P));
     const int nt = shot->nt, r_n = shot->r_n;
@@ -1270,12 +1277,30 @@ int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const fl
     CKR(ensure(ctx, ctx->seis, sizeof(float) * ntr));
     CK(cudaMemsetAsync(ctx->seis.p, 0, sizeof(float) * ntr, ctx->stream));
     J.seis_dev = F(ctx->seis);
-    // 1. forward pass with boundary strips; the final state stays in wave[0]
     CKR(run_forward(ctx, J, P));
     if (syn) {
         CKR(copy_aliases(ctx, P, F(ctx->seis), nt));
         CKR(from_dev(ctx, syn, ctx->seis.p, sizeof(float) * ntr));
     }
+    ctx->kept = swd_ctx::KeptShotState{true, shot->s_ix, shot->s_iz, shot->nt, shot->r_n, ctx->path};
+    return SWD_OK;
+}
+
+// RTM backward pass of the shot whose forward pass is kept: receiver data (-int int dt dt),
+// source reconstruction + receiver back-propagation + FP64 imaging, per-shot post and stack.
+static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *data, unsigned flags, float *image_pp,
+                             float *image_src, float *fimage)
+{
+    const swd_ctx::KeptShotState &k = ctx->kept;
+    if (!shot) return fail(ctx, SWD_ERR_ARG, "shot is NULL");
+    if (!k.valid || k.s_ix != shot->s_ix || k.s_iz != shot->s_iz || k.nt != shot->nt || k.r_n != shot->r_n ||
+        k.path != ctx->path)
+        return fail(ctx, SWD_ERR_STATE, "the backward pass needs the forward pass of the same shot just before it");
+    ctx->kept.valid = false;   // the reconstruction runs the kept wavefield back to time 0
+    ShotPlan P;
+    CKR(plan_shot(ctx, shot, P));
+    const int nt = shot->nt, r_n = shot->r_n;
+    const size_t ntr = (size_t)r_n * nt;
     // 2. receiver data, -int int dt dt
     CKR(ensure(ctx, ctx->rdata, sizeof(float) * 2 * ntr));
     float *raw = F(ctx->rdata), *rms = raw + ntr;
@@ -1404,6 +1429,33 @@ int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const fl
     prof_collect(ctx);
     ctx->have_shot = true;
     return SWD_OK;
+}
+
+int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *data, unsigned flags, float *syn,
+                 float *image_pp, float *image_src, float *fimage)
+{
+    CKR(check_ready(ctx));
+    if (!rick || !data) return fail(ctx, SWD_ERR_ARG, "rick and data are required");
+    CKR(rtm_forward_part(ctx, shot, rick, syn));
+    return rtm_backward_part(ctx, shot, data, flags, image_pp, image_src, fimage);
+}
+
+int swd_rtm_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, float *syn)
+{
+    CKR(check_ready(ctx));
+    if (!rick) return fail(ctx, SWD_ERR_ARG, "rick is required");
+    CKR(rtm_forward_part(ctx, shot, rick, syn));
+    CK(cudaStreamSynchronize(ctx->stream));
+    prof_collect(ctx);
+    return SWD_OK;
+}
+
+int swd_rtm_backward(swd_ctx *ctx, const swd_shot *shot, const float *data, unsigned flags, float *image_pp,
+                     float *image_src, float *fimage)
+{
+    CKR(check_ready(ctx));
+    if (!data) return fail(ctx, SWD_ERR_ARG, "data is required");
+    return rtm_backward_part(ctx, shot, data, flags, image_pp, image_src, fimage);
 }
 
 int swd_rtm_raw(swd_ctx *ctx, double *image, double *illum_src, double *illum_rcv)

@@ -12,7 +12,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, PKG_DIR, rel_l2
+from conftest import GOLDEN, PKG_DIR, ROOT, rel_l2
 
 TOL = 1e-4
 
@@ -112,3 +112,35 @@ def test_decon2d_mine_reproduces_the_reference_program():
             assert len(txt) == nz + 1
         assert np.array_equal(coef, g[f"coef{k}"])
         assert rel_l2(dec, g[f"dec{k}"]) < 1e-3
+
+
+REF_ON_SWD = ROOT / "oracle" / "_ref"
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (REF_ON_SWD / "AVSPRTM_on_swd").exists(), reason="reference hosts on libswd not built")
+def test_reference_host_programs_on_libswd():
+    """The reference's own, unmodified host programs (AFor, AVSPRTM) linked against the compat
+    libraries (libswd_reffwd.so / libswd_refrtm.so) in place of their CUDA files reproduce the
+    files of the reference's complete CUDA programs."""
+    g = np.load(GOLDEN / "ref_gpu_small.npz")
+    mk = _mkg("make_golden_ref_gpu")
+    nx, nz, pml, Lc, nt, swin, window = [int(v) for v in g["case"]]
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        g["acc_vp"].tofile(d / "input" / "acc_vp.bin")
+        rd = lambda name, shape: np.fromfile(d / "output" / name, np.float32).reshape(shape)
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
+        for flag in (0, 1):
+            mk.write_params(d / "parameter.txt", mk.CASE, flag)
+            subprocess.run([str(REF_ON_SWD / "AFor_on_swd")], cwd=d / "forward", check=True, capture_output=True, env=env)
+            subprocess.run([str(REF_ON_SWD / "AVSPRTM_on_swd")], cwd=d, check=True, capture_output=True, env=env)
+        r_n = g["obs"].shape[0]
+        assert rel_l2(rd("1source_seismogram_obs.bin", (r_n, nt)), g["obs"]) < TOL
+        assert rel_l2(rd("1source_seismogram_obsup.bin", (r_n, nt)), g["obsup"]) < TOL
+        assert rel_l2(rd("1source_seismogram_obsdown.bin", (r_n, nt)), g["obsdown"]) < TOL
+        assert rel_l2(rd("image_pp1.bin", (nx, nz)), g["image_pp"]) < TOL
+        assert rel_l2(rd("fimage_pp1.bin", (nx, nz)), g["fimage_pp"]) < TOL
+        assert rel_l2(rd("migration_pp.bin", (nx, nz)), g["migration_pp"]) < TOL
+        assert rel_l2(rd("1source_seismogram_scatterup.bin", (r_n, nt)), g["scatterup"]) < 1e-2
+        assert rel_l2(rd("migration_psf.bin", (nx, nz)), g["migration_psf"]) < 1e-2

@@ -278,3 +278,21 @@ def test_engine_matches_reference_cuda_build(swd, orc):
     out = E.rtm_shot(shot, rick, g["scatterup"])
     assert rel_l2(out["image_pp"], g["image_psf"]) < TOL
     assert rel_l2(out["fimage"], g["fimage_psf"]) < TOL
+
+
+def test_rtm_in_two_calls_equals_one(case, swd, orc):
+    """swd_rtm_forward + swd_rtm_backward (the reference's forward/backward pair) give the images
+    of swd_rtm_shot; a backward pass without its forward pass is refused."""
+    data = orc.forward(case.M, case.G, case.rick)["seis"]
+    one = case.E.rtm_shot(case.shot, case.rick, data, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK, want=("image_pp", "fimage", "syn"))
+    syn = case.E.rtm_forward(case.shot, case.rick, syn=True)
+    two = case.E.rtm_backward(case.shot, data, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK, want=("image_pp", "fimage"))
+    assert np.array_equal(syn, one["syn"])
+    assert np.array_equal(two["image_pp"], one["image_pp"])
+    assert np.array_equal(two["fimage"], one["fimage"])
+    with pytest.raises(swd.SwdError):          # state consumed by the backward pass
+        case.E.rtm_backward(case.shot, data)
+    case.E.rtm_forward(case.shot, case.rick)
+    case.E.forward(case.shot, case.rick)       # another pass reuses the buffers
+    with pytest.raises(swd.SwdError):
+        case.E.rtm_backward(case.shot, data)
