@@ -6,10 +6,10 @@
 // half-node buoyancies and dt*rho*vp^2, formed once per model).  CPML memory variables are only
 // read and written where the profile coefficient a is non-zero (the PML frame).
 //
-// Arithmetic follows the reference kernels term by term (acoustic_HLVSPRTMLc.cu:24-221,
-// 434-817; forward/acoustic_hilbert_fftkz_HLForLc.cu:168-558) so FP32 results agree to
-// rounding noise: derivative sums in tap order, phi = b*phi + a*d, v += dt*b*(d+phi),
-// p += dt*rho*vp*vp*(dvx+phi_x+dvz+phi_z).
+// Arithmetic follows the reference kernels (acoustic_HLVSPRTMLc.cu:24-221, 434-817;
+// forward/acoustic_hilbert_fftkz_HLForLc.cu:168-558) so FP32 results agree to rounding noise:
+// derivative sums in tap order (each tap as (rc*odx)*(a-b), struct Taps), phi = b*phi + a*d,
+// v += dt*b*(d+phi), p += dt*rho*vp*vp*(dvx+phi_x+dvz+phi_z).
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
@@ -162,6 +162,19 @@ __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<floa
 __device__ __forceinline__ float &el(float4 &v, int k) { return (&v.x)[k]; }
 __device__ __forceinline__ float elc(const float4 &v, int k) { return (&v.x)[k]; }
 
+// Stencil coefficients folded with the grid spacing: c[ic] = rc[ic] * (1/dx), so a tap costs
+// one subtraction and one fused multiply-add (the reference forms rc*(a-b)*odx per tap; the
+// folded form differs from it by rounding only).
+template <int LC>
+struct Taps {
+    float c[LC];
+    __device__ __forceinline__ Taps(const Geo &g, float od)
+    {
+#pragma unroll
+        for (int ic = 0; ic < LC; ic++) c[ic] = g.rc[ic] * od;
+    }
+};
+
 // z-window of a column around z0: w[NB*4 + k] holds z0 + k for k in [-NB*4, 4 + NB*4)
 template <int LC>
 struct ZWin {
@@ -187,6 +200,7 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat
 {
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
+    const Taps<LC> tx(g, odx), tz(g, odz);
     // ---- vx: x taps from the neighbouring columns
     const bool colx = x >= LC - 1 && x <= ntx - LC - 1;
     if (colx) {
@@ -204,7 +218,7 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat
             for (int ic = 0; ic < LC; ic++) {
                 const float4 a = ld4(w.p + ip + (size_t)(ic + 1) * ldz), b = ld4(w.p + ip - (size_t)ic * ldz);
 #pragma unroll
-                for (int k = 0; k < 4; k++) el(d, k) += g.rc[ic] * (elc(a, k) - elc(b, k)) * odx;
+                for (int k = 0; k < 4; k++) el(d, k) += tx.c[ic] * (elc(a, k) - elc(b, k));
             }
             const float ax = __ldg(c.axh + x);
             float4 phi = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -244,7 +258,7 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat
 #pragma unroll
             for (int k = 0; k < 4; k++)
 #pragma unroll
-                for (int ic = 0; ic < LC; ic++) el(d, k) += g.rc[ic] * (pw.at(k + ic + 1) - pw.at(k - ic)) * odz;
+                for (int ic = 0; ic < LC; ic++) el(d, k) += tz.c[ic] * (pw.at(k + ic + 1) - pw.at(k - ic));
             float4 phi = make_float4(0.f, 0.f, 0.f, 0.f);
             const float4 az = ldg4(c.azh + z0);
             if (az.x != 0.f || az.y != 0.f || az.z != 0.f || az.w != 0.f) {
@@ -286,6 +300,7 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat
     }
     if (!any) return;
     float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
+    const Taps<LC> tx(g, odx), tz(g, odz);
     ZWin<LC> vw;
     vw.load(w.vz + (size_t)x * ldz, z0);
 #pragma unroll
@@ -293,8 +308,8 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat
         const float4 a = ld4(w.vx + ip + (size_t)ic * ldz), b = ld4(w.vx + ip - (size_t)(ic + 1) * ldz);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            el(dvx, k) += g.rc[ic] * (elc(a, k) - elc(b, k)) * odx;
-            el(dvz, k) += g.rc[ic] * (vw.at(k + ic) - vw.at(k - ic - 1)) * odz;
+            el(dvx, k) += tx.c[ic] * (elc(a, k) - elc(b, k));
+            el(dvz, k) += tz.c[ic] * (vw.at(k + ic) - vw.at(k - ic - 1));
         }
     }
     float4 phx = make_float4(0.f, 0.f, 0.f, 0.f), phz = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -639,6 +654,7 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
     const bool src_here = x == a.sx && a.sz >= z0 && a.sz < z0 + 4;
     if (any) {
         float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
+        const Taps<LC> tx(g, g.odx), tz(g, g.odz);
         ZWin<LC> vw;
         vw.load(a.s.vz + (size_t)x * ldz, z0);
 #pragma unroll
@@ -646,8 +662,8 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
             const float4 p1 = ld4(a.s.vx + ip + (size_t)ic * ldz), p2 = ld4(a.s.vx + ip - (size_t)(ic + 1) * ldz);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                el(dvx, k) += g.rc[ic] * (elc(p1, k) - elc(p2, k)) * g.odx;
-                el(dvz, k) += g.rc[ic] * (vw.at(k + ic) - vw.at(k - ic - 1)) * g.odz;
+                el(dvx, k) += tx.c[ic] * (elc(p1, k) - elc(p2, k));
+                el(dvz, k) += tz.c[ic] * (vw.at(k + ic) - vw.at(k - ic - 1));
             }
         }
         const float4 v = ldg4(a.vp + ip), r = ldg4(a.rho + ip);
@@ -706,12 +722,13 @@ __global__ void __launch_bounds__(256) k_bwd_2(const BwdArgs a0)
     }
     // source wavefield velocities, interior only (:488-573)
     if (any) {
+        const Taps<LC> tx(g, g.odx), tz(g, g.odz);
         float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int ic = 0; ic < LC; ic++) {
             const float4 p1 = ld4(a.s.p + ip + (size_t)(ic + 1) * ldz), p2 = ld4(a.s.p + ip - (size_t)ic * ldz);
 #pragma unroll
-            for (int k = 0; k < 4; k++) el(d, k) += g.rc[ic] * (elc(p1, k) - elc(p2, k)) * g.odx;
+            for (int k = 0; k < 4; k++) el(d, k) += tx.c[ic] * (elc(p1, k) - elc(p2, k));
         }
         // (-dt)*rcp(...) = -cbx exactly
         const float4 cbx = ldg4(a.m.cbx + ip);
@@ -726,7 +743,7 @@ __global__ void __launch_bounds__(256) k_bwd_2(const BwdArgs a0)
 #pragma unroll
         for (int k = 0; k < 4; k++)
 #pragma unroll
-            for (int ic = 0; ic < LC; ic++) el(d, k) += g.rc[ic] * (pw.at(k + ic + 1) - pw.at(k - ic)) * g.odz;
+            for (int ic = 0; ic < LC; ic++) el(d, k) += tz.c[ic] * (pw.at(k + ic + 1) - pw.at(k - ic));
         const float4 cbz = ldg4(a.m.cbz + ip);
         float4 vz = ld4(a.s.vz + ip);
 #pragma unroll
