@@ -89,6 +89,14 @@ int swd_set_cpml(swd_ctx *ctx, const float *a_x, const float *a_x_half,
                  const float *b_z, const float *b_z_half);
 int swd_set_model(swd_ctx *ctx, const float *vp, const float *rho);   /* padded ntx*ntz */
 int swd_set_strip_precision(swd_ctx *ctx, int strip_precision);       /* SWD_STRIP_* */
+/* Source wavefield of the RTM backward pass (no reference counterpart; the reference
+ * reconstructs it from boundary strips, acoustic_HLVSPRTMLc.cu:434-620).  store = 0 (default):
+ * reconstruct, as the reference does.  store = 1: the forward pass stores dp/dt of every step on
+ * the interior at `prec` (SWD_STRIP_*, 16-bit codes with one scale per step and 128x8-cell
+ * block; nt * nx * nz * 2 bytes at 16 bits) and the backward pass propagates only the receiver
+ * wavefield, moving ~40% fewer bytes per step; the image differs from the reconstructed one by
+ * the storage rounding (and not at all in exact arithmetic). */
+int swd_set_source_storage(swd_ctx *ctx, int store, int prec);
 /* kernel path: SWD_PATH_PLAIN (default) runs four cells of a column per thread with 128-bit
  * loads and two launches per time step (the velocity and pressure halves, like the
  * reference's vx/vz/p kernels); SWD_PATH_FUSED (Lc <= 6) runs one launch per time step on

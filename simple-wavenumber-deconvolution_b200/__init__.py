@@ -85,6 +85,7 @@ def lib():
         L.swd_set_model.argtypes = [vp, vp, vp]
         L.swd_set_strip_precision.argtypes = [vp, C.c_int]
         L.swd_set_kernel_path.argtypes = [vp, C.c_int]
+        L.swd_set_source_storage.argtypes = [vp, C.c_int, C.c_int]
         L.swd_forward.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, vp, vp]
         L.swd_rtm_shot.argtypes = [vp, C.POINTER(Shot), vp, vp, C.c_uint, vp, vp, vp, vp]
         L.swd_rtm_raw.argtypes = [vp, vp, vp, vp]
@@ -258,6 +259,11 @@ class Engine:
 
     def set_strip_precision(self, prec: int):
         self._ck(lib().swd_set_strip_precision(self._h, prec))
+
+    def set_source_storage(self, store: int, prec: int = STRIP_I16):
+        """store=1: the RTM forward pass stores dp/dt at `prec` and the backward pass propagates
+        only the receiver wavefield; store=0 reconstructs the source wavefield from strips."""
+        self._ck(lib().swd_set_source_storage(self._h, store, prec))
 
     def set_kernel_path(self, path: int):
         """PATH_PLAIN: one cell per thread, two launches per step; PATH_FUSED: one launch per step."""

@@ -18,7 +18,7 @@ static void launch_fwd_batch(const FwdArgs &a, dim3 grid, cudaStream_t s, cudaEv
     if (ev) cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal);
     k_fwd_v<LC, 1, false, true><<<grid, dim3(32, 8), 0, s>>>(a);
     if (ev) { cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal); }
-    k_fwd_p<LC, 1, false, true><<<grid, dim3(32, 8), 0, s>>>(a);
+    k_fwd_p<LC, 1, FP_PLAIN, true><<<grid, dim3(32, 8), 0, s>>>(a);
     if (ev) cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal);
 }
 

@@ -37,7 +37,22 @@ struct Cpml {
 // ck = ((dt*rho)*vp)*vp.  vx += cbx*(d + phi), vz += cbz*(d + phi), p += ck*(sum).
 struct Mat {
     const float *cbx, *cbz, *ck;
+    const float *kap;    // (rho*vp)*vp, the dp/dt factor of the imaging condition
 };
+
+// dp/dt of the source wavefield, stored by the forward pass on the interior for a backward
+// pass that does not reconstruct the source wavefield.  Layout [step][x - pmlc][z - zlo] with
+// row pitch ldr (the interior rows rounded out to whole 4-cell chunks); prec 0 f32, else a
+// 16-bit code of enc16 with one scale (max |dp/dt|) per (step, 128 x 8 block).
+struct DpStore {
+    void *buf;       // nullptr: not stored
+    float *scale;
+    int prec, zlo, ldr, nblocks;
+    long long step;  // elements per step
+};
+
+// forward pressure-kernel modes
+constexpr int FP_PLAIN = 0, FP_BORN = 1, FP_STORE = 2;
 
 // One wavefield updated in place.
 struct Wave {
@@ -436,6 +451,7 @@ struct FwdArgs {
     const float *dkappa;
     Ckpt ck;             // field-0 state checkpoints, taken by the CKPT instantiation of k_fwd_v
     Batch bt;            // the BATCH instantiations (NW == 1): shot = blockIdx.z
+    DpStore ds;          // the FP_STORE instantiation (NW == 1): dp/dt of each step
 };
 
 // The shot's view of a batched forward launch; false when the shot's record has ended.
@@ -452,6 +468,66 @@ __device__ __forceinline__ bool fwd_view(FwdArgs &a, int it)
     if (a.seis) a.seis += d.seis_off;
     a.strips = shift_strips(a.strips, a.bt, b);
     return true;
+}
+
+__device__ __forceinline__ bool interior(int x, int z, const Geo &g)
+{
+    return z >= g.pmlc && z <= g.ntz - g.pmlc - 1 && x >= g.pmlc && x <= g.ntx - g.pmlc - 1;
+}
+
+// The stored dp/dt chunk of cell4 (x, z0): element offset in its step, or -1 outside the store.
+__device__ __forceinline__ long long dp_offset(const DpStore &ds, const Geo &g, int x, int z0)
+{
+    if (x < g.pmlc || x > g.ntx - g.pmlc - 1 || z0 < ds.zlo || z0 >= ds.zlo + ds.ldr) return -1;
+    return (long long)(x - g.pmlc) * ds.ldr + (z0 - ds.zlo);
+}
+
+// Called by every thread of a (32, 8) block: dp/dt = kap * S of the interior cells of its
+// chunk (zero on the chunk's other cells), block max for 16-bit codes, then the store.
+__device__ __forceinline__ void store_dpdt(const DpStore &ds, const Mat &m, const Geo &g, int it, int x, int z0,
+                                           bool in, float4 s)
+{
+    const long long off = in ? dp_offset(ds, g, x, z0) : -1;
+    float4 dp = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (off >= 0) {
+        const float4 kp = ldg4(m.kap + (size_t)x * g.ldz + z0);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (z0 + k >= g.pmlc && z0 + k <= g.ntz - g.pmlc - 1) el(dp, k) = elc(kp, k) * elc(s, k);
+    }
+    const size_t base = (size_t)it * ds.step;
+    if (ds.prec == 0) {
+        if (off >= 0) st4((float *)ds.buf + base + off, dp);
+        return;
+    }
+    __shared__ float smax;
+    if (threadIdx.x == 0 && threadIdx.y == 0) smax = 0.f;
+    __syncthreads();
+    float v = fmaxf(fmaxf(fabsf(dp.x), fabsf(dp.y)), fmaxf(fabsf(dp.z), fabsf(dp.w)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0 && v > 0.f) atomicMax((int *)&smax, __float_as_int(v));
+    __syncthreads();
+    const float mx = smax;
+    if (threadIdx.x == 0 && threadIdx.y == 0) ds.scale[(size_t)it * ds.nblocks + blockIdx.y * gridDim.x + blockIdx.x] = mx;
+    if (off >= 0) {
+        ushort4 h;
+        h.x = enc16(dp.x, mx, ds.prec); h.y = enc16(dp.y, mx, ds.prec);
+        h.z = enc16(dp.z, mx, ds.prec); h.w = enc16(dp.w, mx, ds.prec);
+        *reinterpret_cast<ushort4 *>((unsigned short *)ds.buf + base + off) = h;
+    }
+}
+
+// stored dp/dt of the chunk at step `it` (decoded), zero outside the store
+__device__ __forceinline__ float4 load_dpdt(const DpStore &ds, const Geo &g, int it, int x, int z0)
+{
+    const long long off = dp_offset(ds, g, x, z0);
+    if (off < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const size_t base = (size_t)it * ds.step;
+    if (ds.prec == 0) return ld4((const float *)ds.buf + base + off);
+    const float mx = ds.scale[(size_t)it * ds.nblocks + blockIdx.y * gridDim.x + blockIdx.x];
+    const ushort4 h = *reinterpret_cast<const ushort4 *>((const unsigned short *)ds.buf + base + off);
+    return make_float4(dec16(h.x, mx, ds.prec), dec16(h.y, mx, ds.prec), dec16(h.z, mx, ds.prec), dec16(h.w, mx, ds.prec));
 }
 
 // block (32, 8): lane -> four rows, warp -> one column; a block covers 128 rows x 8 columns
@@ -480,9 +556,11 @@ __global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
     for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.m, a.w[k], a.g.odx, a.g.odz, x, z0);
 }
 
-template <int LC, int NW, bool BORN, bool BATCH = false>
-__global__ void __launch_bounds__(256, (NW == 1 && !BORN && !BATCH && LC <= 4) ? 5 : 1) k_fwd_p(const FwdArgs a0)
+template <int LC, int NW, int MODE, bool BATCH = false>
+__global__ void __launch_bounds__(256, (NW == 1 && MODE == FP_PLAIN && !BATCH && LC <= 4) ? 5 : 1)
+    k_fwd_p(const FwdArgs a0)
 {
+    constexpr bool BORN = MODE == FP_BORN;
     FwdArgs a = a0;
     const int it = *a.itp + a.itoff;
     if constexpr (BATCH) {
@@ -495,14 +573,14 @@ __global__ void __launch_bounds__(256, (NW == 1 && !BORN && !BATCH && LC <= 4) ?
     float4 pn[NW];
 #pragma unroll
     for (int k = 0; k < NW; k++) pn[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f);   // field 0's p-update sum (Born, store)
     if (in) {
         const size_t ip = (size_t)x * g.ldz + z0;
-        float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int w = 0; w < NW; w++) {
             bool upd[4];
             p_update4<LC>(g, a.c, a.m, a.w[w], g.odx, g.odz, x, z0, pn[w], upd,
-                          (BORN && w == 0) ? &s0 : nullptr);
+                          (MODE != FP_PLAIN && w == 0) ? &s0 : nullptr);
             bool any = upd[0] || upd[1] || upd[2] || upd[3];
             if constexpr (BORN) {
                 if (w == 0 && a.s0_out) st4(a.s0_out + (size_t)(it % a.s0_mod) * a.s0_stride + ip, s0);
@@ -535,6 +613,8 @@ __global__ void __launch_bounds__(256, (NW == 1 && !BORN && !BATCH && LC <= 4) ?
             }
         }
     }
+    // dp/dt = kappa * S on the interior, for the backward pass of the stored-source mode
+    if constexpr (MODE == FP_STORE) store_dpdt(a.ds, a.m, g, it, x, z0, in, s0);
     // strips (field 0): uncompressed store, or per-(step, block) scaled half/bf16
     if (a.strips.buf && block_has_strips(g.ntx, g.ntz, g.pmlc, LC)) {
         int si[4];
@@ -590,6 +670,7 @@ struct BwdArgs {
     const float *rdata;  // [r_n][nt] preprocessed data injected at the receivers
     double *I, *S, *R;   // FP64 imaging accumulators (R nullable)
     Batch bt;            // the BATCH instantiations: shot = blockIdx.z
+    DpStore ds;          // stored-source backward (k_bwd_rcv_*): dp/dt of forward step it+1
 };
 
 // The shot's view of a batched backward launch: its own time index (every shot of a batch
@@ -625,11 +706,6 @@ __device__ __forceinline__ float strip_restore(const Strips &st, int it, int si,
     const float mx = st.scale[(size_t)it * st.nscale + slot];
     if (mx == 0.f) return 0.f;
     return dec16(((const unsigned short *)st.buf)[(size_t)it * st.slen + si], mx, st.prec);
-}
-
-__device__ __forceinline__ bool interior(int x, int z, const Geo &g)
-{
-    return z >= g.pmlc && z <= g.ntz - g.pmlc - 1 && x >= g.pmlc && x <= g.ntx - g.pmlc - 1;
 }
 
 template <int LC, bool BATCH = false>
@@ -768,6 +844,78 @@ __global__ void __launch_bounds__(256) k_bwd_2(const BwdArgs a0)
     // imaging condition in FP64 (sum_image_GPU_kernel_image :785-817)
     if (any) {
         const float4 dp4 = ld4(a.dpdt + ip);
+        double2 *I2 = reinterpret_cast<double2 *>(a.I + ip), *S2 = reinterpret_cast<double2 *>(a.S + ip);
+        double2 i0 = I2[0], i1 = I2[1], s0 = S2[0], s1 = S2[1];
+        double *iv[4] = {&i0.x, &i0.y, &i1.x, &i1.y}, *sv[4] = {&s0.x, &s0.y, &s1.x, &s1.y};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!in[k]) continue;
+            const double dp = (double)elc(dp4, k);
+            *iv[k] += dp * (double)elc(pr, k);
+            *sv[k] += dp * dp;
+        }
+        I2[0] = i0; I2[1] = i1; S2[0] = s0; S2[1] = s1;
+        if (a.R) {
+            double2 *R2 = reinterpret_cast<double2 *>(a.R + ip);
+            double2 q0 = R2[0], q1 = R2[1];
+            double *rv[4] = {&q0.x, &q0.y, &q1.x, &q1.y};
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (in[k]) *rv[k] += (double)elc(pr, k) * (double)elc(pr, k);
+            R2[0] = q0; R2[1] = q1;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Backward step of the stored-source mode: the forward pass stored dp/dt, so only the
+// receiver wavefield propagates.  Backward index it images with the dp/dt of forward step
+// it + 1, the step whose pressure update the reconstruction at index it undoes.
+//   R1: receiver vx, vz (CPML, -dx/-dz, wide guards)
+//   R2: receiver p (CPML) + hard injection; FP64 imaging with the stored dp/dt
+// ------------------------------------------------------------------------------------
+template <int LC>
+__global__ void __launch_bounds__(256) k_bwd_rcv_v(const BwdArgs a)
+{
+    int x, z0;
+    cell4(x, z0);
+    if (x >= a.g.ntx || z0 >= a.g.ntz) return;
+    v_update4<LC, true>(a.g, a.c, a.m, a.r, -a.g.odx, -a.g.odz, x, z0);
+}
+
+template <int LC>
+__global__ void __launch_bounds__(256) k_bwd_rcv_p(const BwdArgs a)
+{
+    const int it = *a.itp + a.itoff;
+    int x, z0;
+    cell4(x, z0);
+    const Geo &g = a.g;
+    if (x >= g.ntx || z0 >= g.ntz) return;
+    const int ldz = g.ldz;
+    const size_t ip = (size_t)x * ldz + z0;
+    bool in[4];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
+    if (any) {
+        prefetch_l2(a.I + ip);
+        prefetch_l2(a.S + ip);
+    }
+    float4 pr;
+    bool upd[4];
+    p_update4<LC>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0, pr, upd);
+    bool wr = upd[0] || upd[1] || upd[2] || upd[3];
+    const int wc = __ldg(a.wells.wcol + x);
+    if (wc >= 0) {
+        const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * ldz + z0));
+        const int t[4] = {tr.x, tr.y, tr.z, tr.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (t[k] >= 0 && z0 + k < g.ntz) { el(pr, k) = a.rdata[(size_t)t[k] * a.nt + it]; wr = true; }
+    }
+    if (wr) st4(a.r.p + ip, pr);
+    if (any) {
+        const float4 dp4 = load_dpdt(a.ds, g, it + 1, x, z0);
         double2 *I2 = reinterpret_cast<double2 *>(a.I + ip), *S2 = reinterpret_cast<double2 *>(a.S + ip);
         double2 i0 = I2[0], i1 = I2[1], s0 = S2[0], s1 = S2[1];
         double *iv[4] = {&i0.x, &i0.y, &i1.x, &i1.y}, *sv[4] = {&s0.x, &s0.y, &s1.x, &s1.y};

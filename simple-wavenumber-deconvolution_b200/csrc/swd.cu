@@ -44,7 +44,7 @@ struct swd_ctx {
     std::string err;
     std::vector<DevBuf *> bufs;
     // model / operator; mat = the update coefficients cbx, cbz, ck (struct Mat)
-    DevBuf vp, rho, cpml[8], mat[3];
+    DevBuf vp, rho, cpml[8], mat[4];
     // wavefields: w[0], w[1] (7 arrays each), dp/dt
     DevBuf wave[2][7], dpdt;
     // second copies of p, vx, vz, phi_p_x, phi_p_z for the fused (double-buffered) path
@@ -71,8 +71,12 @@ struct swd_ctx {
     struct KeptShotState {
         bool valid;
         int s_ix, s_iz, nt, r_n, path;
+        bool stored;     // the forward pass stored dp/dt (no reconstruction needed)
     };
-    KeptShotState kept{false, 0, 0, 0, 0, 0};
+    KeptShotState kept{false, 0, 0, 0, 0, 0, false};
+    // stored-source RTM: the forward pass keeps dp/dt of every step (swd_set_source_storage)
+    int src_store = 0, src_prec = SWD_STRIP_I16;
+    DevBuf dpst, dpsc;
     int batch_opt = 0;      // shots per batched launch; 0 = autotune on first use
     int batch_tuned = 0;    // the autotuner's choice (0 = not tuned yet)
     // chunked CUDA-graph execution of the time loops
@@ -95,7 +99,7 @@ struct swd_ctx {
     {
         DevBuf *all[] = {&vp, &rho, &dpdt, &wcol, &wmap, &seis, &seis2, &rdata, &colbuf, &kzcoef, &tw,
                          &strips, &strip_scale, &I, &S, &R, &stack, &reduce, &stage_in, &stage_out, &ctrl, &wav,
-                         &dk, &gk, &s0, &ckpt, &rbuf, &alias};
+                         &dk, &gk, &s0, &ckpt, &rbuf, &alias, &dpst, &dpsc};
         for (DevBuf *b : all) bufs.push_back(b);
         for (auto &b : adj) bufs.push_back(&b);
         DevBuf *ball[] = {&bat.dpdt, &bat.I, &bat.S, &bat.strips, &bat.scale, &bat.rdata, &bat.wcol, &bat.wmap,
@@ -245,7 +249,7 @@ static Cpml make_cpml(swd_ctx *c)
 static Mat make_mat(swd_ctx *c)
 {
     Mat m;
-    m.cbx = F(c->mat[0]); m.cbz = F(c->mat[1]); m.ck = F(c->mat[2]);
+    m.cbx = F(c->mat[0]); m.cbz = F(c->mat[1]); m.ck = F(c->mat[2]); m.kap = F(c->mat[3]);
     return m;
 }
 
@@ -561,26 +565,28 @@ __global__ void k_smooth(const float *__restrict__ vin, float *vout, const doubl
 
 // Update coefficients of struct Mat on the padded grid (same operations and order as the
 // per-cell expressions of the reference kernels): cbx = dt*rcp(0.5*(rho[x]+rho[x+1])),
-// cbz = dt*rcp(0.5*(rho[z]+rho[z+1])), ck = ((dt*rho)*vp)*vp.  Neighbours past the grid read
+// cbz = dt*rcp(0.5*(rho[z]+rho[z+1])), ck = ((dt*rho)*vp)*vp, kap = (rho*vp)*vp.  Neighbours past the grid read
 // the zeroed padding; coefficients whose denominator is zero are stored as 0 (the updates
 // never use those cells).
 __global__ void k_material(const float *__restrict__ vp, const float *__restrict__ rho, float dt, int ntx, int ntz,
-                           int ldz, float *cbx, float *cbz, float *ck)
+                           int ldz, float *cbx, float *cbz, float *ck, float *kap)
 {
     const size_t n = (size_t)ntx * ldz;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int z = (int)(i % ldz);
-        float bx = 0.f, bz = 0.f, kc = 0.f;
+        float bx = 0.f, bz = 0.f, kc = 0.f, ka = 0.f;
         if (z < ntz) {
             const float r0 = rho[i], r1 = rho[i + ldz], r2 = rho[i + 1], v = vp[i];
             const float sx = 0.5f * (r0 + r1), sz = 0.5f * (r0 + r2);
             if (sx != 0.f) bx = dt * __frcp_rn(sx);
             if (sz != 0.f) bz = dt * __frcp_rn(sz);
             kc = dt * r0 * v * v;
+            ka = r0 * v * v;
         }
         cbx[i] = bx;
         cbz[i] = bz;
         ck[i] = kc;
+        kap[i] = ka;
     }
 }
 
@@ -623,11 +629,12 @@ static void launch_fwd_p(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s)
 {
     const bool born = a.s0_out || a.dkappa;
     if (nw == 2) {
-        if (born) k_fwd_p<LC, 2, true><<<grid, dim3(32, 8), 0, s>>>(a);
-        else k_fwd_p<LC, 2, false><<<grid, dim3(32, 8), 0, s>>>(a);
+        if (born) k_fwd_p<LC, 2, FP_BORN><<<grid, dim3(32, 8), 0, s>>>(a);
+        else k_fwd_p<LC, 2, FP_PLAIN><<<grid, dim3(32, 8), 0, s>>>(a);
     } else {
-        if (born) k_fwd_p<LC, 1, true><<<grid, dim3(32, 8), 0, s>>>(a);
-        else k_fwd_p<LC, 1, false><<<grid, dim3(32, 8), 0, s>>>(a);
+        if (a.ds.buf) k_fwd_p<LC, 1, FP_STORE><<<grid, dim3(32, 8), 0, s>>>(a);
+        else if (born) k_fwd_p<LC, 1, FP_BORN><<<grid, dim3(32, 8), 0, s>>>(a);
+        else k_fwd_p<LC, 1, FP_PLAIN><<<grid, dim3(32, 8), 0, s>>>(a);
     }
 }
 
@@ -636,6 +643,12 @@ static void launch_bwd_1(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_1<
 
 template <int LC>
 static void launch_bwd_2(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_2<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+
+template <int LC>
+static void launch_bwd_rcv_v(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_rcv_v<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+
+template <int LC>
+static void launch_bwd_rcv_p(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_rcv_p<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
 
 template <int LC>
 static void launch_fwd_fused(const FStepArgs &a, int nw, cudaStream_t s)
@@ -709,6 +722,7 @@ struct FwdJob {
     float *s0 = nullptr;     // background p-update sums, slot it % s0_mod
     int s0_mod = 1;
     Ckpt ck{};               // background checkpoints (ck.every == 0: none)
+    DpStore ds{};            // stored source dp/dt (ds.buf == nullptr: none)
 };
 
 // device copies of the shot's wavelet(s): wav[0..nt) = rick, wav[nt..2nt) = Hilbert twin
@@ -824,7 +838,7 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
 {
     ctx->kept.valid = false;   // wave[0], strips and the wavelet buffer are overwritten
     // Born fields, S0 output and checkpoints exist on the plain kernels only
-    if (fused(ctx) && !J.dkappa && !J.s0 && !J.ck.every) return run_forward_fused(ctx, J, P);
+    if (fused(ctx) && !J.dkappa && !J.s0 && !J.ck.every && !J.ds.buf) return run_forward_fused(ctx, J, P);
     const swd_shot *s = J.shot;
     const int nt = s->nt;
     CKR(zero_wave(ctx, 0));
@@ -851,6 +865,7 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     a.s0_mod = J.s0_mod;
     a.dkappa = J.dkappa;
     a.ck = J.ck;
+    a.ds = J.ds;
     const dim3 grid = grid_blocks(ctx);
     if (J.save_strips) {
         const int slen = strip_len(ctx);
@@ -1188,7 +1203,7 @@ int swd_set_model(swd_ctx *ctx, const float *vp, const float *rho)
     CKR(grid_to_dev(ctx, F(ctx->rho), rho));
     for (auto &b : ctx->mat) CKR(ensure_grid(ctx, b, sizeof(float)));
     k_material<<<592, 256, 0, ctx->stream>>>(F(ctx->vp), F(ctx->rho), ctx->grid.dt, ctx->ntx, ctx->ntz, ctx->ldz,
-                                             F(ctx->mat[0]), F(ctx->mat[1]), F(ctx->mat[2]));
+                                             F(ctx->mat[0]), F(ctx->mat[1]), F(ctx->mat[2]), F(ctx->mat[3]));
     ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1201,6 +1216,17 @@ int swd_set_kernel_path(swd_ctx *ctx, int path)
     if (!ctx) return SWD_ERR_ARG;
     if (path != SWD_PATH_PLAIN && path != SWD_PATH_FUSED) return fail(ctx, SWD_ERR_ARG, "unknown kernel path %d", path);
     ctx->path = path;
+    return SWD_OK;
+}
+
+int swd_set_source_storage(swd_ctx *ctx, int store, int prec)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    if (store != 0 && store != 1) return fail(ctx, SWD_ERR_ARG, "source storage mode %d is not 0 or 1", store);
+    if (prec < SWD_STRIP_F32 || prec > SWD_STRIP_I16) return fail(ctx, SWD_ERR_ARG, "unknown precision %d", prec);
+    ctx->src_store = store;
+    ctx->src_prec = prec;
+    ctx->kept.valid = false;
     return SWD_OK;
 }
 
@@ -1262,8 +1288,30 @@ int swd_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, const flo
     return SWD_OK;
 }
 
-// RTM forward pass: boundary strips saved, the final state stays in wave[0] (and in the
-// second copies for the fused path) for rtm_backward_part; the shot it ran is remembered.
+// Layout and buffers of the stored dp/dt of an nt-step shot (interior columns, interior rows
+// rounded out to 4-cell chunks, one step after another).
+static int dp_store_layout(swd_ctx *ctx, int nt, DpStore *ds)
+{
+    memset(ds, 0, sizeof *ds);
+    const dim3 grid = grid_blocks(ctx);
+    const int zlo = ctx->pmlc & ~3, zhi = (ctx->ntz - ctx->pmlc + 3) & ~3;
+    ds->zlo = zlo;
+    ds->ldr = zhi - zlo;
+    ds->step = (long long)ctx->nx * ds->ldr;
+    ds->prec = ctx->src_prec;
+    ds->nblocks = grid.x * grid.y;
+    const size_t esz = ctx->src_prec == SWD_STRIP_F32 ? 4 : 2;
+    CKR(ensure(ctx, ctx->dpst, esz * (size_t)ds->step * nt));
+    ds->buf = ctx->dpst.p;
+    if (ctx->src_prec != SWD_STRIP_F32) {
+        CKR(ensure(ctx, ctx->dpsc, sizeof(float) * (size_t)ds->nblocks * nt));
+        ds->scale = F(ctx->dpsc);
+    }
+    return SWD_OK;
+}
+
+// RTM forward pass: boundary strips saved (or dp/dt stored), the final state stays in wave[0]
+// (and in the second copies for the fused path) for rtm_backward_part; the shot is remembered.
 static int rtm_forward_part(swd_ctx *ctx, const swd_shot *shot, const float *rick, float *syn)
 {
     ShotPlan P;
@@ -1273,7 +1321,9 @@ static int rtm_forward_part(swd_ctx *ctx, const swd_shot *shot, const float *ric
     FwdJob J;
     J.shot = shot;
     CKR(host_copy(ctx, J.rick, rick, nt));
-    J.save_strips = true;
+    const bool stored = ctx->src_store != 0;
+    J.save_strips = !stored;
+    if (stored) CKR(dp_store_layout(ctx, nt, &J.ds));
     CKR(ensure(ctx, ctx->seis, sizeof(float) * ntr));
     CK(cudaMemsetAsync(ctx->seis.p, 0, sizeof(float) * ntr, ctx->stream));
     J.seis_dev = F(ctx->seis);
@@ -1282,7 +1332,7 @@ static int rtm_forward_part(swd_ctx *ctx, const swd_shot *shot, const float *ric
         CKR(copy_aliases(ctx, P, F(ctx->seis), nt));
         CKR(from_dev(ctx, syn, ctx->seis.p, sizeof(float) * ntr));
     }
-    ctx->kept = swd_ctx::KeptShotState{true, shot->s_ix, shot->s_iz, shot->nt, shot->r_n, ctx->path};
+    ctx->kept = swd_ctx::KeptShotState{true, shot->s_ix, shot->s_iz, shot->nt, shot->r_n, ctx->path, stored};
     return SWD_OK;
 }
 
@@ -1296,6 +1346,7 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
     if (!k.valid || k.s_ix != shot->s_ix || k.s_iz != shot->s_iz || k.nt != shot->nt || k.r_n != shot->r_n ||
         k.path != ctx->path)
         return fail(ctx, SWD_ERR_STATE, "the backward pass needs the forward pass of the same shot just before it");
+    const bool stored = k.stored;
     ctx->kept.valid = false;   // the reconstruction runs the kept wavefield back to time 0
     ShotPlan P;
     CKR(plan_shot(ctx, shot, P));
@@ -1312,8 +1363,8 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
     } else {
         CK(cudaMemcpyAsync(rms, raw, sizeof(float) * ntr, cudaMemcpyDeviceToDevice, ctx->stream));
     }
-    // 3. backward: reconstruction + receiver back-propagation + FP64 imaging
-    const bool fz = fused(ctx);
+    // 3. backward: reconstruction (or the stored dp/dt) + receiver back-propagation + FP64 imaging
+    const bool fz = fused(ctx) && !stored;
     CKR(zero_wave(ctx, 1));
     if (fz) {
         CKR(zero_wave2(ctx, 1));
@@ -1389,6 +1440,22 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         const int kid[1] = {5};
         f.itoff = 0;
         CKR(run_steps(ctx, ctx->gbwd, &f, sizeof f, nt - 2, -1, nt - 1, 1, kid, launch));
+    } else if (stored) {
+        // receiver wavefield only; the imaging reads the dp/dt stored by the forward pass
+        b.itp = I32(ctx->ctrl);
+        CKR(dp_store_layout(ctx, nt, &b.ds));
+        auto launch = [&](int k, cudaEvent_t *ev) {
+            BwdArgs q = b;
+            q.itoff = -k;
+            if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
+            LC_DISPATCH(ctx->Lc, launch_bwd_rcv_v, q, grid, ctx->stream);
+            if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
+            LC_DISPATCH(ctx->Lc, launch_bwd_rcv_p, q, grid, ctx->stream);
+            if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
+        };
+        const int kid[2] = {2, 3};
+        b.itoff = 0;
+        CKR(run_steps(ctx, ctx->gbwd, &b, sizeof b, nt - 2, -1, nt - 1, 2, kid, launch));
     } else {
         b.itp = I32(ctx->ctrl);
         b.wavsub = F(ctx->wav);

@@ -296,3 +296,24 @@ def test_rtm_in_two_calls_equals_one(case, swd, orc):
     case.E.forward(case.shot, case.rick)       # another pass reuses the buffers
     with pytest.raises(swd.SwdError):
         case.E.rtm_backward(case.shot, data)
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-4), (3, 1e-3), (1, 3e-3), (2, 3e-2)], ids=["f32", "i16", "f16", "bf16"])
+def test_stored_source_rtm(case, swd, orc, prec, tol):
+    """RTM whose forward pass stores dp/dt (and whose backward pass propagates only the receiver
+    wavefield) against the FP64 oracle; FP32 storage also against the reconstructing engine."""
+    data = orc.forward(case.M, case.G, case.rick)["seis"]
+    flags = swd.RTM_PREPROCESS | swd.RTM_NO_STACK
+    recon = case.E.rtm_shot(case.shot, case.rick, data, flags=flags)["image_pp"]
+    case.E.set_source_storage(1, prec)
+    try:
+        got = case.E.rtm_shot(case.shot, case.rick, data, flags=flags)["image_pp"]
+    finally:
+        case.E.set_source_storage(0)
+    p = case.pmlc
+    ref = _rtm(case, orc, data, np.float64)[1][p:-p, p:-p]
+    e = rel_l2(got, ref)
+    print(f"stored dp/dt precision {prec}: image rel-L2 vs FP64 oracle {e:.3e}")
+    assert e < tol
+    if prec == 0:
+        assert rel_l2(got, recon) < 1e-5
