@@ -258,6 +258,30 @@ def run_ours(args, rank, world, dist):
     with ClockSampler(dev) as clk:
         t_val, launches, prof = timed(d_data, d_rick, d_img, d_fim, args.steps, args.warmup, profile=True)
         t_e2e, _, _ = timed(h_data, h_rick, h_img, h_fim, args.steps, max(1, args.warmup // 3))
+    stored = None
+    if not args.no_stored:
+        # the stored-source option: dp/dt kept at 16 bits by the forward pass, receiver-only
+        # backward; its speed, and its raw image against the reconstruction away from the
+        # Lc band at the interior edge (where the reconstruction reads a frozen frame)
+        I0, S0, _ = E.rtm_raw()
+        need = 2 * w.nt * w.nx * (w.nz + 8)
+        free = torch.cuda.mem_get_info()[0]
+        if need < 0.8 * free:
+            E.set_source_storage(1, swd.STRIP_I16)
+            ks = max(2, args.steps // 2)
+            t_st, _, _ = timed(d_data, d_rick, d_img, d_fim, ks, 2)
+            I1, S1, _ = E.rtm_raw()
+            E.set_source_storage(0)
+            m = w.pmlc + w.Lc
+            sl = (slice(m, -m), slice(m, -m))
+            rel = lambda a, b: float(np.linalg.norm(a[sl] - b[sl]) / np.linalg.norm(b[sl]))
+            t_st, = max_over_ranks(dist, [t_st], "cuda")
+            stored = {"value": replica_throughput(ks, world, t_st), "unit": "shots/s", "precision": "i16",
+                      "store_bytes_per_shot": int(need), "image_rel_l2_vs_reconstruction": rel(I1, I0),
+                      "illumination_rel_l2_vs_reconstruction": rel(S1, S0),
+                      "compared_on": "raw I and S, interior without the Lc band at its edge"}
+        else:
+            stored = {"skipped": f"store of {need / 1e9:.1f} GB exceeds 80% of free device memory"}
     t_val, t_e2e = max_over_ranks(dist, [t_val, t_e2e], "cuda")
     if rank != 0:
         return None
@@ -315,6 +339,7 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": launches,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
+        "stored_source": stored,
     }
 
 
@@ -660,6 +685,7 @@ def main():
     ap.add_argument("--path", type=int, default=None, help="kernel path: 0 plain (two launches per step), 1 fused")
     ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch"], default="rtm")
     ap.add_argument("--config", choices=["c2", "c5"], default="c2", help="grid of --workload rtm")
+    ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
     ap.add_argument("--ckpt-prec", choices=["f32", "f16", "bf16", "i16"], default="bf16",
                     help="checkpoint precision of --workload lsrtm")
     args = ap.parse_args()

@@ -298,22 +298,25 @@ def test_rtm_in_two_calls_equals_one(case, swd, orc):
         case.E.rtm_backward(case.shot, data)
 
 
-@pytest.mark.parametrize("prec,tol", [(0, 1e-4), (3, 1e-3), (1, 3e-3), (2, 3e-2)], ids=["f32", "i16", "f16", "bf16"])
+@pytest.mark.parametrize("prec,tol", [(0, 1e-3), (3, 1e-3), (1, 1e-3), (2, 3e-3)], ids=["f32", "i16", "f16", "bf16"])
 def test_stored_source_rtm(case, swd, orc, prec, tol):
-    """RTM whose forward pass stores dp/dt (and whose backward pass propagates only the receiver
-    wavefield) against the FP64 oracle; FP32 storage also against the reconstructing engine."""
+    """RTM whose forward pass stores dp/dt (the backward pass propagates only the receiver
+    wavefield) against the FP64 oracle of the reference's method, on the raw images I and S
+    away from the Lc-wide band at the interior edge.  In that band the reference's interior-only
+    reconstruction reads velocities of the absorbing frame frozen at the final forward state,
+    so its dp/dt there is not the forward one; the stored mode keeps the forward dp/dt, and the
+    reconstruction's error also reaches into the interior at the few 1e-4 level."""
     data = orc.forward(case.M, case.G, case.rick)["seis"]
     flags = swd.RTM_PREPROCESS | swd.RTM_NO_STACK
-    recon = case.E.rtm_shot(case.shot, case.rick, data, flags=flags)["image_pp"]
     case.E.set_source_storage(1, prec)
     try:
-        got = case.E.rtm_shot(case.shot, case.rick, data, flags=flags)["image_pp"]
+        case.E.rtm_shot(case.shot, case.rick, data, flags=flags)
+        I, S, _ = case.E.rtm_raw()
     finally:
         case.E.set_source_storage(0)
-    p = case.pmlc
-    ref = _rtm(case, orc, data, np.float64)[1][p:-p, p:-p]
-    e = rel_l2(got, ref)
-    print(f"stored dp/dt precision {prec}: image rel-L2 vs FP64 oracle {e:.3e}")
-    assert e < tol
-    if prec == 0:
-        assert rel_l2(got, recon) < 1e-5
+    sh = orc.rtm_shot(case.M, case.G, case.rick, data, dtype=np.float64)
+    m = case.pmlc + case.Lc
+    sl = (slice(m, -m), slice(m, -m))
+    eI, eS = rel_l2(I[sl], sh["img"][sl]), rel_l2(S[sl], sh["illum"][sl])
+    print(f"stored dp/dt precision {prec}: interior I {eI:.3e}, S {eS:.3e} vs the FP64 oracle")
+    assert eI < tol and eS < tol
