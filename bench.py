@@ -269,7 +269,7 @@ def run_ours(args, rank, world, dist):
         if need < 0.8 * free:
             E.set_source_storage(1, swd.STRIP_I16)
             ks = max(2, args.steps // 2)
-            t_st, _, _ = timed(d_data, d_rick, d_img, d_fim, ks, 2)
+            t_st, _, prof_st = timed(d_data, d_rick, d_img, d_fim, ks, 2, profile=True)
             I1, S1, _ = E.rtm_raw()
             E.set_source_storage(0)
             m = w.pmlc + w.Lc
@@ -279,7 +279,9 @@ def run_ours(args, rank, world, dist):
             stored = {"value": replica_throughput(ks, world, t_st), "unit": "shots/s", "precision": "i16",
                       "store_bytes_per_shot": int(need), "image_rel_l2_vs_reconstruction": rel(I1, I0),
                       "illumination_rel_l2_vs_reconstruction": rel(S1, S0),
-                      "compared_on": "raw I and S, interior without the Lc band at its edge"}
+                      "compared_on": "raw I and S, interior without the Lc band at its edge",
+                      "step_us": {k: ms / n * 1e3 for k, (ms, n) in prof_st.items() if n and k in
+                                  ("fwd_v", "fwd_p", "bwd_1", "bwd_2", "fwd_pass_step", "bwd_pass_step")}}
         else:
             stored = {"skipped": f"store of {need / 1e9:.1f} GB exceeds 80% of free device memory"}
     t_val, t_e2e = max_over_ranks(dist, [t_val, t_e2e], "cuda")

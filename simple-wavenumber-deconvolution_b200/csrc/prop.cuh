@@ -43,11 +43,13 @@ struct Mat {
 // dp/dt of the source wavefield, stored by the forward pass on the interior for a backward
 // pass that does not reconstruct the source wavefield.  Layout [step][x - pmlc][z - zlo] with
 // row pitch ldr (the interior rows rounded out to whole 4-cell chunks); prec 0 f32, else a
-// 16-bit code of enc16 with one scale (max |dp/dt|) per (step, 128 x 8 block).
+// 16-bit code of enc16 with one scale (max |dp/dt|) per (step, warp of cell4), i.e. per 128
+// rows of one column, so no block-wide reduction is needed.  Stores and loads are streaming
+// (evict-first): each step's values are read once, by the backward pass.
 struct DpStore {
     void *buf;       // nullptr: not stored
     float *scale;
-    int prec, zlo, ldr, nblocks;
+    int prec, zlo, ldr, nwarps;
     long long step;  // elements per step
 };
 
@@ -482,8 +484,13 @@ __device__ __forceinline__ long long dp_offset(const DpStore &ds, const Geo &g, 
     return (long long)(x - g.pmlc) * ds.ldr + (z0 - ds.zlo);
 }
 
-// Called by every thread of a (32, 8) block: dp/dt = kap * S of the interior cells of its
-// chunk (zero on the chunk's other cells), block max for 16-bit codes, then the store.
+__device__ __forceinline__ int warp_slot()
+{
+    return (blockIdx.y * gridDim.x + blockIdx.x) * (blockDim.y) + threadIdx.y;
+}
+
+// dp/dt = kap * S of the interior cells of this thread's chunk (zero on the chunk's other
+// cells), the warp's max for 16-bit codes, then a streaming store.  Whole warps call it.
 __device__ __forceinline__ void store_dpdt(const DpStore &ds, const Mat &m, const Geo &g, int it, int x, int z0,
                                            bool in, float4 s)
 {
@@ -497,24 +504,18 @@ __device__ __forceinline__ void store_dpdt(const DpStore &ds, const Mat &m, cons
     }
     const size_t base = (size_t)it * ds.step;
     if (ds.prec == 0) {
-        if (off >= 0) st4((float *)ds.buf + base + off, dp);
+        if (off >= 0) __stcs(reinterpret_cast<float4 *>((float *)ds.buf + base + off), dp);
         return;
     }
-    __shared__ float smax;
-    if (threadIdx.x == 0 && threadIdx.y == 0) smax = 0.f;
-    __syncthreads();
-    float v = fmaxf(fmaxf(fabsf(dp.x), fabsf(dp.y)), fmaxf(fabsf(dp.z), fabsf(dp.w)));
+    float mx = fmaxf(fmaxf(fabsf(dp.x), fabsf(dp.y)), fmaxf(fabsf(dp.z), fabsf(dp.w)));
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (threadIdx.x == 0 && v > 0.f) atomicMax((int *)&smax, __float_as_int(v));
-    __syncthreads();
-    const float mx = smax;
-    if (threadIdx.x == 0 && threadIdx.y == 0) ds.scale[(size_t)it * ds.nblocks + blockIdx.y * gridDim.x + blockIdx.x] = mx;
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (threadIdx.x == 0) __stcs(ds.scale + (size_t)it * ds.nwarps + warp_slot(), mx);
     if (off >= 0) {
         ushort4 h;
         h.x = enc16(dp.x, mx, ds.prec); h.y = enc16(dp.y, mx, ds.prec);
         h.z = enc16(dp.z, mx, ds.prec); h.w = enc16(dp.w, mx, ds.prec);
-        *reinterpret_cast<ushort4 *>((unsigned short *)ds.buf + base + off) = h;
+        __stcs(reinterpret_cast<ushort4 *>((unsigned short *)ds.buf + base + off), h);
     }
 }
 
@@ -524,9 +525,9 @@ __device__ __forceinline__ float4 load_dpdt(const DpStore &ds, const Geo &g, int
     const long long off = dp_offset(ds, g, x, z0);
     if (off < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
     const size_t base = (size_t)it * ds.step;
-    if (ds.prec == 0) return ld4((const float *)ds.buf + base + off);
-    const float mx = ds.scale[(size_t)it * ds.nblocks + blockIdx.y * gridDim.x + blockIdx.x];
-    const ushort4 h = *reinterpret_cast<const ushort4 *>((const unsigned short *)ds.buf + base + off);
+    if (ds.prec == 0) return __ldcs(reinterpret_cast<const float4 *>((const float *)ds.buf + base + off));
+    const float mx = __ldcs(ds.scale + (size_t)it * ds.nwarps + warp_slot());
+    const ushort4 h = __ldcs(reinterpret_cast<const ushort4 *>((const unsigned short *)ds.buf + base + off));
     return make_float4(dec16(h.x, mx, ds.prec), dec16(h.y, mx, ds.prec), dec16(h.z, mx, ds.prec), dec16(h.w, mx, ds.prec));
 }
 
@@ -557,7 +558,7 @@ __global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
 }
 
 template <int LC, int NW, int MODE, bool BATCH = false>
-__global__ void __launch_bounds__(256, (NW == 1 && MODE == FP_PLAIN && !BATCH && LC <= 4) ? 5 : 1)
+__global__ void __launch_bounds__(256, (NW == 1 && MODE != FP_BORN && !BATCH && LC <= 4) ? 5 : 1)
     k_fwd_p(const FwdArgs a0)
 {
     constexpr bool BORN = MODE == FP_BORN;
@@ -774,7 +775,7 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
 }
 
 template <int LC, bool BATCH = false>
-__global__ void __launch_bounds__(256) k_bwd_2(const BwdArgs a0)
+__global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_2(const BwdArgs a0)
 {
     BwdArgs a = a0;
     int it = *a.itp + a.itoff;
@@ -884,7 +885,7 @@ __global__ void __launch_bounds__(256) k_bwd_rcv_v(const BwdArgs a)
 }
 
 template <int LC>
-__global__ void __launch_bounds__(256) k_bwd_rcv_p(const BwdArgs a)
+__global__ void __launch_bounds__(256, 5) k_bwd_rcv_p(const BwdArgs a)
 {
     const int it = *a.itp + a.itoff;
     int x, z0;

@@ -1299,12 +1299,12 @@ static int dp_store_layout(swd_ctx *ctx, int nt, DpStore *ds)
     ds->ldr = zhi - zlo;
     ds->step = (long long)ctx->nx * ds->ldr;
     ds->prec = ctx->src_prec;
-    ds->nblocks = grid.x * grid.y;
+    ds->nwarps = grid.x * grid.y * 8;   // (32, 8) blocks of cell4
     const size_t esz = ctx->src_prec == SWD_STRIP_F32 ? 4 : 2;
     CKR(ensure(ctx, ctx->dpst, esz * (size_t)ds->step * nt));
     ds->buf = ctx->dpst.p;
     if (ctx->src_prec != SWD_STRIP_F32) {
-        CKR(ensure(ctx, ctx->dpsc, sizeof(float) * (size_t)ds->nblocks * nt));
+        CKR(ensure(ctx, ctx->dpsc, sizeof(float) * (size_t)ds->nwarps * nt));
         ds->scale = F(ctx->dpsc);
     }
     return SWD_OK;
