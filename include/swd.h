@@ -217,6 +217,10 @@ typedef struct {
     int psfwinx, psfwinz, filterwinx, filterwinz, snapwinx, snapwinz;
     float epsilon;
     int fft_nx, fft_nz;
+    /* 0: the nearest lattice PSF (the reference's rule, :586-598); 1: bilinear interpolation
+     * of the four lattice PSFs around the window centre, within the same clamped lattice range
+     * (project option: the reference declares but does not implement it, headpsf.h:166-167) */
+    int psf_interp;
 } swd_decon_params;
 int swd_decon_geometry(const swd_decon_params *p, int *windows, int *fft_nx, int *fft_nz);
 int swd_decon(swd_ctx *ctx, const swd_decon_params *p, const float *migreal,

@@ -400,6 +400,25 @@ int orc_decon_geometry(const orc_decon_params *p, int *out)
     return 0;
 }
 
+/* Bracketing lattice points of a window-centre coordinate for PSF interpolation (project
+ * option): f0 = floor((c - h)/w) and f1 = f0 + 1 clamped to [3, n - 4] (the reference's
+ * range), t the fractional position between them in [0, 1] (0 when they coincide). */
+static void orc_psf_bracket(int c, int h, int w, int n, int *f0, int *f1, double *t)
+{
+    const double pos = (double)(c - h) / (double)w;
+    int a = (int)floor(pos);
+    if (a < 3) a = 3;
+    if (a > n - 4) a = n - 4;
+    int b = a + 1 > n - 4 ? n - 4 : a + 1;
+    double u = pos - (double)a;
+    if (u < 0.0) u = 0.0;
+    if (u > 1.0) u = 1.0;
+    if (b == a) u = 0.0;
+    *f0 = a;
+    *f1 = b;
+    *t = u;
+}
+
 int orc_decon(const orc_decon_params *p, const float *migreal, const float *migpsf,
               float *out_dec, float *out_coef, int nthreads)
 {
@@ -473,19 +492,39 @@ int orc_decon(const orc_decon_params *p, const float *migreal, const float *migp
             for (size_t ip = 0; ip < nbuf; ip++) snapm[2 * ip] /= pp_max;
             orc_fft2(g.n0, g.n1, snapm, -1);
 
-            int ixf = (ix - g.halfpsfwx) / p->psfwinx;
-            int izf = (iz - g.halfpsfwz) / p->psfwinz;
-            if (ixf <= 2) ixf = 3;
-            if (ixf >= g.nxwpsf - 3) ixf = g.nxwpsf - 4;
-            if (izf <= 2) izf = 3;
-            if (izf >= g.nzwpsf - 3) izf = g.nzwpsf - 4;
-            int ixp = g.halfpsfwx + ixf * p->psfwinx;
-            int izp = g.halfpsfwz + izf * p->psfwinz;
-            for (int ixx = 0; ixx < p->psfwinx; ixx++)
-                for (int izz = 0; izz < p->psfwinz; izz++) {
-                    int ip = ixx * g.FZ + izz;
-                    snapsf[2 * ip] = migpsff[(size_t)(ixp + ixx - g.halfpsfwx) * nzp + (izp + izz - g.halfpsfwz)];
-                }
+            if (!p->psf_interp) {
+                int ixf = (ix - g.halfpsfwx) / p->psfwinx;
+                int izf = (iz - g.halfpsfwz) / p->psfwinz;
+                if (ixf <= 2) ixf = 3;
+                if (ixf >= g.nxwpsf - 3) ixf = g.nxwpsf - 4;
+                if (izf <= 2) izf = 3;
+                if (izf >= g.nzwpsf - 3) izf = g.nzwpsf - 4;
+                int ixp = g.halfpsfwx + ixf * p->psfwinx;
+                int izp = g.halfpsfwz + izf * p->psfwinz;
+                for (int ixx = 0; ixx < p->psfwinx; ixx++)
+                    for (int izz = 0; izz < p->psfwinz; izz++) {
+                        int ip = ixx * g.FZ + izz;
+                        snapsf[2 * ip] = migpsff[(size_t)(ixp + ixx - g.halfpsfwx) * nzp + (izp + izz - g.halfpsfwz)];
+                    }
+            } else {
+                /* project option: bilinear weights of the two lattice points bracketing the
+                 * window centre on each axis, inside the clamped range [3, nwpsf-4] */
+                int fx0, fx1, fz0, fz1;
+                double tx, tz;
+                orc_psf_bracket(ix, g.halfpsfwx, p->psfwinx, g.nxwpsf, &fx0, &fx1, &tx);
+                orc_psf_bracket(iz, g.halfpsfwz, p->psfwinz, g.nzwpsf, &fz0, &fz1, &tz);
+                const int xa = g.halfpsfwx + fx0 * p->psfwinx - g.halfpsfwx, xb = g.halfpsfwx + fx1 * p->psfwinx - g.halfpsfwx;
+                const int za = g.halfpsfwz + fz0 * p->psfwinz - g.halfpsfwz, zb = g.halfpsfwz + fz1 * p->psfwinz - g.halfpsfwz;
+                for (int ixx = 0; ixx < p->psfwinx; ixx++)
+                    for (int izz = 0; izz < p->psfwinz; izz++) {
+                        const double a = migpsff[(size_t)(xa + ixx) * nzp + za + izz];
+                        const double b = migpsff[(size_t)(xb + ixx) * nzp + za + izz];
+                        const double c = migpsff[(size_t)(xa + ixx) * nzp + zb + izz];
+                        const double d = migpsff[(size_t)(xb + ixx) * nzp + zb + izz];
+                        snapsf[2 * (ixx * g.FZ + izz)] =
+                            (float)((1.0 - tz) * ((1.0 - tx) * a + tx * b) + tz * ((1.0 - tx) * c + tx * d));
+                    }
+            }
             float psf_max = 0.0;
             for (size_t ip = 0; ip < nbuf; ip++) psf_max += fabs(snapsf[2 * ip]);
             for (size_t ip = 0; ip < nbuf; ip++) snapsf[2 * ip] /= psf_max;

@@ -104,6 +104,7 @@ typedef struct {
     int psfwinx, psfwinz, filterwinx, filterwinz, snapwinx, snapwinz;
     float epsilon;
     int fft_n0, fft_n1;
+    int psf_interp;   /* 1: bilinear interpolation of the lattice PSFs (project option) */
 } orc_decon_params;
 
 int orc_decon_geometry(const orc_decon_params *p, int *out /* 16 ints, see swd_oracle.c */);

@@ -30,7 +30,24 @@ struct DeconGeo {
     int FX, FZ, n0, n1, midpx, midpz, ocx, ocz;
     int outwinx, outwinz, halfoutwx, halfoutwz, stepwinx, stepwinz, stepnumx, stepnumz, totalnum, nxp, nzp;
     float epsilon;
+    int psf_interp;   // 1: bilinear interpolation of the lattice PSFs (project option)
 };
+
+// Bracketing lattice points of a window-centre coordinate for PSF interpolation: f0 =
+// floor((c - h)/w) and f1 = f0 + 1 clamped to [3, n - 4] (the reference's lattice range), t the
+// fractional position in [0, 1] (0 when they coincide).
+__device__ __forceinline__ void psf_bracket(int c, int h, int w, int n, int &f0, int &f1, double &t)
+{
+    const double pos = (double)(c - h) / (double)w;
+    int a = (int)floor(pos);
+    a = a < 3 ? 3 : (a > n - 4 ? n - 4 : a);
+    const int b = a + 1 > n - 4 ? n - 4 : a + 1;
+    double u = pos - (double)a;
+    u = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
+    f0 = a;
+    f1 = b;
+    t = b == a ? 0.0 : u;
+}
 
 // expanded-image read (edge replication of :303-339): clamp to the last row/column
 __device__ __forceinline__ float img_at(const float *__restrict__ im, int nx, int nz, int ix, int iz)
@@ -97,6 +114,24 @@ __global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *_
     if (izf <= 2) izf = 3;
     if (izf >= g.nzwpsf - 3) izf = g.nzwpsf - 4;
     const int ixp = g.halfpsfwx + ixf * g.psfwinx, izp = g.halfpsfwz + izf * g.psfwinz;
+    // PSF patch value: the nearest lattice PSF, or (psf_interp) the bilinear blend of the four
+    // around the window centre, formed in double without contraction and rounded to float
+    int fx0 = 0, fx1 = 0, fz0 = 0, fz1 = 0;
+    double tx = 0.0, tz = 0.0;
+    if (g.psf_interp) {
+        psf_bracket(ix, g.halfpsfwx, g.psfwinx, g.nxwpsf, fx0, fx1, tx);
+        psf_bracket(iz, g.halfpsfwz, g.psfwinz, g.nzwpsf, fz0, fz1, tz);
+    }
+    auto psf_val = [&](int ixx, int izz) -> float {
+        if (!g.psf_interp) return img_at(psf, g.nx, g.nz, ixp + ixx - g.halfpsfwx, izp + izz - g.halfpsfwz);
+        const int xa = fx0 * g.psfwinx + ixx, xb = fx1 * g.psfwinx + ixx;
+        const int za = fz0 * g.psfwinz + izz, zb = fz1 * g.psfwinz + izz;
+        const double a = img_at(psf, g.nx, g.nz, xa, za), b = img_at(psf, g.nx, g.nz, xb, za);
+        const double c = img_at(psf, g.nx, g.nz, xa, zb), d = img_at(psf, g.nx, g.nz, xb, zb);
+        const double s1 = __dadd_rn(__dmul_rn(1.0 - tx, a), __dmul_rn(tx, b));
+        const double s2 = __dadd_rn(__dmul_rn(1.0 - tx, c), __dmul_rn(tx, d));
+        return (float)__dadd_rn(__dmul_rn(1.0 - tz, s1), __dmul_rn(tz, s2));
+    };
 
     for (int j = tid; j < n; j += nthr) Z[j] = make_float2(0.f, 0.f);
     for (int j = tid; j < g.n0; j += nthr) {
@@ -125,7 +160,7 @@ __global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *_
         float ps = 0.0f;
         for (int ixx = 0; ixx < g.psfwinx; ixx++)
             for (int izz = 0; izz < g.psfwinz; izz++)
-                ps = (float)((double)ps + fabs((double)img_at(psf, g.nx, g.nz, ixp + ixx - g.halfpsfwx, izp + izz - g.halfpsfwz)));
+                ps = (float)((double)ps + fabs((double)psf_val(ixx, izz)));
         s_psfmax = ps;
     }
     if (tid == 64) s_fmax = 0u;
@@ -141,7 +176,7 @@ __global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *_
     }
     for (int j = tid; j < g.psfwinx * g.psfwinz; j += nthr) {
         const int ixx = j / g.psfwinz, izz = j % g.psfwinz;
-        Z[ixx * g.FZ + izz].y = (float)((double)img_at(psf, g.nx, g.nz, ixp + ixx - g.halfpsfwx, izp + izz - g.halfpsfwz) / psm);
+        Z[ixx * g.FZ + izz].y = (float)((double)psf_val(ixx, izz) / psm);
     }
     __syncthreads();
     dft2(Z, tw0, tw1, g.n0, g.n1, -1);

@@ -6,7 +6,8 @@
 // writes the reference's diagnostics and the deconvolved image (the decon file named in
 // parameter.txt) plus migration_coef.{bin,txt}, start.flag and end.flag into ./output/.
 // All windows run as one batched launch on the GPU (swd_decon).
-// Extensions (parameter.txt lines `swd.key = value`): device, fft_nx / fft_nz (zero-padded
+// Extensions (parameter.txt lines `swd.key = value`): device, psf_interp (1: bilinear blend of
+// the lattice PSFs around each window, a project option), fft_nx / fft_nz (zero-padded
 // FFT size instead of filterwin + psfwin - 1).
 #include <math.h>
 #include "common.h"
@@ -78,7 +79,7 @@ int main(int, char **)
     printf("vp_max = %f\n", vp_max);
 
     swd_decon_params p{nx, nz, psfwinx, psfwinz, filterwinx, filterwinz, snapwinx, snapwinz, epsilon,
-                       ext_int(ext, "fft_nx", 0), ext_int(ext, "fft_nz", 0)};
+                       ext_int(ext, "fft_nx", 0), ext_int(ext, "fft_nz", 0), ext_int(ext, "psf_interp", 0)};
     int windows = 0, fx = 0, fz = 0;
     if (swd_decon_geometry(&p, &windows, &fx, &fz) != SWD_OK) {
         printf("Invalid deconvolution window geometry\n");

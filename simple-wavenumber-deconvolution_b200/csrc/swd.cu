@@ -988,6 +988,8 @@ static int decon_geo(const swd_decon_params *p, DeconGeo &g)
     g.nx = p->nx; g.nz = p->nz;
     g.psfwinx = p->psfwinx; g.psfwinz = p->psfwinz; g.filterwinx = p->filterwinx; g.filterwinz = p->filterwinz;
     g.snapwinx = p->snapwinx; g.snapwinz = p->snapwinz; g.epsilon = p->epsilon;
+    if (p->psf_interp != 0 && p->psf_interp != 1) return SWD_ERR_ARG;
+    g.psf_interp = p->psf_interp;
     g.halfpsfwx = p->psfwinx / 2; g.halfpsfwz = p->psfwinz / 2;
     g.halfltwx = p->filterwinx / 2; g.halfltwz = p->filterwinz / 2;
     g.nzwpsf = (int)ceil(1.0 * p->nz / p->psfwinz);

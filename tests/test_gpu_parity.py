@@ -320,3 +320,21 @@ def test_stored_source_rtm(case, swd, orc, prec, tol):
     eI, eS = rel_l2(I[sl], sh["img"][sl]), rel_l2(S[sl], sh["illum"][sl])
     print(f"stored dp/dt precision {prec}: interior I {eI:.3e}, S {eS:.3e} vs the FP64 oracle")
     assert eI < tol and eS < tol
+
+
+def test_decon_psf_interpolation_matches_oracle(swd, orc):
+    """The bilinear PSF interpolation option against the oracle's restatement of it, and a
+    check that it differs from the nearest-PSF result where the lattice PSFs differ."""
+    import importlib.util
+    from conftest import GOLDEN
+    spec = importlib.util.spec_from_file_location("mk", GOLDEN / "make_golden.py")
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    nx, nz, psf, flt, snap, eps, seed = mk.DECON_CASES[0]
+    mig, psfimg, _ = mk.synthetic_decon_inputs(nx, nz, psf, seed)
+    near, _ = swd.decon(mig, psfimg, psf, flt, snap, eps)
+    got, coef = swd.decon(mig, psfimg, psf, flt, snap, eps, psf_interp=1)
+    ref, ref_coef = orc.decon(nx, nz, mig, psfimg, psf, flt, snap, eps, psf_interp=1)
+    assert np.array_equal(coef, ref_coef)
+    assert rel_l2(got, ref) < TOL_DECON
+    assert rel_l2(got, near) > 1e-6
