@@ -45,6 +45,7 @@ extern "C" {
 #define SWD_RTM_PREPROCESS 1u     /* apply rms = -int int d dt dt to the data first (reference default) */
 #define SWD_RTM_ILLUM_RCV 2u      /* also accumulate the receiver illumination R = sum p_r^2 */
 #define SWD_RTM_NO_STACK 4u       /* do not add this shot's filtered image to the stack */
+#define SWD_RTM_CIG 8u            /* also accumulate angle-domain common-image gathers (swd_set_cig) */
 
 typedef struct swd_ctx swd_ctx;
 
@@ -138,6 +139,15 @@ int swd_rtm_shot(swd_ctx *ctx, const swd_shot *shot, const float *rick, const fl
 int swd_rtm_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, float *syn);
 int swd_rtm_backward(swd_ctx *ctx, const swd_shot *shot, const float *data, unsigned flags,
                      float *image_pp, float *image_src, float *fimage);
+/* Angle-domain common-image gathers of the reference's Poynting-vector kernel
+ * (sum_image_GPU_kernel_imageCIG, acoustic_HLVSPRTMLc.cu:819-905, declared and allocated by the
+ * reference but never launched): with SWD_RTM_CIG, every backward step adds p_s*p_r into
+ * 1-degree reflection-angle bins 2 .. thetan-1 of each interior cell, the angle taken from the
+ * source and receiver Poynting vectors averaged over delt steps (the reference host uses
+ * thetan = 10, delt = 1).  Plain kernel path and reconstructed source only.  swd_rtm_cig copies
+ * the last shot's gathers, nx*nz*thetan floats with the angle fastest. */
+int swd_set_cig(swd_ctx *ctx, int thetan, int delt);
+int swd_rtm_cig(swd_ctx *ctx, float *cig);
 /* raw accumulators of the last shot on the padded grid: I, S (and R if accumulated), FP64 */
 int swd_rtm_raw(swd_ctx *ctx, double *image, double *illum_src, double *illum_rcv);
 /* the stacked image nx*nz, optionally with the reference's edge zeroing

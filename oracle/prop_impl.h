@@ -285,9 +285,46 @@ void FN(orc_preprocess)(int nrec, int nt, float dtf, const float *d, T *rms)
     free(frms);
 }
 
+/* Angle-domain common-image gathers of one backward step (sum_image_GPU_kernel_imageCIG,
+ * acoustic_HLVSPRTMLc.cu:819-905; the reference never launches it): Poynting vectors -p*v of
+ * the source and receiver wavefields, their dot product and magnitude product kept over the
+ * last delt steps, the reflection half-angle ftheta = 0.5*acos(dot/mag) in degrees, and
+ * p_s*p_r spread over the five 1-degree bins around it with weights exp(-ii^2/18); bins < 2 and
+ * >= thetan are dropped, as are cells whose angle is undefined (zero magnitude).  Float
+ * arithmetic with the reference's mixed float/double expressions. */
+static void FN(cig_step)(const FN(orc_mdl) *M, const FN(orc_fld) *s, const FN(orc_fld) *r, int it, int nt, int thetan,
+                         int delt, float *ring, float *cig)
+{
+    const int ntx = M->ntx, ntz = M->ntz, pmlc = M->pmlc;
+    const size_t ntp = (size_t)ntx * ntz;
+    for (int ix = pmlc; ix <= ntx - pmlc - 1; ix++)
+        for (int iz = pmlc; iz <= ntz - pmlc - 1; iz++) {
+            const size_t ip = (size_t)ix * ntz + iz;
+            const float ps = (float)s->p[ip], pr = (float)r->p[ip];
+            const float fx = -ps * (float)s->vx[ip], fz = -ps * (float)s->vz[ip];
+            const float fxr = -pr * (float)r->vx[ip], fzr = -pr * (float)r->vz[ip];
+            ring[(size_t)(it % delt) * 2 * ntp + ip] = fx * fxr + fz * fzr;
+            ring[((size_t)(it % delt) * 2 + 1) * ntp + ip] = sqrtf(fx * fx + fz * fz) * sqrtf(fxr * fxr + fzr * fzr);
+            if (nt - 2 - it + 1 < delt) continue;
+            float pre = 0.0f, pst = 0.0f;
+            for (int ii = 0; ii < delt; ii++) {
+                pre += ring[(size_t)ii * 2 * ntp + ip];
+                pst += ring[((size_t)ii * 2 + 1) * ntp + ip];
+            }
+            const float tht = pre / pst;
+            const float ftheta = (float)(0.5 * acosf(tht) * 180.0 / 3.1415926);
+            if (!(ftheta == ftheta)) continue;   /* undefined angle */
+            for (int ii = -2; ii <= 2; ii++) {
+                const int itheta = (int)ceilf((float)(ftheta + ii - 0.5));
+                const float betaf = (float)(1.0 * ii * ii / (2.0 * 9.0));
+                if (itheta >= 2 && itheta < thetan) cig[ip * thetan + itheta] += ps * pr * expf(-betaf);
+            }
+        }
+}
+
 void FN(orc_rtm_backward)(const orc_model *m, const orc_geom *g, const float *rick,
                           const T *rms, const T *strips, const T *final_state,
-                          T *img, T *illum_s, T *illum_r)
+                          T *img, T *illum_s, T *illum_r, int thetan, int delt, float *cig)
 {
     FN(orc_mdl) M;
     FN(mdl_init)(&M, m);
@@ -307,6 +344,8 @@ void FN(orc_rtm_backward)(const orc_model *m, const orc_geom *g, const float *ri
     const size_t src = (size_t)g->s_ix * ntz + g->s_iz;
     const T odx = (T)(1.0 / (double)m->dx), odz = (T)(1.0 / (double)m->dz);
     const T mdt = -M.dt;
+    float *ring = cig ? (float *)calloc((size_t)2 * delt * ntp, sizeof(float)) : NULL;
+    if (cig) memset(cig, 0, sizeof(float) * ntp * thetan);
     for (int it = nt - 2; it >= 0; it--) {
         /* source wavefield: p (interior, -dt) and dp_dt -- fdtd_2d_GPU_kernel_p_backward :434-485 */
 #pragma omp parallel for schedule(static)
@@ -358,7 +397,9 @@ void FN(orc_rtm_backward)(const orc_model *m, const orc_geom *g, const float *ri
                 illum_s[ip] += dpdt[ip] * dpdt[ip];
                 if (illum_r) illum_r[ip] += r.p[ip] * r.p[ip];
             }
+        if (cig) FN(cig_step)(&M, &s, &r, it, nt, thetan, delt, ring, cig);
     }
+    free(ring);
     free(dpdt);
     FN(fld_free)(&s);
     FN(fld_free)(&r);

@@ -85,7 +85,8 @@ def lib():
                                                        _i32p, _i32p, tp, tp]
             getattr(L, f"orc_preprocess_{sfx}").argtypes = [C.c_int, C.c_int, C.c_float, _f32p, tp]
             getattr(L, f"orc_rtm_backward_{sfx}").argtypes = [C.POINTER(OrcModel), C.POINTER(OrcGeom), _f32p, tp, tp,
-                                                              tp, tp, tp, C.c_void_p]
+                                                              tp, tp, tp, C.c_void_p, C.c_int, C.c_int,
+                                                              C.c_void_p]
             getattr(L, f"orc_rtm_post_{sfx}").argtypes = [C.POINTER(OrcModel), tp, tp, tp, tp]
             getattr(L, f"orc_born_{sfx}").argtypes = [C.POINTER(OrcModel), C.POINTER(OrcGeom), _f32p, _f32p, tp]
             getattr(L, f"orc_born_adjoint_{sfx}").argtypes = [C.POINTER(OrcModel), C.POINTER(OrcGeom), _f32p, _f32p, tp]
@@ -239,15 +240,18 @@ def preprocess(d, dt, dtype=np.float32):
     return out
 
 
-def rtm_backward(model: Model, geom: Geom, rick, rms, strips, final, dtype=np.float32, illum_r=False):
+def rtm_backward(model: Model, geom: Geom, rick, rms, strips, final, dtype=np.float32, illum_r=False, cig=None):
+    """cig = (thetan, delt) also returns the angle gathers (ntx, ntz, thetan) as a 4th value."""
     sfx = "f32" if dtype == np.float32 else "f64"
     shp = (model.ntx, model.ntz)
     img, s = np.zeros(shp, dtype), np.zeros(shp, dtype)
     r = np.zeros(shp, dtype) if illum_r else None
+    thetan, delt = cig if cig else (0, 1)
+    g = np.zeros(shp + (thetan,), np.float32) if cig else None
     getattr(lib(), f"orc_rtm_backward_{sfx}")(C.byref(model.s), C.byref(geom.s), np.ascontiguousarray(rick, np.float32),
                                               np.ascontiguousarray(rms, dtype), np.ascontiguousarray(strips, dtype),
-                                              np.ascontiguousarray(final, dtype), img, s, _ptr(r))
-    return img, s, r
+                                              np.ascontiguousarray(final, dtype), img, s, _ptr(r), thetan, delt, _ptr(g))
+    return (img, s, r, g) if cig else (img, s, r)
 
 
 def rtm_post(model: Model, img, illum, dtype=np.float32):
@@ -266,12 +270,16 @@ def edge_zero(img, Lc):
     return a
 
 
-def rtm_shot(model: Model, geom: Geom, rick, data, dtype=np.float32):
-    """One reference RTM shot: forward with strips -> -integral-integral data -> backward."""
+def rtm_shot(model: Model, geom: Geom, rick, data, dtype=np.float32, cig=None):
+    """One reference RTM shot: forward with strips -> -integral-integral data -> backward;
+    cig = (thetan, delt) adds the angle gathers under key "cig"."""
     fw = forward(model, geom, rick, strips=True, final=True, dtype=dtype)
     rms = preprocess(data, model.dt, dtype)
-    img, ill, _ = rtm_backward(model, geom, rick, rms, fw["strips"], fw["final"], dtype)
-    return dict(img=img, illum=ill, syn=fw["seis"], rms=rms)
+    out = rtm_backward(model, geom, rick, rms, fw["strips"], fw["final"], dtype, cig=cig)
+    res = dict(img=out[0], illum=out[1], syn=fw["seis"], rms=rms)
+    if cig:
+        res["cig"] = out[3]
+    return res
 
 
 def decon(nx, nz, migreal, migpsf, psfwin, filterwin, snapwin, epsilon, fft_n=(0, 0), nthreads=0, psf_interp=0):

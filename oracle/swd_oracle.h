@@ -78,7 +78,8 @@ int orc_strip_len(const orc_model *m);
        (acoustic_HLVSPRTMLc.cu:434-817,1073-1148) */                                        \
     void orc_rtm_backward_##S(const orc_model *m, const orc_geom *g, const float *rick,     \
                               const T *rms, const T *strips, const T *final_state,          \
-                              T *img, T *illum_s, T *illum_r);                              \
+                              T *img, T *illum_s, T *illum_r,                               \
+                              int thetan, int delt, float *cig /* nullable */);             \
     /* per-shot normalisation + -vp^2 Laplacian (acoustic_HLVSPRTMC.cpp:663-743) */          \
     void orc_rtm_post_##S(const orc_model *m, const T *img, const T *illum_s,               \
                           T *img_norm, T *fimage);                                          \

@@ -27,7 +27,7 @@ LIB_PATH = PKG_DIR / "libswd.so"
 SWD_OK, SWD_ERR_ARG, SWD_ERR_CUDA, SWD_ERR_ALLOC, SWD_ERR_STATE, SWD_ERR_DEVICE = range(6)
 STRIP_F32, STRIP_F16, STRIP_BF16, STRIP_I16 = 0, 1, 2, 3
 PATH_PLAIN, PATH_FUSED = 0, 1
-RTM_PREPROCESS, RTM_ILLUM_RCV, RTM_NO_STACK = 1, 2, 4
+RTM_PREPROCESS, RTM_ILLUM_RCV, RTM_NO_STACK, RTM_CIG = 1, 2, 4, 8
 OPT_GRAPHS, OPT_BATCH, OPT_BATCH_TUNED = 1, 2, 3
 
 
@@ -86,6 +86,8 @@ def lib():
         L.swd_set_strip_precision.argtypes = [vp, C.c_int]
         L.swd_set_kernel_path.argtypes = [vp, C.c_int]
         L.swd_set_source_storage.argtypes = [vp, C.c_int, C.c_int]
+        L.swd_set_cig.argtypes = [vp, C.c_int, C.c_int]
+        L.swd_rtm_cig.argtypes = [vp, vp]
         L.swd_forward.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, vp, vp]
         L.swd_rtm_shot.argtypes = [vp, C.POINTER(Shot), vp, vp, C.c_uint, vp, vp, vp, vp]
         L.swd_rtm_raw.argtypes = [vp, vp, vp, vp]
@@ -358,6 +360,18 @@ class Engine:
         self._ck(lib().swd_rtm_backward(self._h, C.byref(sh), _ptr(d), flags, _ptr(outs.get("image_pp")),
                                         _ptr(outs.get("image_src")), _ptr(outs.get("fimage"))))
         return outs
+
+    def set_cig(self, thetan=10, delt=1):
+        """Angle gathers for RTM shots run with flags | RTM_CIG: thetan 1-degree bins, Poynting
+        vectors averaged over delt steps."""
+        self._ck(lib().swd_set_cig(self._h, thetan, delt))
+        self._cig_thetan = thetan
+
+    def rtm_cig(self):
+        """The last shot's angle gathers, (nx, nz, thetan) float32."""
+        out = np.zeros((self.nx, self.nz, self._cig_thetan), np.float32)
+        self._ck(lib().swd_rtm_cig(self._h, _ptr(out)))
+        return out
 
     def rtm_raw(self, rcv=False):
         shp = (self.ntx, self.ntz)

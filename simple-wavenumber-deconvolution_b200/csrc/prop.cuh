@@ -940,4 +940,55 @@ __global__ void __launch_bounds__(256, 5) k_bwd_rcv_p(const BwdArgs a)
     }
 }
 
+// ------------------------------------------------------------------------------------
+// Angle-domain common-image gathers (sum_image_GPU_kernel_imageCIG, acoustic_HLVSPRTMLc.cu:
+// 819-905, which the reference never launches), one launch per backward step after k_bwd_2:
+// Poynting vectors -p*v of the source and receiver wavefields, their dot and magnitude
+// products over the last delt steps (a ring of delt slots), the reflection half-angle
+// 0.5*acos(dot/mag) in degrees, and p_s*p_r spread over the five 1-degree bins around it with
+// weights exp(-ii^2/18) (bins < 2 and >= thetan dropped; cells with an undefined angle
+// skipped).  Float arithmetic without contraction, the reference's mixed float/double angle.
+// ------------------------------------------------------------------------------------
+struct CigArgs {
+    Geo g;
+    Wave s, r;           // p, vx, vz of the source and receiver wavefields after the step
+    const int *itp;      // time index = *itp + itoff
+    int itoff, nt, thetan, delt;
+    float *ring;         // [delt][2][ntx*ldz]
+    float *cig;          // [ntx*ldz][thetan]
+};
+
+__global__ void __launch_bounds__(256) k_cig(const CigArgs a)
+{
+    const int it = *a.itp + a.itoff;
+    const Geo &g = a.g;
+    const int z = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
+    if (x >= g.ntx || z >= g.ntz || !interior(x, z, g)) return;
+    const size_t fs = (size_t)g.ntx * g.ldz, ip = (size_t)x * g.ldz + z;
+    const float ps = a.s.p[ip], pr = a.r.p[ip];
+    const float fx = __fmul_rn(-ps, a.s.vx[ip]), fz = __fmul_rn(-ps, a.s.vz[ip]);
+    const float fxr = __fmul_rn(-pr, a.r.vx[ip]), fzr = __fmul_rn(-pr, a.r.vz[ip]);
+    const int slot = it % a.delt;
+    a.ring[(size_t)slot * 2 * fs + ip] = __fadd_rn(__fmul_rn(fx, fxr), __fmul_rn(fz, fzr));
+    a.ring[((size_t)slot * 2 + 1) * fs + ip] = __fmul_rn(sqrtf(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fz, fz))),
+                                                         sqrtf(__fadd_rn(__fmul_rn(fxr, fxr), __fmul_rn(fzr, fzr))));
+    if (a.nt - 2 - it + 1 < a.delt) return;
+    float pre = 0.f, pst = 0.f;
+    for (int ii = 0; ii < a.delt; ii++) {
+        pre = __fadd_rn(pre, a.ring[(size_t)ii * 2 * fs + ip]);
+        pst = __fadd_rn(pst, a.ring[((size_t)ii * 2 + 1) * fs + ip]);
+    }
+    const float tht = __fdiv_rn(pre, pst);
+    const float ftheta = (float)(__ddiv_rn(__dmul_rn(__dmul_rn(0.5, (double)acosf(tht)), 180.0), 3.1415926));
+    if (isnan(ftheta)) return;
+    const float pp = __fmul_rn(ps, pr);
+    float *c = a.cig + ip * a.thetan;
+#pragma unroll
+    for (int ii = -2; ii <= 2; ii++) {
+        const int itheta = (int)ceilf((float)__dsub_rn((double)__fadd_rn(ftheta, (float)ii), 0.5));
+        const float betaf = (float)(1.0 * ii * ii / (2.0 * 9.0));
+        if (itheta >= 2 && itheta < a.thetan) c[itheta] = __fadd_rn(c[itheta], __fmul_rn(pp, expf(-betaf)));
+    }
+}
+
 }  // namespace swd

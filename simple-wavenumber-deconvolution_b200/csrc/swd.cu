@@ -77,6 +77,10 @@ struct swd_ctx {
     // stored-source RTM: the forward pass keeps dp/dt of every step (swd_set_source_storage)
     int src_store = 0, src_prec = SWD_STRIP_I16;
     DevBuf dpst, dpsc;
+    // angle-domain common-image gathers (SWD_RTM_CIG)
+    int cig_thetan = 0, cig_delt = 1;
+    bool have_cig = false;
+    DevBuf cig, cigring;
     int batch_opt = 0;      // shots per batched launch; 0 = autotune on first use
     int batch_tuned = 0;    // the autotuner's choice (0 = not tuned yet)
     // chunked CUDA-graph execution of the time loops
@@ -99,7 +103,7 @@ struct swd_ctx {
     {
         DevBuf *all[] = {&vp, &rho, &dpdt, &wcol, &wmap, &seis, &seis2, &rdata, &colbuf, &kzcoef, &tw,
                          &strips, &strip_scale, &I, &S, &R, &stack, &reduce, &stage_in, &stage_out, &ctrl, &wav,
-                         &dk, &gk, &s0, &ckpt, &rbuf, &alias, &dpst, &dpsc};
+                         &dk, &gk, &s0, &ckpt, &rbuf, &alias, &dpst, &dpsc, &cig, &cigring};
         for (DevBuf *b : all) bufs.push_back(b);
         for (auto &b : adj) bufs.push_back(&b);
         DevBuf *ball[] = {&bat.dpdt, &bat.I, &bat.S, &bat.strips, &bat.scale, &bat.rdata, &bat.wcol, &bat.wmap,
@@ -1221,6 +1225,31 @@ int swd_set_kernel_path(swd_ctx *ctx, int path)
     return SWD_OK;
 }
 
+int swd_set_cig(swd_ctx *ctx, int thetan, int delt)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    if (thetan < 3 || thetan > 180 || delt < 1 || delt > 64)
+        return fail(ctx, SWD_ERR_ARG, "swd_set_cig: thetan %d outside [3, 180] or delt %d outside [1, 64]", thetan, delt);
+    ctx->cig_thetan = thetan;
+    ctx->cig_delt = delt;
+    return SWD_OK;
+}
+
+int swd_rtm_cig(swd_ctx *ctx, float *cig)
+{
+    if (!ctx || !cig) return SWD_ERR_ARG;
+    if (!ctx->have_cig) return fail(ctx, SWD_ERR_STATE, "the last RTM shot accumulated no angle gathers");
+    CK(cudaSetDevice(ctx->dev));
+    const int th = ctx->cig_thetan;
+    // interior cells of each column are contiguous in the [x*ldz + z][thetan] layout
+    CK(cudaMemcpy2DAsync(cig, sizeof(float) * (size_t)ctx->nz * th,
+                         F(ctx->cig) + ((size_t)ctx->pmlc * ctx->ldz + ctx->pmlc) * th, sizeof(float) * (size_t)ctx->ldz * th,
+                         sizeof(float) * (size_t)ctx->nz * th, ctx->nx,
+                         is_device_ptr(cig) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SWD_OK;
+}
+
 int swd_set_source_storage(swd_ctx *ctx, int store, int prec)
 {
     if (!ctx) return SWD_ERR_ARG;
@@ -1367,6 +1396,17 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
     }
     // 3. backward: reconstruction (or the stored dp/dt) + receiver back-propagation + FP64 imaging
     const bool fz = fused(ctx) && !stored;
+    const bool want_cig = (flags & SWD_RTM_CIG) != 0;
+    ctx->have_cig = false;
+    if (want_cig) {
+        if (ctx->cig_thetan <= 0) return fail(ctx, SWD_ERR_STATE, "SWD_RTM_CIG needs swd_set_cig first");
+        if (fz || stored) return fail(ctx, SWD_ERR_ARG, "angle gathers need the plain kernel path and the reconstructed source");
+        const size_t fsz = (size_t)ctx->ntx * ctx->ldz;
+        CKR(ensure(ctx, ctx->cig, sizeof(float) * fsz * ctx->cig_thetan));
+        CKR(ensure(ctx, ctx->cigring, sizeof(float) * fsz * 2 * ctx->cig_delt));
+        CK(cudaMemsetAsync(ctx->cig.p, 0, sizeof(float) * fsz * ctx->cig_thetan, ctx->stream));
+        CK(cudaMemsetAsync(ctx->cigring.p, 0, sizeof(float) * fsz * 2 * ctx->cig_delt, ctx->stream));
+    }
     CKR(zero_wave(ctx, 1));
     if (fz) {
         CKR(zero_wave2(ctx, 1));
@@ -1461,6 +1501,14 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
     } else {
         b.itp = I32(ctx->ctrl);
         b.wavsub = F(ctx->wav);
+        CigArgs cg;
+        memset(&cg, 0, sizeof cg);
+        if (want_cig) {
+            cg.g = b.g; cg.s = b.s; cg.r = b.r; cg.itp = b.itp; cg.nt = nt;
+            cg.thetan = ctx->cig_thetan; cg.delt = ctx->cig_delt;
+            cg.ring = F(ctx->cigring); cg.cig = F(ctx->cig);
+        }
+        const dim3 cgrid((ctx->ntz + 31) / 32, (ctx->ntx + 7) / 8);
         auto launch = [&](int k, cudaEvent_t *ev) {
             BwdArgs q = b;
             q.itoff = -k;
@@ -1469,10 +1517,20 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
             if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
             LC_DISPATCH(ctx->Lc, launch_bwd_2, q, grid, ctx->stream);
             if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
+            if (want_cig) {
+                CigArgs cq = cg;
+                cq.itoff = -k;
+                k_cig<<<cgrid, dim3(32, 8), 0, ctx->stream>>>(cq);
+            }
         };
         const int kid[2] = {2, 3};
         b.itoff = 0;
-        CKR(run_steps(ctx, ctx->gbwd, &b, sizeof b, nt - 2, -1, nt - 1, 2, kid, launch));
+        // the CIG switch is part of the captured graph's identity
+        std::vector<char> key((const char *)&b, (const char *)&b + sizeof b);
+        key.insert(key.end(), (const char *)&cg, (const char *)&cg + sizeof cg);
+        CKR(run_steps(ctx, ctx->gbwd, key.data(), key.size(), nt - 2, -1, nt - 1, 2, kid, launch));
+        if (want_cig) ctx->launches += nt - 1;
+        ctx->have_cig = want_cig;
     }
     CK(cudaGetLastError());
     // 4. per-shot post and stack
