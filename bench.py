@@ -26,6 +26,12 @@ stacked by swd_rtm_batch (autotuned batch size, CUDA graphs, FP32 strips); the s
 through the plain engine (one shot per launch sequence, host launches, FP32 strips) is timed
 beside it, and the stacks are compared (also for int16 strips, which halve the strip memory).
 
+--workload decon measures the windowed wavenumber PSF deconvolution (swd_decon) of the c2 or
+c5 image (--config): a step deconvolves the whole image, every window of the lattice; value
+is windows/s with image, PSF image and outputs in HBM, e2e the same call on pinned host
+arrays.  The oracle's restatement of the reference's window loop (OpenMP over windows, FP64
+FFTs) on the host cores is the CPU baseline, and its output the parity check.
+
 --workload lsrtm measures the differentiable LSRTM gradient instead (801 x 401, nt = 4000,
 16 shots, reflectivity spikes at 1 % density): a step is one evaluation of
 J(r) = 1/2 sum_s ||L_s r - d_s||^2 and its gradient through the torch autograd path (Born
@@ -598,6 +604,114 @@ def run_batch(args, rank, world, dist):
     }
 
 
+def decon_bytes(case, lay):
+    """Algorithmic bytes of one deconvolution: image and PSF reads, the two padded float
+    accumulators (mig_dec, mig_coef) written once."""
+    return 4 * case.nx * case.nz * 2 + 8 * lay["nxp"] * lay["nzp"]
+
+
+def decon_flops(lay):
+    """FFT-equivalent flops of one deconvolution: 3 complex 2D transforms per window."""
+    n = lay["fullx"] * lay["fullz"]
+    return lay["windows"] * 3 * 5 * n * np.log2(n)
+
+
+def decon_cpu(case, mig, psf):
+    """The oracle's restatement of the reference's window loop on all host cores."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as orc
+    cores = os.cpu_count() or 1
+    t = time.perf_counter()
+    dec, coef = orc.decon(case.nx, case.nz, mig, psf, case.psfwin, case.filterwin, case.snapwin, case.epsilon,
+                          nthreads=cores)
+    return time.perf_counter() - t, cores, dec, coef
+
+
+def run_decon(args, rank, world, dist):
+    import ctypes as C
+    import torch
+    swd = load_pkg()
+    from swd_b200 import configs
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    case = configs.decon_case(args.config)
+    lay = configs.decon_layout(case)
+    mig, psf = configs.decon_inputs(case)
+    E = swd.Engine(case.nx, case.nz, 30, 4, 5.0, 5.0, 4e-4, 2, device=dev)   # owns the stream and decon scratch
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    E.set_stream(stream.cuda_stream)
+    L = swd.lib()
+    p = swd.DeconParams(case.nx, case.nz, case.psfwin[0], case.psfwin[1], case.filterwin[0], case.filterwin[1],
+                        case.snapwin[0], case.snapwin[1], case.epsilon, 0, 0, 0, 0)
+    d_mig, d_psf = torch.from_numpy(mig).cuda(), torch.from_numpy(psf).cuda()
+    d_dec, d_coef = torch.empty_like(d_mig), torch.empty_like(d_mig)
+    h_mig, h_psf = torch.from_numpy(mig).pin_memory(), torch.from_numpy(psf).pin_memory()
+    h_dec, h_coef = torch.empty(mig.shape).pin_memory(), torch.empty(mig.shape).pin_memory()
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+
+    def call(a, b, c, d):
+        rc = L.swd_decon(E._h, C.byref(p), a, b, c, d)
+        if rc != swd.SWD_OK:
+            raise swd.SwdError(rc, L.swd_last_error(E._h).decode())
+
+    dev_args = (d_mig.data_ptr(), d_psf.data_ptr(), d_dec.data_ptr(), d_coef.data_ptr())
+    host_args = (h_mig.data_ptr(), h_psf.data_ptr(), h_dec.data_ptr(), h_coef.data_ptr())
+
+    def timed(args_, K, W):
+        for _ in range(W):
+            call(*args_)
+        torch.cuda.synchronize()
+        n0 = E.launch_count()
+        total = 0.0
+        for _ in range(K):
+            flush.add_(1.0)                       # 256 MiB write: inputs out of L2
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            call(*args_)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total, E.launch_count() - n0
+
+    with ClockSampler(dev) as clk:
+        t_dev, launches = timed(dev_args, args.steps, args.warmup)
+    t_e2e, _ = timed(host_args, args.steps, 1)
+    t_dev, t_e2e = max_over_ranks(dist, [t_dev, t_e2e], "cuda")
+    value = replica_throughput(lay["windows"] * args.steps, world, t_dev)
+    e2e = replica_throughput(lay["windows"] * args.steps, world, t_e2e)
+    ms = t_dev / args.steps
+    hbm, src = peaks()
+    nbytes = decon_bytes(case, lay)
+    out = {
+        "metric": "decon windows/s", "value": value, "unit": "windows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (FP64 spectral division)", "data": "synthetic (seeded image and PSF lattice)",
+        "config": {"workload": case.name, "parallelism": f"replicas x{world}", "windows": lay["windows"],
+                   "transform": [lay["fullx"], lay["fullz"]],
+                   "variant": "shared memory" if (lay["fullx"] * lay["fullz"] + lay["fullx"] + lay["fullz"]) * 8 <= 200 * 1024
+                   else "global workspace",
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "e2e": {"value": e2e, "unit": "windows/s", "h2d_bytes_per_step": 2 * mig.nbytes,
+                "d2h_bytes_per_step": 2 * mig.nbytes},
+        "roofline": {"bound": "hbm", "kernel": "decon_window + decon_gather", "achieved": nbytes / (ms * 1e6),
+                     "peak": hbm, "peak_source": src, "unit": "GB/s", "frac": nbytes / (ms * 1e6) / hbm,
+                     "traffic": None, "algorithmic_bytes_per_launch": nbytes,
+                     "note": "the window transforms are shared-memory DFTs (SIMT FP32); HBM is not the bound",
+                     "fft_equivalent_gflops": decon_flops(lay) / (ms * 1e6)},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1:
+        cpu_s, cores, odec, ocoef = decon_cpu(case, mig, psf)
+        gdec = d_dec.cpu().numpy()
+        out["cpu_baseline"] = {"value": lay["windows"] / cpu_s, "unit": "windows/s", "cores": cores, "kind": "port",
+                               "sample": f"the whole image ({lay['windows']} windows), {cpu_s:.2f} s"}
+        out["parity"] = {"dec_rel_l2_vs_oracle": float(np.linalg.norm(gdec - odec) / np.linalg.norm(odec)),
+                         "coef_equal": bool(np.array_equal(d_coef.cpu().numpy(), ocoef))}
+    return out
+
+
 def lsrtm_cpu_baseline(w, nsteps=100):
     """The oracle's Born modelling + adjoint (FP32, OpenMP stencils, serial adjoint scatters)
     for one shot over nsteps steps on the full grid, extrapolated to nt."""
@@ -655,7 +769,32 @@ def run_profile_kernels(args):
                       "kernels_us": {k: ms / n * 1e3 for k, (ms, n) in prof.items() if n}}))
 
 
+def run_reference_decon(args):
+    configs = sys.modules["swd_b200"].configs
+    case = configs.decon_case(args.config)
+    lay = configs.decon_layout(case)
+    mig, psf = configs.decon_inputs(case)
+    t0 = time.perf_counter()
+    times, cores = [], 1
+    for i in range(args.warmup + args.steps):
+        dt, cores, _, _ = decon_cpu(case, mig, psf)
+        if i >= args.warmup:
+            times.append(dt)
+    mean = float(np.mean(times))
+    value = lay["windows"] / mean
+    return {"metric": "decon windows/s", "value": value, "unit": "windows/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 FFTs", "data": "synthetic", "impl": "reference",
+            "config": {"workload": case.name, "parallelism": "host OpenMP"},
+            "cpu_baseline": {"value": value, "unit": "windows/s", "cores": cores, "kind": "port",
+                             "sample": f"the whole image ({lay['windows']} windows) per step"},
+            "e2e": {"value": value, "unit": "windows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+
+
 def run_reference(args):
+    if args.workload == "decon":
+        return run_reference_decon(args)
     from swd_b200 import configs  # noqa: F401  (package already loaded by caller)
     w = sys.modules["swd_b200"].configs.c2()
     t0 = time.perf_counter()
@@ -685,8 +824,9 @@ def main():
     ap.add_argument("--profile-kernels", action="store_true", help="one short shot for ncu captures")
     ap.add_argument("--nt", type=int, default=30, help="record length of --profile-kernels")
     ap.add_argument("--path", type=int, default=None, help="kernel path: 0 plain (two launches per step), 1 fused")
-    ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch"], default="rtm")
-    ap.add_argument("--config", choices=["c2", "c5"], default="c2", help="grid of --workload rtm")
+    ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch", "decon"], default="rtm")
+    ap.add_argument("--config", choices=["c2", "c5", "shipped"], default="c2",
+                    help="grid of --workload rtm (c2, c5) or decon (c2, c5, shipped: the reference's window geometry)")
     ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
     ap.add_argument("--ckpt-prec", choices=["f32", "f16", "bf16", "i16"], default="bf16",
                     help="checkpoint precision of --workload lsrtm")
@@ -709,7 +849,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = td
-    runner = {"rtm": run_ours, "lsrtm": run_lsrtm, "batch": run_batch}[args.workload]
+    runner = {"rtm": run_ours, "lsrtm": run_lsrtm, "batch": run_batch, "decon": run_decon}[args.workload]
     out = runner(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(out), flush=True)

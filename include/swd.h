@@ -231,6 +231,10 @@ typedef struct {
      * of the four lattice PSFs around the window centre, within the same clamped lattice range
      * (project option: the reference declares but does not implement it, headpsf.h:166-167) */
     int psf_interp;
+    /* 0: the window's transform buffer in shared memory when it fits (FX*FZ*8 bytes up to about
+     * 200 KB, e.g. 158 x 158), otherwise in a global-memory workspace with each transform pass
+     * staged through shared memory (same arithmetic, same bits); 1: always the workspace */
+    int workspace;
 } swd_decon_params;
 int swd_decon_geometry(const swd_decon_params *p, int *windows, int *fft_nx, int *fft_nz);
 int swd_decon(swd_ctx *ctx, const swd_decon_params *p, const float *migreal,

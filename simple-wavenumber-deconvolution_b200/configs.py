@@ -165,7 +165,7 @@ def c4(nshots=16):
 def c5():
     """Large imaging: 4001x1601 at 4 m, nt=8000, dt=0.35 ms, 25 Hz; random-field model
     1800-4500 m/s with 3 dipping interfaces; 24 surface shots; 1201 receivers in a central
-    well (z = 200..1400 cells); scatter points on a 40x16 lattice (spacing 100 cells, offset 50);
+    well (z = 200..1400 cells); scatter points on a 40x16 lattice (spacing 99 cells, offset 49);
     FP16-scaled boundary strips."""
     rng = np.random.default_rng(SEED0 + 5)
     nx, nz = 4001, 1601
@@ -173,8 +173,9 @@ def c5():
     w = Workload("c5_4001x1601_nt8000", nx, nz, 4.0, 4.0, 8000, 3.5e-4, 30, 4, 25.0, v, box_smooth(v, 15),
                  sx=[int(round(50 + s * (nx - 100) / 23)) for s in range(24)], sz=0,
                  rec_x=np.full(1201, 2000, np.int32), rec_z=np.arange(200, 1401, dtype=np.int32))
-    w.scatter_x = 50 + 100 * np.arange(40)
-    w.scatter_z = 50 + 100 * np.arange(16)
+    # 40 x 16 scatter points, spacing 99 cells from 49 (odd spacing keeps a decon PSF lattice)
+    w.scatter_x = 49 + 99 * np.arange(40)
+    w.scatter_z = 49 + 99 * np.arange(16)
     w.extra["strips"] = "f16"
     return w
 
@@ -190,3 +191,64 @@ def small(nx=100, nz=60, nt=400, pml=10, Lc=4, dx=5.0, dz=5.0, dt=5.0e-4, f0=25.
 
 
 CONFIGS = {"c1": c1, "c2": c2, "c3": c3, "c4": c4, "c5": c5}
+
+
+@dataclass
+class DeconCase:
+    """One windowed PSF deconvolution: image size, PSF lattice spacing (= PSF patch size),
+    filter window and taper width, damping."""
+    name: str
+    nx: int
+    nz: int
+    psfwin: tuple
+    filterwin: tuple
+    snapwin: tuple
+    epsilon: float
+    seed: int
+
+
+def decon_case(cfg):
+    """The deconvolution of the c2 / c5 images (PSFs on the configuration's scatter lattice;
+    output windows of about 64^2 and 128^2) and the reference's own window geometry."""
+    if cfg == "c2":
+        return DeconCase("c2 decon: 1601x801 image, PSFs on the 79-cell scatter lattice, 63^2 output windows, "
+                         "157^2 transforms", 1601, 801, (79, 79), (79, 79), (24, 24), 5e-4, SEED0 + 2)
+    if cfg == "c5":
+        return DeconCase("c5 decon: 4001x1601 image, PSFs on the 99-cell scatter lattice, 127^2 output windows, "
+                         "227^2 transforms", 4001, 1601, (99, 99), (129, 129), (54, 54), 5e-4, SEED0 + 5)
+    if cfg == "shipped":
+        return DeconCase("reference window geometry: 845x702 image, 31^2 PSFs, 71^2 filter, 101^2 transforms",
+                         845, 702, (31, 31), (71, 71), (11, 11), 5e-4, SEED0)
+    raise KeyError(cfg)
+
+
+def decon_inputs(case):
+    """Seeded migration image (box-smoothed white reflectivity) and PSF image (a separable
+    Ricker blob of random amplitude at every lattice point halfpsfwin + k*psfwin)."""
+    rng = np.random.default_rng(case.seed)
+    mig = box_smooth(rng.standard_normal((case.nx, case.nz)).astype(np.float32), 3)
+    t = np.arange(-7, 8, dtype=np.float64) * 0.3
+    r = ((1 - 2 * t * t) * np.exp(-t * t)).astype(np.float32)
+    blob = np.outer(r, r)
+    psf = np.zeros((case.nx, case.nz), np.float32)
+    hx, hz = case.psfwin[0] // 2, case.psfwin[1] // 2
+    for ix in range(hx, case.nx, case.psfwin[0]):
+        for iz in range(hz, case.nz, case.psfwin[1]):
+            x0, z0 = max(ix - 7, 0), max(iz - 7, 0)
+            x1, z1 = min(ix + 8, case.nx), min(iz + 8, case.nz)
+            psf[x0:x1, z0:z1] += np.float32(rng.uniform(0.5, 1.5)) * blob[x0 - ix + 7:x1 - ix + 7, z0 - iz + 7:z1 - iz + 7]
+    return mig, psf
+
+
+def decon_layout(case):
+    """Window lattice of a deconvolution (the reference's formulas): windows, transform size,
+    output window, padded image size."""
+    out = {}
+    for a, k in (("x", 0), ("z", 1)):
+        full = case.filterwin[k] + case.psfwin[k] - 1
+        outwin = 2 * (case.psfwin[k] // 10) + 2 * case.snapwin[k] + 1
+        step = outwin - case.snapwin[k]
+        n = -(-(getattr(case, "n" + a) + full) // step) + 1
+        out.update({f"full{a}": full, f"outwin{a}": outwin, f"stepnum{a}": n, f"n{a}p": n * step})
+    out["windows"] = out["stepnumx"] * out["stepnumz"]
+    return out

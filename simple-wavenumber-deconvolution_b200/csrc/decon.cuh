@@ -11,6 +11,11 @@
 //   d = IDFT2(D) (unnormalised); the outwin^2 centre, times the Hann-edged taper, is
 //   written to a per-window slot.  A second kernel overlap-adds the slots in window order.
 //
+// Windows whose buffer does not fit in shared memory (or workspace = 1) keep it in a per-CTA
+// global-memory workspace instead; each transform pass then copies a chunk of whole
+// transforms into shared memory, transforms it there and writes it back (dft2_staged), with
+// the same per-output arithmetic, so both variants give the same bits.
+//
 // The buffer index is ixx*FZ + izz and the 2D transform is taken over (n0 rows x n1
 // columns) of that linear buffer, which is how the reference plans it
 // (fftw_plan_dft_2d(fullwz, fullwx) on an x-major buffer, :490-493).  Transforms are FP32
@@ -31,6 +36,7 @@ struct DeconGeo {
     int outwinx, outwinz, halfoutwx, halfoutwz, stepwinx, stepwinz, stepnumx, stepnumz, totalnum, nxp, nzp;
     float epsilon;
     int psf_interp;   // 1: bilinear interpolation of the lattice PSFs (project option)
+    int staged;       // 1: buffer in a global workspace, passes staged through shared memory
 };
 
 // Bracketing lattice points of a window-centre coordinate for PSF interpolation: f0 =
@@ -94,17 +100,58 @@ __device__ void dft2(float2 *s, const float2 *tw0, const float2 *tw1, int n0, in
     dft_pass(s, tw0, n0, n1, n1, 1, sign);   // columns (length n0)
 }
 
-__global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *__restrict__ mig,
-                                                      const float *__restrict__ psf, const float *__restrict__ coefr,
-                                                      float *__restrict__ winout)
+// dft2 on a buffer Zg in global memory: row transforms (length n1, contiguous) and then column
+// transforms (length n0, stride n1) are copied cap elements at a time into the shared chunk,
+// transformed by dft_pass and written back.  cap >= max(n0, n1).
+__device__ void dft2_staged(float2 *Zg, float2 *chunk, int cap, const float2 *tw0, const float2 *tw1, int n0, int n1,
+                            int sign)
 {
-    extern __shared__ float2 sm[];
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int R = cap / n1;
+    for (int r0 = 0; r0 < n0; r0 += R) {
+        const int nr = min(R, n0 - r0), m = nr * n1;
+        float2 *src = Zg + (size_t)r0 * n1;
+        for (int j = tid; j < m; j += nthr) chunk[j] = src[j];
+        __syncthreads();
+        dft_pass(chunk, tw1, n1, nr, 1, n1, sign);
+        for (int j = tid; j < m; j += nthr) src[j] = chunk[j];
+        __syncthreads();
+    }
+    const int Cc = cap / n0;
+    for (int c0 = 0; c0 < n1; c0 += Cc) {
+        const int nc = min(Cc, n1 - c0), m = n0 * nc;
+        for (int j = tid; j < m; j += nthr) chunk[j] = Zg[(size_t)(j / nc) * n1 + c0 + j % nc];
+        __syncthreads();
+        dft_pass(chunk, tw0, n0, nc, nc, 1, sign);
+        for (int j = tid; j < m; j += nthr) Zg[(size_t)(j / nc) * n1 + c0 + j % nc] = chunk[j];
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void decon_twiddles(const DeconGeo &g, float2 *tw0, float2 *tw1)
+{
+    for (int j = threadIdx.x; j < g.n0; j += blockDim.x) {
+        float s, c;
+        sincospi(-2.0f * (float)j / (float)g.n0, &s, &c);
+        tw0[j] = make_float2(c, s);
+    }
+    for (int j = threadIdx.x; j < g.n1; j += blockDim.x) {
+        float s, c;
+        sincospi(-2.0f * (float)j / (float)g.n1, &s, &c);
+        tw1[j] = make_float2(c, s);
+    }
+}
+
+// One window w on the buffer Z (shared memory, or global memory when STAGED with the shared
+// chunk of cap elements); the twiddle tables are filled by the caller.
+template <bool STAGED>
+__device__ void decon_window(const DeconGeo &g, const float *__restrict__ mig, const float *__restrict__ psf,
+                             float *__restrict__ winout, int w, float2 *Z, const float2 *tw0, const float2 *tw1,
+                             float2 *chunk, int cap)
+{
     const int n = g.FX * g.FZ;
-    float2 *Z = sm;
-    float2 *tw0 = Z + n, *tw1 = tw0 + g.n0;
     __shared__ float s_ppmax, s_psfmax;
     __shared__ unsigned s_fmax;
-    const int w = blockIdx.x;
     const int ix = g.stepwinx * (w / g.stepnumz), iz = g.stepwinz * (w % g.stepnumz);
     const int tid = threadIdx.x, nthr = blockDim.x;
     // nearest PSF on the lattice, indices clamped to [3, nwpsf-4] (:586-598)
@@ -134,16 +181,6 @@ __global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *_
     };
 
     for (int j = tid; j < n; j += nthr) Z[j] = make_float2(0.f, 0.f);
-    for (int j = tid; j < g.n0; j += nthr) {
-        float s, c;
-        sincospi(-2.0f * (float)j / (float)g.n0, &s, &c);
-        tw0[j] = make_float2(c, s);
-    }
-    for (int j = tid; j < g.n1; j += nthr) {
-        float s, c;
-        sincospi(-2.0f * (float)j / (float)g.n1, &s, &c);
-        tw1[j] = make_float2(c, s);
-    }
     // L1 norms in the reference's order and rounding (:554-576, :618-620): thread 0 sums
     // the image patch, thread 32 the PSF, while the rest of the block fills the buffer
     if (tid == 0) {
@@ -179,7 +216,8 @@ __global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *_
         Z[ixx * g.FZ + izz].y = (float)((double)psf_val(ixx, izz) / psm);
     }
     __syncthreads();
-    dft2(Z, tw0, tw1, g.n0, g.n1, -1);
+    if (STAGED) dft2_staged(Z, chunk, cap, tw0, tw1, g.n0, g.n1, -1);
+    else dft2(Z, tw0, tw1, g.n0, g.n1, -1);
     // |S^|^2 maximum over all bins (float compare of the double square, :625-633)
     float fm = 0.f;
     for (int j = tid; j < n; j += nthr) {
@@ -210,13 +248,41 @@ __global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *_
         if (jm != j) Z[jm] = make_float2((float)dr, (float)-di);   // D(-k) = conj D(k)
     }
     __syncthreads();
-    dft2(Z, tw0, tw1, g.n0, g.n1, +1);
+    if (STAGED) dft2_staged(Z, chunk, cap, tw0, tw1, g.n0, g.n1, +1);
+    else dft2(Z, tw0, tw1, g.n0, g.n1, +1);
     const int nout = g.outwinx * g.outwinz;
     float *o = winout + (size_t)w * nout;
     for (int j = tid; j < nout; j += nthr) {
         const int ixx = j / g.outwinz, izz = j % g.outwinz;
         const int ip = (g.ocx - g.halfoutwx + ixx) * g.FZ + g.ocz - g.halfoutwz + izz;
         o[j] = Z[ip].x;
+    }
+}
+
+// One CTA per window, the whole buffer and the twiddles in shared memory.
+__global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *__restrict__ mig,
+                                                      const float *__restrict__ psf, float *__restrict__ winout)
+{
+    extern __shared__ float2 sm[];
+    float2 *Z = sm, *tw0 = Z + (size_t)g.FX * g.FZ, *tw1 = tw0 + g.n0;
+    decon_twiddles(g, tw0, tw1);
+    decon_window<false>(g, mig, psf, winout, blockIdx.x, Z, tw0, tw1, nullptr, 0);
+}
+
+// Persistent CTAs, each with its own buffer of FX*FZ elements in the global workspace ws,
+// working through windows blockIdx.x, blockIdx.x + gridDim.x, ...; shared memory holds the
+// twiddles and a chunk of cap elements for the staged passes.
+__global__ void __launch_bounds__(512) k_decon_window_staged(DeconGeo g, const float *__restrict__ mig,
+                                                             const float *__restrict__ psf, float *__restrict__ winout,
+                                                             float2 *__restrict__ ws, int cap)
+{
+    extern __shared__ float2 sm[];
+    float2 *tw0 = sm, *tw1 = tw0 + g.n0, *chunk = tw1 + g.n1;
+    float2 *Z = ws + (size_t)blockIdx.x * g.FX * g.FZ;
+    decon_twiddles(g, tw0, tw1);
+    for (int w = blockIdx.x; w < g.totalnum; w += gridDim.x) {
+        decon_window<true>(g, mig, psf, winout, w, Z, tw0, tw1, chunk, cap);
+        __syncthreads();   // the next window's fill overwrites Z and the shared scalars
     }
 }
 

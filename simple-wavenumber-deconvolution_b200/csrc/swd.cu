@@ -81,6 +81,9 @@ struct swd_ctx {
     int cig_thetan = 0, cig_delt = 1;
     bool have_cig = false;
     DevBuf cig, cigring;
+    // deconvolution scratch kept between swd_decon calls: inputs, taper, window slots,
+    // outputs, staged workspaces
+    DevBuf dcn[5];
     int batch_opt = 0;      // shots per batched launch; 0 = autotune on first use
     int batch_tuned = 0;    // the autotuner's choice (0 = not tuned yet)
     // chunked CUDA-graph execution of the time loops
@@ -106,6 +109,7 @@ struct swd_ctx {
                          &dk, &gk, &s0, &ckpt, &rbuf, &alias, &dpst, &dpsc, &cig, &cigring};
         for (DevBuf *b : all) bufs.push_back(b);
         for (auto &b : adj) bufs.push_back(&b);
+        for (auto &b : dcn) bufs.push_back(&b);
         DevBuf *ball[] = {&bat.dpdt, &bat.I, &bat.S, &bat.strips, &bat.scale, &bat.rdata, &bat.wcol, &bat.wmap,
                           &bat.desc, &bat.wav, &bat.reduce};
         for (DevBuf *b : ball) bufs.push_back(b);
@@ -1017,10 +1021,46 @@ static int decon_geo(const swd_decon_params *p, DeconGeo &g)
     g.nxp = g.stepnumx * g.stepwinx; g.nzp = g.stepnumz * g.stepwinz;
     if (p->filterwinx < p->psfwinx || p->filterwinz < p->psfwinz) return SWD_ERR_ARG;
     if (p->filterwinx < g.outwinx || p->filterwinz < g.outwinz) return SWD_ERR_ARG;
-    if (g.n0 > 512 || g.n1 > 512 || (size_t)g.FX * g.FZ * 8 + (g.n0 + g.n1) * 8 > 200 * 1024) return SWD_ERR_ARG;
+    if (g.n0 > 512 || g.n1 > 512) return SWD_ERR_ARG;
+    if (p->workspace != 0 && p->workspace != 1) return SWD_ERR_ARG;
+    g.staged = p->workspace == 1 || (size_t)g.FX * g.FZ * 8 + (g.n0 + g.n1) * 8 > 200 * 1024;
     // the PSF lattice must hold at least 7 cells per axis so the clamp range [3, n-4] exists
     if (g.nxwpsf < 7 || g.nzwpsf < 7) return SWD_ERR_ARG;
     return SWD_OK;
+}
+
+// Launch shape of the staged window kernel: a 96 KB shared chunk (at least one transform) and
+// as many persistent CTAs as are resident at once, each owning FX*FZ float2 of workspace.
+static size_t decon_staged_cap(const DeconGeo &g) { return std::max<size_t>(12288, std::max(g.n0, g.n1)); }
+static size_t decon_staged_smem(const DeconGeo &g) { return sizeof(float2) * (g.n0 + g.n1 + decon_staged_cap(g)); }
+static int decon_staged_blocks(const DeconGeo &g, int dev)
+{
+    int nsm = 0, occ = 0;
+    const size_t sm = decon_staged_smem(g);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(k_decon_window_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_decon_window_staged, 512, sm) != cudaSuccess)
+        return 0;
+    return std::max(1, std::min(g.totalnum, nsm * std::max(occ, 1)));
+}
+
+// Window kernel of g: one CTA per window in shared memory, or nblk persistent CTAs over the
+// workspace ws (staged).
+static cudaError_t launch_decon_windows(const DeconGeo &g, const float *mig, const float *psf, float *winout,
+                                        float2 *ws, int nblk, cudaStream_t st)
+{
+    if (g.staged) {
+        const size_t sm = decon_staged_smem(g);
+        cudaError_t e = cudaFuncSetAttribute(k_decon_window_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        k_decon_window_staged<<<nblk, 512, sm, st>>>(g, mig, psf, winout, ws, (int)decon_staged_cap(g));
+    } else {
+        const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + g.n0 + g.n1);
+        cudaError_t e = cudaFuncSetAttribute(k_decon_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        k_decon_window<<<g.totalnum, 512, sm, st>>>(g, mig, psf, winout);
+    }
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------------------
@@ -1751,31 +1791,42 @@ int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, 
                 else cz = 1.0;
                 coefr[(size_t)ix * g.outwinz + iz] = cx * cz;
             }
+        // device arrays are read and written in place; host arrays go through the scratch
         const size_t np = (size_t)g.nx * g.nz, nout = coefr.size();
-        DevBuf bin, bcoef, bwin, bout;
-        rc = ensure(ctx, bin, sizeof(float) * 2 * np);
+        const bool din = is_device_ptr(migreal) && is_device_ptr(migpsf);
+        const bool dout = is_device_ptr(mig_dec) && is_device_ptr(mig_coef);
+        DevBuf &bin = ctx->dcn[0], &bcoef = ctx->dcn[1], &bwin = ctx->dcn[2], &bout = ctx->dcn[3], &bws = ctx->dcn[4];
+        const int nblk = g.staged ? decon_staged_blocks(g, ctx->dev) : 0;
+        if (g.staged && nblk < 1) { rc = fail(ctx, SWD_ERR_CUDA, "decon: no launch shape for the staged window kernel"); break; }
+        if (g.staged) rc = ensure(ctx, bws, sizeof(float2) * (size_t)nblk * g.FX * g.FZ);
+        if (!rc && !din) rc = ensure(ctx, bin, sizeof(float) * 2 * np);
         if (!rc) rc = ensure(ctx, bcoef, sizeof(float) * nout);
         if (!rc) rc = ensure(ctx, bwin, sizeof(float) * nout * g.totalnum);
-        if (!rc) rc = ensure(ctx, bout, sizeof(float) * 2 * np);
-        if (!rc) rc = to_dev(ctx, bin.p, migreal, sizeof(float) * np);
-        if (!rc) rc = to_dev(ctx, F(bin) + np, migpsf, sizeof(float) * np);
+        if (!rc && !dout) rc = ensure(ctx, bout, sizeof(float) * 2 * np);
+        const float *im = din ? migreal : F(bin), *ps = din ? migpsf : F(bin) + np;
+        float *od = dout ? mig_dec : F(bout), *oc = dout ? mig_coef : F(bout) + np;
+        if (!rc && !din) rc = to_dev(ctx, bin.p, migreal, sizeof(float) * np);
+        if (!rc && !din) rc = to_dev(ctx, F(bin) + np, migpsf, sizeof(float) * np);
         if (!rc && cudaMemcpyAsync(bcoef.p, coefr.data(), sizeof(float) * nout, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
             rc = fail(ctx, SWD_ERR_CUDA, "decon: coefficient upload");
         if (!rc) {
-            const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + g.n0 + g.n1);
-            cudaFuncSetAttribute(k_decon_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k_decon_window<<<g.totalnum, 512, sm, ctx->stream>>>(g, F(bin), F(bin) + np, F(bcoef), F(bwin));
-            k_decon_gather<<<592, 256, 0, ctx->stream>>>(g, F(bwin), F(bcoef), F(bout), F(bout) + np);
-            cudaError_t e = cudaGetLastError();
+            cudaError_t e = launch_decon_windows(g, im, ps, F(bwin), (float2 *)bws.p, nblk, ctx->stream);
+            if (e == cudaSuccess) {
+                k_decon_gather<<<592, 256, 0, ctx->stream>>>(g, F(bwin), F(bcoef), od, oc);
+                e = cudaGetLastError();
+            }
             if (e != cudaSuccess) rc = fail(ctx, SWD_ERR_CUDA, "decon kernels: %s", cudaGetErrorString(e));
+            else ctx->launches += 2;
         }
-        if (!rc) rc = from_dev(ctx, mig_dec, bout.p, sizeof(float) * np);
-        if (!rc) rc = from_dev(ctx, mig_coef, F(bout) + np, sizeof(float) * np);
+        if (!rc && !dout) rc = from_dev(ctx, mig_dec, od, sizeof(float) * np);
+        if (!rc && !dout) rc = from_dev(ctx, mig_coef, oc, sizeof(float) * np);
         cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (!rc && e != cudaSuccess) rc = fail(ctx, SWD_ERR_CUDA, "decon: %s", cudaGetErrorString(e));
-        cudaFree(bin.p); cudaFree(bcoef.p); cudaFree(bwin.p); cudaFree(bout.p);
     } while (0);
-    if (!ctx_in) cudaStreamDestroy(tmp.stream);
+    if (!ctx_in) {
+        for (DevBuf &b : tmp.dcn) cudaFree(b.p);
+        cudaStreamDestroy(tmp.stream);
+    }
     return rc;
 }
 
@@ -1788,7 +1839,11 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
     DeconGeo g;
     if (!p || decon_geo(p, g) != SWD_OK) return SWD_ERR_ARG;
     const size_t nout = (size_t)g.outwinx * g.outwinz;
-    if ((size_t)g.totalnum * nout + nout > SWD_DECON_STATIC_SCRATCH_FLOATS) return SWD_ERR_CAPACITY;
+    // scratch: taper, window slots, then (staged) the CTA workspaces from an even offset; the
+    // staged kernel runs on as many CTAs as have a workspace that fits
+    const size_t used = (size_t)g.totalnum * nout + nout, wsoff = (used + 1) & ~(size_t)1;
+    if (used > SWD_DECON_STATIC_SCRATCH_FLOATS) return SWD_ERR_CAPACITY;
+    int nblk = 0;
     const void *ptrs[4] = {migreal, migpsf, mig_dec, mig_coef};
     for (const void *q : ptrs)
         if (!is_device_ptr(q)) return SWD_ERR_ARG;
@@ -1802,13 +1857,17 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
         }
         scratch_addr[dev] = (float *)a;
     }
+    if (g.staged) {
+        const size_t per = (size_t)2 * g.FX * g.FZ;
+        const size_t fit = wsoff < SWD_DECON_STATIC_SCRATCH_FLOATS ? (SWD_DECON_STATIC_SCRATCH_FLOATS - wsoff) / per : 0;
+        nblk = std::min<long long>(decon_staged_blocks(g, dev), (long long)fit);
+        if (nblk < 1) return SWD_ERR_CAPACITY;
+    }
     float *coefr = scratch_addr[dev], *winout = coefr + nout;
     cudaStream_t st = (cudaStream_t)cuda_stream;
-    const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + g.n0 + g.n1);
-    if (cudaFuncSetAttribute(k_decon_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-        return SWD_ERR_CUDA;
     k_decon_taper<<<(int)((nout + 255) / 256), 256, 0, st>>>(coefr, g.outwinx, g.outwinz, p->snapwinx, p->snapwinz);
-    k_decon_window<<<g.totalnum, 512, sm, st>>>(g, migreal, migpsf, coefr, winout);
+    if (launch_decon_windows(g, migreal, migpsf, winout, (float2 *)(coefr + wsoff), nblk, st) != cudaSuccess)
+        return SWD_ERR_CUDA;
     k_decon_gather<<<592, 256, 0, st>>>(g, winout, coefr, mig_dec, mig_coef);
     return cudaGetLastError() == cudaSuccess ? SWD_OK : SWD_ERR_CUDA;
 }

@@ -228,6 +228,37 @@ def test_decon_shipped_geometry(swd, orc):
     assert rel_l2(dec, odec) < TOL_DECON
 
 
+def test_decon_workspace_variant_same_bits(swd):
+    """The staged variant (transform buffer in a global workspace, passes through shared
+    memory) against the shared-memory one on the reference's window geometry: same bits."""
+    rng = np.random.default_rng(12)
+    nx, nz = 845, 702
+    mig = rng.standard_normal((nx, nz)).astype(np.float32)
+    psf = np.zeros((nx, nz), np.float32)
+    psf[15::31, 15::31] = 1.0
+    psf[16::31, 15::31] = -0.5
+    a, ca = swd.decon(mig, psf, (31, 31), (71, 71), (11, 11), 5e-4)
+    b, cb = swd.decon(mig, psf, (31, 31), (71, 71), (11, 11), 5e-4, workspace=1)
+    assert np.array_equal(a, b) and np.array_equal(ca, cb)
+
+
+def test_decon_large_windows_match_oracle(swd, orc):
+    """Windows whose 181 x 181 transform buffer (262 KB) exceeds shared memory take the
+    workspace variant automatically; against the oracle."""
+    rng = np.random.default_rng(13)
+    nx, nz = 300, 260
+    mig = rng.standard_normal((nx, nz)).astype(np.float32)
+    psf = np.zeros((nx, nz), np.float32)
+    psf[20::41, 20::41] = 1.0
+    psf[21::41, 20::41] = -0.4
+    psf[20::41, 22::41] = 0.3
+    assert swd.decon_geometry(nx, nz, (41, 41), (141, 141), (20, 20))[1:] == (181, 181)
+    dec, coef = swd.decon(mig, psf, (41, 41), (141, 141), (20, 20), 1e-3)
+    odec, ocoef = orc.decon(nx, nz, mig, psf, (41, 41), (141, 141), (20, 20), 1e-3)
+    assert np.array_equal(coef, ocoef)
+    assert rel_l2(dec, odec) < TOL_DECON
+
+
 @pytest.mark.skipif(not (GOLDEN / "ref_gpu_small.npz").exists(), reason="reference-GPU golden not generated")
 def test_engine_matches_reference_cuda_build(swd, orc):
     """libswd vs the reference's own CUDA programs (AFor + AVSPRTM) on the golden case."""

@@ -33,16 +33,17 @@ def test_noalloc_decon_matches_allocating_decon_twice(swd):
     L = swd.lib()
     L.swd_decon_noalloc.argtypes = [C.POINTER(swd.DeconParams)] + [C.c_void_p] * 5
     L.swd_decon_noalloc.restype = C.c_int
-    cases = [(845, 702, (31, 31), (71, 71), (11, 11), 5e-4, 21),   # the reference's own window geometry
-             (300, 257, (11, 9), (25, 21), (5, 4), 1e-3, 22)]
+    cases = [(845, 702, (31, 31), (71, 71), (11, 11), 5e-4, 21, 0),   # the reference's own window geometry
+             (300, 257, (11, 9), (25, 21), (5, 4), 1e-3, 22, 0),
+             (300, 257, (11, 9), (25, 21), (5, 4), 1e-3, 23, 1)]       # buffers in the scratch workspace
     stream = torch.cuda.current_stream()
-    for nx, nz, psfw, fltw, snapw, eps, seed in cases:
+    for nx, nz, psfw, fltw, snapw, eps, seed, ws in cases:
         mig, psf = _inputs(seed, nx, nz, psfw)
-        ref_dec, ref_coef = swd.decon(mig, psf, psfw, fltw, snapw, eps)
+        ref_dec, ref_coef = swd.decon(mig, psf, psfw, fltw, snapw, eps, workspace=ws)
         d_mig, d_psf = torch.from_numpy(mig).cuda(), torch.from_numpy(psf).cuda()
         d_dec = torch.full((nx, nz), float("nan"), device="cuda")
         d_coef = torch.full((nx, nz), float("nan"), device="cuda")
-        p = swd.DeconParams(nx, nz, psfw[0], psfw[1], fltw[0], fltw[1], snapw[0], snapw[1], eps, 0, 0)
+        p = swd.DeconParams(nx, nz, psfw[0], psfw[1], fltw[0], fltw[1], snapw[0], snapw[1], eps, 0, 0, 0, ws)
         rc = L.swd_decon_noalloc(C.byref(p), d_mig.data_ptr(), d_psf.data_ptr(), d_dec.data_ptr(),
                                  d_coef.data_ptr(), stream.cuda_stream)
         assert rc == swd.SWD_OK
