@@ -643,7 +643,7 @@ def run_decon(args, rank, world, dist):
     E.set_stream(stream.cuda_stream)
     L = swd.lib()
     p = swd.DeconParams(case.nx, case.nz, case.psfwin[0], case.psfwin[1], case.filterwin[0], case.filterwin[1],
-                        case.snapwin[0], case.snapwin[1], case.epsilon, 0, 0, 0, 0)
+                        case.snapwin[0], case.snapwin[1], case.epsilon, 0, 0, 0, 0, args.decon_iters, 2e-2, 6e-2)
     d_mig, d_psf = torch.from_numpy(mig).cuda(), torch.from_numpy(psf).cuda()
     d_dec, d_coef = torch.empty_like(d_mig), torch.empty_like(d_mig)
     h_mig, h_psf = torch.from_numpy(mig).pin_memory(), torch.from_numpy(psf).pin_memory()
@@ -691,7 +691,9 @@ def run_decon(args, rank, world, dist):
                    "transform": [lay["fullx"], lay["fullz"]],
                    "variant": "shared memory" if (lay["fullx"] * lay["fullz"] + lay["fullx"] + lay["fullz"]) * 8 <= 200 * 1024
                    else "global workspace",
-                   "l2": "flushed (256 MiB write) before every timed step"},
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "iterations": args.decon_iters, "reg_l1": 2e-2 if args.decon_iters else 0.0,
+                   "reg_l2": 6e-2 if args.decon_iters else 0.0},
         "e2e": {"value": e2e, "unit": "windows/s", "h2d_bytes_per_step": 2 * mig.nbytes,
                 "d2h_bytes_per_step": 2 * mig.nbytes},
         "roofline": {"bound": "hbm", "kernel": "decon_window + decon_gather", "achieved": nbytes / (ms * 1e6),
@@ -702,7 +704,7 @@ def run_decon(args, rank, world, dist):
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.decon_iters:
         cpu_s, cores, odec, ocoef = decon_cpu(case, mig, psf)
         gdec = d_dec.cpu().numpy()
         out["cpu_baseline"] = {"value": lay["windows"] / cpu_s, "unit": "windows/s", "cores": cores, "kind": "port",
@@ -828,6 +830,8 @@ def main():
     ap.add_argument("--config", choices=["c2", "c5", "shipped"], default="c2",
                     help="grid of --workload rtm (c2, c5) or decon (c2, c5, shipped: the reference's window geometry)")
     ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
+    ap.add_argument("--decon-iters", type=int, default=0,
+                    help="--workload decon: FISTA iterations of the regularised option (L1 0.02, L2 0.06)")
     ap.add_argument("--ckpt-prec", choices=["f32", "f16", "bf16", "i16"], default="bf16",
                     help="checkpoint precision of --workload lsrtm")
     args = ap.parse_args()

@@ -235,6 +235,15 @@ typedef struct {
      * 200 KB, e.g. 158 x 158), otherwise in a global-memory workspace with each transform pass
      * staged through shared memory (same arithmetic, same bits); 1: always the workspace */
     int workspace;
+    /* Iterative regularised deconvolution (project option: the reference parses reg_eps and its
+     * parameter file lists an L2 coefficient and an iteration count, kkdecon_acoustic/
+     * parameter.txt:35-40, but never uses them).  iters > 0 refines each window's damped
+     * spectral solution x0 with iters FISTA steps on
+     *   1/2 |psf * x - patch|^2 + mu/2 |x|^2 + lambda |x|_1,  mu = reg_l2 * max|PSF^|^2,
+     * step 1/(max|PSF^|^2 + mu), soft threshold reg_l1 * max|x0| per step (both the patch and
+     * the PSF L1-normalised as in the direct path).  iters = 0: the reference's direct division. */
+    int iters;
+    float reg_l1, reg_l2;
 } swd_decon_params;
 int swd_decon_geometry(const swd_decon_params *p, int *windows, int *fft_nx, int *fft_nz);
 int swd_decon(swd_ctx *ctx, const swd_decon_params *p, const float *migreal,

@@ -46,7 +46,8 @@ class OrcGeom(C.Structure):
 class OrcDeconParams(C.Structure):
     _fields_ = [("nx", C.c_int), ("nz", C.c_int), ("psfwinx", C.c_int), ("psfwinz", C.c_int),
                 ("filterwinx", C.c_int), ("filterwinz", C.c_int), ("snapwinx", C.c_int), ("snapwinz", C.c_int),
-                ("epsilon", C.c_float), ("fft_n0", C.c_int), ("fft_n1", C.c_int), ("psf_interp", C.c_int)]
+                ("epsilon", C.c_float), ("fft_n0", C.c_int), ("fft_n1", C.c_int), ("psf_interp", C.c_int),
+                ("iters", C.c_int), ("reg_l1", C.c_float), ("reg_l2", C.c_float)]
 
 
 _lib = None
@@ -282,9 +283,10 @@ def rtm_shot(model: Model, geom: Geom, rick, data, dtype=np.float32, cig=None):
     return res
 
 
-def decon(nx, nz, migreal, migpsf, psfwin, filterwin, snapwin, epsilon, fft_n=(0, 0), nthreads=0, psf_interp=0):
+def decon(nx, nz, migreal, migpsf, psfwin, filterwin, snapwin, epsilon, fft_n=(0, 0), nthreads=0, psf_interp=0,
+          iters=0, reg_l1=0.0, reg_l2=0.0):
     p = OrcDeconParams(nx, nz, psfwin[0], psfwin[1], filterwin[0], filterwin[1], snapwin[0], snapwin[1],
-                       epsilon, fft_n[0], fft_n[1], psf_interp)
+                       epsilon, fft_n[0], fft_n[1], psf_interp, iters, reg_l1, reg_l2)
     dec = np.zeros((nx, nz), np.float32)
     coef = np.zeros((nx, nz), np.float32)
     rc = lib().orc_decon(C.byref(p), np.ascontiguousarray(migreal, np.float32), np.ascontiguousarray(migpsf, np.float32),

@@ -472,6 +472,15 @@ int orc_decon(const orc_decon_params *p, const float *migreal, const float *migp
         double *snapm = (double *)malloc(sizeof(double) * 2 * nbuf);
         double *snapsf = (double *)malloc(sizeof(double) * 2 * nbuf);
         double *decon = (double *)malloc(sizeof(double) * 2 * nbuf);
+        /* iterative option: B = M^ conj S^, P = |S^|^2, iterates, and a transform buffer */
+        double *itB = NULL, *itP = NULL, *itX = NULL, *itXP = NULL, *itW = NULL;
+        if (p->iters > 0) {
+            itB = (double *)malloc(sizeof(double) * 2 * nbuf);
+            itP = (double *)malloc(sizeof(double) * nbuf);
+            itX = (double *)malloc(sizeof(double) * nbuf);
+            itXP = (double *)malloc(sizeof(double) * nbuf);
+            itW = (double *)malloc(sizeof(double) * 2 * nbuf);
+        }
 #pragma omp for schedule(dynamic, 4)
         for (int stepindex = 0; stepindex < g.totalnum; stepindex++) {
             int ix = g.stepwinx * (stepindex / g.stepnumz);
@@ -535,6 +544,7 @@ int orc_decon(const orc_decon_params *p, const float *migreal, const float *migp
                 tmpfloat = (snapsf[2 * ip] * snapsf[2 * ip] + snapsf[2 * ip + 1] * snapsf[2 * ip + 1]);
                 if (fft_max < tmpfloat) fft_max = tmpfloat;
             }
+            const double smax2 = fft_max;   /* max |S^|^2 before the damping factor */
             fft_max *= p->epsilon;
             if (fft_max == 0.0) fft_max = 1.0e-15;
             for (size_t ip = 0; ip < nbuf; ip++) {
@@ -543,6 +553,41 @@ int orc_decon(const orc_decon_params *p, const float *migreal, const float *migp
                 decon[2 * ip + 1] = (-snapm[2 * ip] * snapsf[2 * ip + 1] + snapm[2 * ip + 1] * snapsf[2 * ip]) / tmpfloat;
             }
             orc_fft2(g.n0, g.n1, decon, +1);
+            if (p->iters > 0 && smax2 > 0.0) {
+                /* FISTA from x0 = IDFT2(D)/n; gradient IDFT2((P + mu) Y^ - B)/n */
+                const double n = (double)nbuf, mu = p->reg_l2 * smax2, tau = 1.0 / (smax2 + mu);
+                double xmax = 0.0, t = 1.0;
+                for (size_t ip = 0; ip < nbuf; ip++) {
+                    itB[2 * ip] = snapm[2 * ip] * snapsf[2 * ip] + snapm[2 * ip + 1] * snapsf[2 * ip + 1];
+                    itB[2 * ip + 1] = snapm[2 * ip + 1] * snapsf[2 * ip] - snapm[2 * ip] * snapsf[2 * ip + 1];
+                    itP[ip] = snapsf[2 * ip] * snapsf[2 * ip] + snapsf[2 * ip + 1] * snapsf[2 * ip + 1];
+                    itX[ip] = itXP[ip] = decon[2 * ip] / n;
+                    if (fabs(itX[ip]) > xmax) xmax = fabs(itX[ip]);
+                }
+                const double thr = p->reg_l1 * xmax;
+                for (int k = 0; k < p->iters; k++) {
+                    const double tn = 0.5 * (1.0 + sqrt(1.0 + 4.0 * t * t)), beta = (t - 1.0) / tn;
+                    t = tn;
+                    for (size_t ip = 0; ip < nbuf; ip++) {
+                        itW[2 * ip] = itX[ip] + beta * (itX[ip] - itXP[ip]);
+                        itW[2 * ip + 1] = 0.0;
+                    }
+                    orc_fft2(g.n0, g.n1, itW, -1);
+                    for (size_t ip = 0; ip < nbuf; ip++) {
+                        const double q = itP[ip] + mu;
+                        itW[2 * ip] = q * itW[2 * ip] - itB[2 * ip];
+                        itW[2 * ip + 1] = q * itW[2 * ip + 1] - itB[2 * ip + 1];
+                    }
+                    orc_fft2(g.n0, g.n1, itW, +1);
+                    for (size_t ip = 0; ip < nbuf; ip++) {
+                        const double x = itX[ip], y = x + beta * (x - itXP[ip]);
+                        const double v = y - tau * itW[2 * ip] / n;
+                        itXP[ip] = x;
+                        itX[ip] = v > thr ? v - thr : (v < -thr ? v + thr : 0.0);
+                    }
+                }
+                for (size_t ip = 0; ip < nbuf; ip++) decon[2 * ip] = itX[ip] * n;
+            }
             double *wo = winout + (size_t)stepindex * nout;
             for (int ixx = 0; ixx < g.outwinx; ixx++)
                 for (int izz = 0; izz < g.outwinz; izz++) {
@@ -551,6 +596,7 @@ int orc_decon(const orc_decon_params *p, const float *migreal, const float *migp
                 }
         }
         free(snapm); free(snapsf); free(decon);
+        free(itB); free(itP); free(itX); free(itXP); free(itW);
     }
     /* overlap-add in window order, float accumulators as in the reference (:656-673) */
     for (int stepindex = 0; stepindex < g.totalnum; stepindex++) {

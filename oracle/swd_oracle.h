@@ -106,6 +106,11 @@ typedef struct {
     float epsilon;
     int fft_n0, fft_n1;
     int psf_interp;   /* 1: bilinear interpolation of the lattice PSFs (project option) */
+    /* project option, no reference counterpart (its reg_eps and itn are parsed, never used):
+     * iters FISTA steps from the damped solution x0 on 1/2|s*x-m|^2 + mu/2|x|^2 + lambda|x|_1,
+     * mu = reg_l2*max|S^|^2, step 1/(max|S^|^2 + mu), soft threshold reg_l1*max|x0| */
+    int iters;
+    float reg_l1, reg_l2;
 } orc_decon_params;
 
 int orc_decon_geometry(const orc_decon_params *p, int *out /* 16 ints, see swd_oracle.c */);

@@ -56,7 +56,7 @@ class DeconParams(C.Structure):
     _fields_ = [("nx", C.c_int), ("nz", C.c_int), ("psfwinx", C.c_int), ("psfwinz", C.c_int),
                 ("filterwinx", C.c_int), ("filterwinz", C.c_int), ("snapwinx", C.c_int), ("snapwinz", C.c_int),
                 ("epsilon", C.c_float), ("fft_nx", C.c_int), ("fft_nz", C.c_int), ("psf_interp", C.c_int),
-                ("workspace", C.c_int)]
+                ("workspace", C.c_int), ("iters", C.c_int), ("reg_l1", C.c_float), ("reg_l2", C.c_float)]
 
 
 _lib = None
@@ -449,9 +449,10 @@ class Engine:
         self._ck(lib().swd_preprocess(self._h, d.shape[0], d.shape[1], dt, _ptr(d), _ptr(out)))
         return out
 
-    def decon(self, migreal, migpsf, psfwin, filterwin, snapwin, epsilon, fft_n=(0, 0), psf_interp=0, workspace=0):
+    def decon(self, migreal, migpsf, psfwin, filterwin, snapwin, epsilon, fft_n=(0, 0), psf_interp=0, workspace=0,
+              iters=0, reg_l1=0.0, reg_l2=0.0):
         return decon(migreal, migpsf, psfwin, filterwin, snapwin, epsilon, fft_n, ctx=self._h, psf_interp=psf_interp,
-                     workspace=workspace)
+                     workspace=workspace, iters=iters, reg_l1=reg_l1, reg_l2=reg_l2)
 
 
 def decon_geometry(nx, nz, psfwin, filterwin, snapwin, fft_n=(0, 0)):
@@ -464,15 +465,19 @@ def decon_geometry(nx, nz, psfwin, filterwin, snapwin, fft_n=(0, 0)):
     return w.value, fx.value, fz.value
 
 
-def decon(migreal, migpsf, psfwin, filterwin, snapwin, epsilon, fft_n=(0, 0), ctx=None, psf_interp=0, workspace=0):
+def decon(migreal, migpsf, psfwin, filterwin, snapwin, epsilon, fft_n=(0, 0), ctx=None, psf_interp=0, workspace=0,
+          iters=0, reg_l1=0.0, reg_l2=0.0):
     """Windowed wavenumber PSF deconvolution on the GPU (decon2d_mine's window loop);
     psf_interp=1 blends the four lattice PSFs around each window bilinearly; workspace=1 keeps
     every window's transform buffer in global memory (automatic for windows too large for
-    shared memory)."""
+    shared memory); iters > 0 refines each window by FISTA with the L1 threshold reg_l1 (a
+    fraction of the damped solution's peak) and the Tikhonov weight reg_l2 (a fraction of the
+    PSF spectrum's peak power)."""
     migreal, migpsf = _f32(migreal), _f32(migpsf)
     nx, nz = migreal.shape
     p = DeconParams(nx, nz, psfwin[0], psfwin[1], filterwin[0], filterwin[1], snapwin[0], snapwin[1],
-                    float(epsilon), fft_n[0], fft_n[1], int(psf_interp), int(workspace))
+                    float(epsilon), fft_n[0], fft_n[1], int(psf_interp), int(workspace), int(iters), float(reg_l1),
+                    float(reg_l2))
     dec = np.zeros((nx, nz), np.float32)
     coef = np.zeros((nx, nz), np.float32)
     rc = lib().swd_decon(ctx, C.byref(p), _ptr(migreal), _ptr(migpsf), _ptr(dec), _ptr(coef))

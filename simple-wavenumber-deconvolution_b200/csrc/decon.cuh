@@ -16,6 +16,14 @@
 // transforms into shared memory, transforms it there and writes it back (dft2_staged), with
 // the same per-output arithmetic, so both variants give the same bits.
 //
+// Iterative option (iters > 0, no counterpart in the reference, which parses reg_eps and itn
+// but never uses them): the damped solution x0 = IDFT2(D)/n of the window starts FISTA on
+//   f(x) = 1/(2n) |S^ X^ - M^|^2 + mu/2 |x|^2 + lambda |x|_1,   mu = reg_l2 * max|S^|^2,
+// step tau = 1/(max|S^|^2 + mu), soft threshold tau*lambda = reg_l1 * max|x0|; gradient
+// IDFT2((|S^|^2 + mu) Y^ - M^ conj S^)/n, two 2D transforms per iteration; B = M^ conj S^,
+// P = |S^|^2 and the iterates live in the global workspace.  The output is n*x, the scale of
+// the direct path's unnormalised inverse transform.
+//
 // The buffer index is ixx*FZ + izz and the 2D transform is taken over (n0 rows x n1
 // columns) of that linear buffer, which is how the reference plans it
 // (fftw_plan_dft_2d(fullwz, fullwx) on an x-major buffer, :490-493).  Transforms are FP32
@@ -37,6 +45,15 @@ struct DeconGeo {
     float epsilon;
     int psf_interp;   // 1: bilinear interpolation of the lattice PSFs (project option)
     int staged;       // 1: buffer in a global workspace, passes staged through shared memory
+    int iters;        // FISTA iterations (0: the reference's direct division)
+    float reg_l1, reg_l2;
+};
+
+// Per-CTA global scratch of the iterative option (n = FX*FZ elements each)
+struct DeconIter {
+    float2 *B;        // M^ conj S^
+    float *P;         // |S^|^2
+    float *X, *XP;    // current and previous iterate
 };
 
 // Bracketing lattice points of a window-centre coordinate for PSF interpolation: f0 =
@@ -145,9 +162,64 @@ __device__ __forceinline__ void decon_twiddles(const DeconGeo &g, float2 *tw0, f
 // One window w on the buffer Z (shared memory, or global memory when STAGED with the shared
 // chunk of cap elements); the twiddle tables are filled by the caller.
 template <bool STAGED>
+__device__ __forceinline__ void window_dft2(float2 *Z, float2 *chunk, int cap, const float2 *tw0, const float2 *tw1,
+                                            const DeconGeo &g, int sign)
+{
+    if (STAGED) dft2_staged(Z, chunk, cap, tw0, tw1, g.n0, g.n1, sign);
+    else dft2(Z, tw0, tw1, g.n0, g.n1, sign);
+}
+
+// FISTA refinement of the window solution held (unnormalised) in Z.x; leaves n*x in Z.x.
+template <bool STAGED>
+__device__ void decon_iterate(const DeconGeo &g, float2 *Z, const DeconIter &it, float fmax, const float2 *tw0,
+                              const float2 *tw1, float2 *chunk, int cap)
+{
+    __shared__ unsigned s_xmax;
+    const int n = g.FX * g.FZ, tid = threadIdx.x, nthr = blockDim.x;
+    const float invn = 1.0f / (float)n, mu = g.reg_l2 * fmax, tau = 1.0f / (fmax + mu);
+    if (tid == 0) s_xmax = 0u;
+    __syncthreads();
+    float am = 0.f;
+    for (int j = tid; j < n; j += nthr) {
+        const float x = Z[j].x * invn;
+        it.X[j] = x;
+        it.XP[j] = x;
+        am = fmaxf(am, fabsf(x));
+    }
+    for (int o = 16; o > 0; o >>= 1) am = fmaxf(am, __shfl_xor_sync(0xffffffffu, am, o));
+    if ((tid & 31) == 0) atomicMax(&s_xmax, __float_as_uint(am));
+    __syncthreads();
+    const float thr = g.reg_l1 * __uint_as_float(s_xmax);
+    float t = 1.0f;
+    for (int k = 0; k < g.iters; k++) {
+        const float tn = 0.5f * (1.0f + sqrtf(1.0f + 4.0f * t * t)), beta = (t - 1.0f) / tn;
+        t = tn;
+        for (int j = tid; j < n; j += nthr) Z[j] = make_float2(it.X[j] + beta * (it.X[j] - it.XP[j]), 0.f);
+        __syncthreads();
+        window_dft2<STAGED>(Z, chunk, cap, tw0, tw1, g, -1);
+        for (int j = tid; j < n; j += nthr) {
+            const float2 y = Z[j], b = it.B[j];
+            const float q = it.P[j] + mu;
+            Z[j] = make_float2(q * y.x - b.x, q * y.y - b.y);
+        }
+        __syncthreads();
+        window_dft2<STAGED>(Z, chunk, cap, tw0, tw1, g, +1);
+        for (int j = tid; j < n; j += nthr) {
+            const float x = it.X[j], y = x + beta * (x - it.XP[j]);
+            const float v = y - tau * (Z[j].x * invn);
+            it.XP[j] = x;
+            it.X[j] = copysignf(fmaxf(fabsf(v) - thr, 0.f), v);
+        }
+        __syncthreads();
+    }
+    for (int j = tid; j < n; j += nthr) Z[j].x = it.X[j] * (float)n;
+    __syncthreads();
+}
+
+template <bool STAGED>
 __device__ void decon_window(const DeconGeo &g, const float *__restrict__ mig, const float *__restrict__ psf,
                              float *__restrict__ winout, int w, float2 *Z, const float2 *tw0, const float2 *tw1,
-                             float2 *chunk, int cap)
+                             float2 *chunk, int cap, const DeconIter &itr)
 {
     const int n = g.FX * g.FZ;
     __shared__ float s_ppmax, s_psfmax;
@@ -216,8 +288,7 @@ __device__ void decon_window(const DeconGeo &g, const float *__restrict__ mig, c
         Z[ixx * g.FZ + izz].y = (float)((double)psf_val(ixx, izz) / psm);
     }
     __syncthreads();
-    if (STAGED) dft2_staged(Z, chunk, cap, tw0, tw1, g.n0, g.n1, -1);
-    else dft2(Z, tw0, tw1, g.n0, g.n1, -1);
+    window_dft2<STAGED>(Z, chunk, cap, tw0, tw1, g, -1);
     // |S^|^2 maximum over all bins (float compare of the double square, :625-633)
     float fm = 0.f;
     for (int j = tid; j < n; j += nthr) {
@@ -246,10 +317,19 @@ __device__ void decon_window(const DeconGeo &g, const float *__restrict__ mig, c
         const double di = (-mr * si + mi * sr) / (double)den;
         Z[j] = make_float2((float)dr, (float)di);
         if (jm != j) Z[jm] = make_float2((float)dr, (float)-di);   // D(-k) = conj D(k)
+        if (g.iters > 0) {
+            const float2 b = make_float2((float)(mr * sr + mi * si), (float)(mi * sr - mr * si));
+            const float pk = (float)(sr * sr + si * si);
+            itr.B[j] = b;
+            itr.P[j] = pk;
+            itr.B[jm] = make_float2(b.x, -b.y);
+            itr.P[jm] = pk;
+        }
     }
     __syncthreads();
-    if (STAGED) dft2_staged(Z, chunk, cap, tw0, tw1, g.n0, g.n1, +1);
-    else dft2(Z, tw0, tw1, g.n0, g.n1, +1);
+    window_dft2<STAGED>(Z, chunk, cap, tw0, tw1, g, +1);
+    if (g.iters > 0 && __uint_as_float(s_fmax) > 0.0f)
+        decon_iterate<STAGED>(g, Z, itr, __uint_as_float(s_fmax), tw0, tw1, chunk, cap);
     const int nout = g.outwinx * g.outwinz;
     float *o = winout + (size_t)w * nout;
     for (int j = tid; j < nout; j += nthr) {
@@ -266,22 +346,50 @@ __global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *_
     extern __shared__ float2 sm[];
     float2 *Z = sm, *tw0 = Z + (size_t)g.FX * g.FZ, *tw1 = tw0 + g.n0;
     decon_twiddles(g, tw0, tw1);
-    decon_window<false>(g, mig, psf, winout, blockIdx.x, Z, tw0, tw1, nullptr, 0);
+    decon_window<false>(g, mig, psf, winout, blockIdx.x, Z, tw0, tw1, nullptr, 0, DeconIter{});
 }
 
-// Persistent CTAs, each with its own buffer of FX*FZ elements in the global workspace ws,
-// working through windows blockIdx.x, blockIdx.x + gridDim.x, ...; shared memory holds the
-// twiddles and a chunk of cap elements for the staged passes.
-__global__ void __launch_bounds__(512) k_decon_window_staged(DeconGeo g, const float *__restrict__ mig,
-                                                             const float *__restrict__ psf, float *__restrict__ winout,
-                                                             float2 *__restrict__ ws, int cap)
+// Floats of global workspace one persistent CTA of k_decon_window_ws needs: the staged
+// transform buffer and the iterative option's B, P and iterates.
+__host__ __device__ inline size_t decon_ws_floats(const DeconGeo &g)
+{
+    const size_t n = (size_t)g.FX * g.FZ;
+    return ((g.staged ? 2 * n : 0) + (g.iters > 0 ? 5 * n : 0) + 63) & ~(size_t)63;   // 256-byte aligned slices
+}
+
+// Persistent CTAs working through windows blockIdx.x, blockIdx.x + gridDim.x, ..., each with
+// decon_ws_floats(g) floats of the global workspace ws.  STAGED: the transform buffer is in
+// that workspace and shared memory holds the twiddles and a chunk of cap elements for the
+// staged passes; otherwise the buffer and the twiddles are in shared memory.
+template <bool STAGED>
+__global__ void __launch_bounds__(512) k_decon_window_ws(DeconGeo g, const float *__restrict__ mig,
+                                                         const float *__restrict__ psf, float *__restrict__ winout,
+                                                         float *__restrict__ ws, int cap)
 {
     extern __shared__ float2 sm[];
-    float2 *tw0 = sm, *tw1 = tw0 + g.n0, *chunk = tw1 + g.n1;
-    float2 *Z = ws + (size_t)blockIdx.x * g.FX * g.FZ;
+    const size_t n = (size_t)g.FX * g.FZ;
+    float *mine = ws + (size_t)blockIdx.x * decon_ws_floats(g);
+    float2 *Z, *tw0, *chunk = nullptr;
+    if (STAGED) {
+        Z = (float2 *)mine;
+        mine += 2 * n;
+        tw0 = sm;
+        chunk = sm + g.n0 + g.n1;
+    } else {
+        Z = sm;
+        tw0 = sm + n;
+    }
+    float2 *tw1 = tw0 + g.n0;
+    DeconIter itr{};
+    if (g.iters > 0) {
+        itr.B = (float2 *)mine;
+        itr.P = mine + 2 * n;
+        itr.X = itr.P + n;
+        itr.XP = itr.X + n;
+    }
     decon_twiddles(g, tw0, tw1);
     for (int w = blockIdx.x; w < g.totalnum; w += gridDim.x) {
-        decon_window<true>(g, mig, psf, winout, w, Z, tw0, tw1, chunk, cap);
+        decon_window<STAGED>(g, mig, psf, winout, w, Z, tw0, tw1, chunk, cap, itr);
         __syncthreads();   // the next window's fill overwrites Z and the shared scalars
     }
 }

@@ -68,6 +68,11 @@ inline int ext_int(const std::map<std::string, std::string> &kv, const char *k, 
     auto it = kv.find(k);
     return it == kv.end() ? def : atoi(it->second.c_str());
 }
+inline float ext_float(const std::map<std::string, std::string> &kv, const char *k, float def)
+{
+    auto it = kv.find(k);
+    return it == kv.end() ? def : (float)atof(it->second.c_str());
+}
 inline std::string ext_str(const std::map<std::string, std::string> &kv, const char *k, const char *def)
 {
     auto it = kv.find(k);

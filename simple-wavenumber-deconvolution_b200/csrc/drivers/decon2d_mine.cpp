@@ -8,7 +8,9 @@
 // All windows run as one batched launch on the GPU (swd_decon).
 // Extensions (parameter.txt lines `swd.key = value`): device, psf_interp (1: bilinear blend of
 // the lattice PSFs around each window, a project option), fft_nx / fft_nz (zero-padded
-// FFT size instead of filterwin + psfwin - 1).
+// FFT size instead of filterwin + psfwin - 1), iterative (1: the regularised deconvolution with
+// the parameter file's own L1 coefficient reg_eps, L2 coefficient and iteration count, which
+// the reference reads in part but never uses; reg_l1 / reg_l2 / iters override them).
 #include <math.h>
 #include "common.h"
 
@@ -17,7 +19,8 @@ using namespace drv;
 int main(int, char **)
 {
     int nx, nz, psfwinx, psfwinz, filterwinx, filterwinz, snapwinx, snapwinz, shift_flag;
-    float epsilon, reg_eps;
+    float epsilon, reg_eps, reg_l2_file = 0.0f;
+    int itn_file = 0;
     char vp_file[150], vp0_file[150], rho_file[150], migreal_file[150], migpsf_file[150], decon_file[150], ipsf_file[150];
     {
         ParamReader r("parameter.txt");
@@ -32,6 +35,13 @@ int main(int, char **)
         if (!r.ok) {
             printf("parameter.txt is incomplete\n");
             return 1;
+        }
+        // the two entries after reg_eps (L2 coefficient, iteration count) are optional
+        r.get(&reg_l2_file);
+        r.get(&itn_file);
+        if (!r.ok) {
+            reg_l2_file = 0.0f;
+            itn_file = 0;
         }
     }
     auto ext = extensions("parameter.txt");
@@ -80,6 +90,12 @@ int main(int, char **)
 
     swd_decon_params p{nx, nz, psfwinx, psfwinz, filterwinx, filterwinz, snapwinx, snapwinz, epsilon,
                        ext_int(ext, "fft_nx", 0), ext_int(ext, "fft_nz", 0), ext_int(ext, "psf_interp", 0)};
+    if (ext_int(ext, "iterative", 0)) {
+        p.iters = ext_int(ext, "iters", itn_file);
+        p.reg_l1 = ext_float(ext, "reg_l1", reg_eps);
+        p.reg_l2 = ext_float(ext, "reg_l2", reg_l2_file);
+        printf("Iterative regularised deconvolution: %d iterations, L1 %g, L2 %g\n", p.iters, p.reg_l1, p.reg_l2);
+    }
     int windows = 0, fx = 0, fz = 0;
     if (swd_decon_geometry(&p, &windows, &fx, &fz) != SWD_OK) {
         printf("Invalid deconvolution window geometry\n");

@@ -1024,36 +1024,50 @@ static int decon_geo(const swd_decon_params *p, DeconGeo &g)
     if (g.n0 > 512 || g.n1 > 512) return SWD_ERR_ARG;
     if (p->workspace != 0 && p->workspace != 1) return SWD_ERR_ARG;
     g.staged = p->workspace == 1 || (size_t)g.FX * g.FZ * 8 + (g.n0 + g.n1) * 8 > 200 * 1024;
+    if (p->iters < 0 || p->iters > 100000 || !(p->reg_l1 >= 0.0f) || !(p->reg_l2 >= 0.0f)) return SWD_ERR_ARG;
+    g.iters = p->iters;
+    g.reg_l1 = p->reg_l1;
+    g.reg_l2 = p->reg_l2;
     // the PSF lattice must hold at least 7 cells per axis so the clamp range [3, n-4] exists
     if (g.nxwpsf < 7 || g.nzwpsf < 7) return SWD_ERR_ARG;
     return SWD_OK;
 }
 
-// Launch shape of the staged window kernel: a 96 KB shared chunk (at least one transform) and
-// as many persistent CTAs as are resident at once, each owning FX*FZ float2 of workspace.
+// Launch shape of the persistent window kernel (staged transforms or the iterative option): a
+// 96 KB shared chunk when staged, else the buffer in shared memory; as many CTAs as are
+// resident at once, each owning decon_ws_floats(g) floats of workspace.
+static bool decon_persistent(const DeconGeo &g) { return g.staged || g.iters > 0; }
 static size_t decon_staged_cap(const DeconGeo &g) { return std::max<size_t>(12288, std::max(g.n0, g.n1)); }
-static size_t decon_staged_smem(const DeconGeo &g) { return sizeof(float2) * (g.n0 + g.n1 + decon_staged_cap(g)); }
-static int decon_staged_blocks(const DeconGeo &g, int dev)
+static size_t decon_ws_smem(const DeconGeo &g)
+{
+    return sizeof(float2) * (g.n0 + g.n1 + (g.staged ? decon_staged_cap(g) : (size_t)g.FX * g.FZ));
+}
+static const void *decon_ws_kernel(const DeconGeo &g)
+{
+    return g.staged ? (const void *)k_decon_window_ws<true> : (const void *)k_decon_window_ws<false>;
+}
+static int decon_ws_blocks(const DeconGeo &g, int dev)
 {
     int nsm = 0, occ = 0;
-    const size_t sm = decon_staged_smem(g);
+    const size_t sm = decon_ws_smem(g);
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    if (cudaFuncSetAttribute(k_decon_window_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_decon_window_staged, 512, sm) != cudaSuccess)
+    if (cudaFuncSetAttribute(decon_ws_kernel(g), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decon_ws_kernel(g), 512, sm) != cudaSuccess)
         return 0;
     return std::max(1, std::min(g.totalnum, nsm * std::max(occ, 1)));
 }
 
 // Window kernel of g: one CTA per window in shared memory, or nblk persistent CTAs over the
-// workspace ws (staged).
+// workspace ws (staged transforms or iterations).
 static cudaError_t launch_decon_windows(const DeconGeo &g, const float *mig, const float *psf, float *winout,
-                                        float2 *ws, int nblk, cudaStream_t st)
+                                        float *ws, int nblk, cudaStream_t st)
 {
-    if (g.staged) {
-        const size_t sm = decon_staged_smem(g);
-        cudaError_t e = cudaFuncSetAttribute(k_decon_window_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (decon_persistent(g)) {
+        const size_t sm = decon_ws_smem(g);
+        cudaError_t e = cudaFuncSetAttribute(decon_ws_kernel(g), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        k_decon_window_staged<<<nblk, 512, sm, st>>>(g, mig, psf, winout, ws, (int)decon_staged_cap(g));
+        if (g.staged) k_decon_window_ws<true><<<nblk, 512, sm, st>>>(g, mig, psf, winout, ws, (int)decon_staged_cap(g));
+        else k_decon_window_ws<false><<<nblk, 512, sm, st>>>(g, mig, psf, winout, ws, 0);
     } else {
         const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + g.n0 + g.n1);
         cudaError_t e = cudaFuncSetAttribute(k_decon_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -1796,9 +1810,9 @@ int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, 
         const bool din = is_device_ptr(migreal) && is_device_ptr(migpsf);
         const bool dout = is_device_ptr(mig_dec) && is_device_ptr(mig_coef);
         DevBuf &bin = ctx->dcn[0], &bcoef = ctx->dcn[1], &bwin = ctx->dcn[2], &bout = ctx->dcn[3], &bws = ctx->dcn[4];
-        const int nblk = g.staged ? decon_staged_blocks(g, ctx->dev) : 0;
-        if (g.staged && nblk < 1) { rc = fail(ctx, SWD_ERR_CUDA, "decon: no launch shape for the staged window kernel"); break; }
-        if (g.staged) rc = ensure(ctx, bws, sizeof(float2) * (size_t)nblk * g.FX * g.FZ);
+        const int nblk = decon_persistent(g) ? decon_ws_blocks(g, ctx->dev) : 0;
+        if (decon_persistent(g) && nblk < 1) { rc = fail(ctx, SWD_ERR_CUDA, "decon: no launch shape for the window kernel"); break; }
+        if (decon_persistent(g)) rc = ensure(ctx, bws, sizeof(float) * (size_t)nblk * decon_ws_floats(g));
         if (!rc && !din) rc = ensure(ctx, bin, sizeof(float) * 2 * np);
         if (!rc) rc = ensure(ctx, bcoef, sizeof(float) * nout);
         if (!rc) rc = ensure(ctx, bwin, sizeof(float) * nout * g.totalnum);
@@ -1810,7 +1824,7 @@ int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, 
         if (!rc && cudaMemcpyAsync(bcoef.p, coefr.data(), sizeof(float) * nout, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
             rc = fail(ctx, SWD_ERR_CUDA, "decon: coefficient upload");
         if (!rc) {
-            cudaError_t e = launch_decon_windows(g, im, ps, F(bwin), (float2 *)bws.p, nblk, ctx->stream);
+            cudaError_t e = launch_decon_windows(g, im, ps, F(bwin), F(bws), nblk, ctx->stream);
             if (e == cudaSuccess) {
                 k_decon_gather<<<592, 256, 0, ctx->stream>>>(g, F(bwin), F(bcoef), od, oc);
                 e = cudaGetLastError();
@@ -1839,9 +1853,9 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
     DeconGeo g;
     if (!p || decon_geo(p, g) != SWD_OK) return SWD_ERR_ARG;
     const size_t nout = (size_t)g.outwinx * g.outwinz;
-    // scratch: taper, window slots, then (staged) the CTA workspaces from an even offset; the
-    // staged kernel runs on as many CTAs as have a workspace that fits
-    const size_t used = (size_t)g.totalnum * nout + nout, wsoff = (used + 1) & ~(size_t)1;
+    // scratch: taper, window slots, then (persistent kernel) the CTA workspaces from a 256-byte
+    // aligned offset; that kernel runs on as many CTAs as have a workspace that fits
+    const size_t used = (size_t)g.totalnum * nout + nout, wsoff = (used + 63) & ~(size_t)63;
     if (used > SWD_DECON_STATIC_SCRATCH_FLOATS) return SWD_ERR_CAPACITY;
     int nblk = 0;
     const void *ptrs[4] = {migreal, migpsf, mig_dec, mig_coef};
@@ -1857,16 +1871,16 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
         }
         scratch_addr[dev] = (float *)a;
     }
-    if (g.staged) {
-        const size_t per = (size_t)2 * g.FX * g.FZ;
+    if (decon_persistent(g)) {
+        const size_t per = decon_ws_floats(g);
         const size_t fit = wsoff < SWD_DECON_STATIC_SCRATCH_FLOATS ? (SWD_DECON_STATIC_SCRATCH_FLOATS - wsoff) / per : 0;
-        nblk = std::min<long long>(decon_staged_blocks(g, dev), (long long)fit);
+        nblk = std::min<long long>(decon_ws_blocks(g, dev), (long long)fit);
         if (nblk < 1) return SWD_ERR_CAPACITY;
     }
     float *coefr = scratch_addr[dev], *winout = coefr + nout;
     cudaStream_t st = (cudaStream_t)cuda_stream;
     k_decon_taper<<<(int)((nout + 255) / 256), 256, 0, st>>>(coefr, g.outwinx, g.outwinz, p->snapwinx, p->snapwinz);
-    if (launch_decon_windows(g, migreal, migpsf, winout, (float2 *)(coefr + wsoff), nblk, st) != cudaSuccess)
+    if (launch_decon_windows(g, migreal, migpsf, winout, coefr + wsoff, nblk, st) != cudaSuccess)
         return SWD_ERR_CUDA;
     k_decon_gather<<<592, 256, 0, st>>>(g, winout, coefr, mig_dec, mig_coef);
     return cudaGetLastError() == cudaSuccess ? SWD_OK : SWD_ERR_CUDA;

@@ -114,6 +114,33 @@ def test_decon2d_mine_reproduces_the_reference_program():
         assert rel_l2(dec, g[f"dec{k}"]) < 1e-3
 
 
+@pytest.mark.gpu
+def test_decon2d_mine_iterative_option(orc):
+    """`swd.iterative = 1` runs the regularised deconvolution with the parameter file's own
+    reg_eps (L1), L2 coefficient and iteration count, the entries the reference lists after
+    reg_eps; checked against the oracle."""
+    mk = _mkg("make_golden")
+    nx, nz, psf, flt, snap, eps, seed = mk.DECON_CASES[0]
+    mig, psfimg, vp = mk.synthetic_decon_inputs(nx, nz, psf, seed)
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        (d / "input").mkdir()
+        (d / "output").mkdir()
+        mk.write_decon_params(d / "parameter.txt", nx, nz, psf, flt, snap, eps)
+        with open(d / "parameter.txt", "a") as f:
+            f.write("--Regularization coefficient: reg_eps L2-5e-3\n  6.0e-2\n-- total iteration number: itn\n  30\n"
+                    "swd.iterative = 1\n")
+        vp.tofile(d / "input" / "acc_vp.bin")
+        vp.tofile(d / "input" / "ini_vp.bin")
+        mig.tofile(d / "input" / "mig.bin")
+        psfimg.tofile(d / "input" / "psf.bin")
+        r = subprocess.run([str(PKG_DIR / "decon2d_mine")], cwd=d, check=True, capture_output=True, text=True)
+        assert "30 iterations" in r.stdout
+        dec = np.fromfile(d / "output" / "dec.bin", np.float32).reshape(nx, nz)
+    ref, _ = orc.decon(nx, nz, mig, psfimg, psf, flt, snap, eps, iters=30, reg_l1=2e-2, reg_l2=6e-2)
+    assert rel_l2(dec, ref) < 1e-3
+
+
 REF_ON_SWD = ROOT / "oracle" / "_ref"
 
 

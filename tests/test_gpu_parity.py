@@ -415,3 +415,27 @@ def test_rtm_angle_gathers_reject_stored_source(case, swd, orc):
             case.E.rtm_shot(case.shot, case.rick, data, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK | swd.RTM_CIG)
     finally:
         case.E.set_source_storage(0)
+
+
+@pytest.mark.parametrize("ws", [0, 1], ids=["shared", "workspace"])
+def test_decon_iterative_matches_oracle(swd, orc, ws):
+    """The iterative regularised deconvolution (FISTA, L1 threshold and Tikhonov damping)
+    against the oracle's FP64 restatement, with the transform buffer in shared memory and in
+    the global workspace (same bits)."""
+    rng = np.random.default_rng(14)
+    nx, nz = 160, 130
+    mig = rng.standard_normal((nx, nz)).astype(np.float32)
+    psf = np.zeros((nx, nz), np.float32)
+    psf[5::11, 5::11] = 1.0
+    psf[6::11, 5::11] = -0.5
+    psf[5::11, 7::11] = 0.3
+    geo = ((11, 11), (21, 21), (5, 5))
+    kw = dict(iters=40, reg_l1=2e-2, reg_l2=6e-2)
+    got, coef = swd.decon(mig, psf, *geo, 5e-4, workspace=ws, **kw)
+    ref, ref_coef = orc.decon(nx, nz, mig, psf, *geo, 5e-4, **kw)
+    direct, _ = swd.decon(mig, psf, *geo, 5e-4)
+    assert np.array_equal(coef, ref_coef)
+    assert rel_l2(got, ref) < TOL_DECON
+    assert rel_l2(got, direct) > 1e-2
+    other, _ = swd.decon(mig, psf, *geo, 5e-4, workspace=1 - ws, **kw)
+    assert np.array_equal(got, other)

@@ -204,3 +204,43 @@ def test_oracle_born_is_the_linearised_forward(orc):
             outs.append(orc.forward(M2, G, rick, dtype=np.float64)["seis"])
         errs.append(rel_l2((outs[0] - outs[1]) / (2 * eps), d_born))
     assert errs[1] < 1e-4 and errs[0] / errs[1] > 30
+
+
+def _decon_case():
+    rng = np.random.default_rng(31)
+    nx, nz = 120, 100
+    mig = rng.standard_normal((nx, nz)).astype(np.float32)
+    psf = np.zeros((nx, nz), np.float32)
+    psf[5::11, 5::11] = 1.0
+    psf[6::11, 5::11] = -0.5
+    psf[5::11, 7::11] = 0.3
+    return nx, nz, mig, psf
+
+
+def test_decon_oracle_iterations_fixed_point_and_tikhonov_limit(orc):
+    """The iterative option's oracle: started at the damped solution of the same damping and
+    without the L1 term, FISTA stays at it (it is the minimiser); with a different damping
+    reg_l2 it converges to the direct solution of epsilon = reg_l2."""
+    nx, nz, mig, psf = _decon_case()
+    geo = ((11, 11), (21, 21), (5, 5))
+    d1, c1 = orc.decon(nx, nz, mig, psf, *geo, 1e-2)
+    it1, ic1 = orc.decon(nx, nz, mig, psf, *geo, 1e-2, iters=20, reg_l1=0.0, reg_l2=1e-2)
+    assert np.array_equal(c1, ic1)
+    assert rel_l2(it1, d1) < 1e-6
+    d5, _ = orc.decon(nx, nz, mig, psf, *geo, 5e-2)
+    it5, _ = orc.decon(nx, nz, mig, psf, *geo, 1e-3, iters=200, reg_l1=0.0, reg_l2=5e-2)
+    d3, _ = orc.decon(nx, nz, mig, psf, *geo, 1e-3)
+    assert rel_l2(d3, d5) > 1e-2            # the two dampings differ visibly
+    assert rel_l2(it5, d5) < 1e-5
+
+
+def test_decon_oracle_l1_threshold_sparsifies(orc):
+    """A positive L1 threshold shrinks the deconvolved image (smaller L1 norm, more exact
+    zeros) and leaves it close to the damped solution for a small threshold."""
+    nx, nz, mig, psf = _decon_case()
+    geo = ((11, 11), (21, 21), (5, 5))
+    base, _ = orc.decon(nx, nz, mig, psf, *geo, 5e-2, iters=60, reg_l1=0.0, reg_l2=5e-2)
+    small, _ = orc.decon(nx, nz, mig, psf, *geo, 5e-2, iters=60, reg_l1=1e-3, reg_l2=5e-2)
+    big, _ = orc.decon(nx, nz, mig, psf, *geo, 5e-2, iters=60, reg_l1=5e-2, reg_l2=5e-2)
+    assert rel_l2(small, base) < 5e-2
+    assert np.abs(big).sum() < np.abs(small).sum() < np.abs(base).sum()
