@@ -162,8 +162,9 @@ def algorithmic_bytes(kernel, w, cp, strip_len, r_n, strip_esz=4):
         #                        source v, p r/w, vp, rho, dp/dt (interior); strips
         return 28 * N + 28 * Ni + 8 * x_v + strip_esz * strip_len
     if kernel == "bwd_2":      # receiver v, p r/w, ck (all cells) + phi in the frame; source p, v r/w,
-        #                        cbx, cbz (interior); dp/dt and FP64 I, S r/w (interior); traces
-        return 20 * N + 64 * Ni + 8 * x_p + 4 * r_n
+        #                        cbx, cbz (interior); imaging (interior): dp/dt, the FP32 block sums of
+        #                        I and S r/w every step, the FP64 I and S r/w on one step in 64; traces
+        return 20 * N + 28 * Ni + 20 * Ni + Ni // 2 + 8 * x_p + 4 * r_n
     if kernel == "fwd_step":   # one fused launch per forward step: p, vx, vz r/w, vp, rho, CPML, strips
         return 32 * N + 8 * (x_v + x_p) + strip_esz * strip_len + 4 * r_n
     if kernel == "bwd_step":   # one fused launch per backward step: receiver 24N, material 8N, source 24Ni, FP64 image 32Ni
@@ -340,6 +341,8 @@ def run_ours(args, rank, world, dist):
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": ab, "avg_launch_us": live[dom] * 1e3,
                      "kernels_us": {k: v * 1e3 for k, v in live.items()},
+                     "kernels_frac": {k: algorithmic_bytes(k, w, cp, slen, r_n, 4 if strips == "f32" else 2) / v / 1e6 / peak
+                                      for k, v in live.items()},
                      "step_us": {k: per_launch[k] * 1e3 for k in ("fwd_pass_step", "bwd_pass_step") if k in per_launch},
                      "timing": "CUDA events around each whole forward / backward pass of every timed shot (per step = "
                                "pass / steps), split between a step's two launches by the ratio of events around one "

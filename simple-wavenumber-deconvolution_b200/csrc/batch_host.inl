@@ -118,6 +118,10 @@ static int rtm_batch_run(swd_ctx *ctx, const swd_shot *shots, const float *const
     CKR(ensure_bgrid(ctx, ctx->bat.dpdt, sizeof(float), nb));
     CKR(ensure_bgrid(ctx, ctx->bat.I, sizeof(double), nb));
     CKR(ensure_bgrid(ctx, ctx->bat.S, sizeof(double), nb));
+    if (ctx->image_blocks) {
+        CKR(ensure_bgrid(ctx, ctx->bat.Ip, sizeof(float), nb));
+        CKR(ensure_bgrid(ctx, ctx->bat.Sp, sizeof(float), nb));
+    }
     // boundary strips: [shot][nt_max][slen] (+ scales [shot][nt_max][nscale] at 16 bits); the
     // per-shot stride uses the context's nt_max so every batch shares one captured graph
     const dim3 grid2 = grid_blocks(ctx);
@@ -185,6 +189,8 @@ static int rtm_batch_run(swd_ctx *ctx, const swd_shot *shots, const float *const
     bb.rdata = rms;
     bb.I = D(ctx->bat.I);
     bb.S = D(ctx->bat.S);
+    bb.Ip = ctx->image_blocks ? F(ctx->bat.Ip) : nullptr;
+    bb.Sp = ctx->image_blocks ? F(ctx->bat.Sp) : nullptr;
     bb.bt = bt;
     const int nbk = probe_steps > 0 ? std::min(probe_steps, ntmax - 1) : ntmax - 1;
     {
@@ -294,6 +300,10 @@ int swd_set_option(swd_ctx *ctx, int option, int value)
             if (value < 0 || value > 64) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_BATCH takes 0 (autotune) .. 64");
             ctx->batch_opt = value;
             return SWD_OK;
+        case SWD_OPT_IMAGE_BLOCKS:
+            if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_IMAGE_BLOCKS takes 0 or 1");
+            ctx->image_blocks = value;
+            return SWD_OK;
         default:
             return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
@@ -306,6 +316,7 @@ int swd_get_option(swd_ctx *ctx, int option, int *value)
         case SWD_OPT_GRAPHS: *value = ctx->use_graphs; return SWD_OK;
         case SWD_OPT_BATCH: *value = ctx->batch_opt; return SWD_OK;
         case SWD_OPT_BATCH_TUNED: *value = ctx->batch_tuned; return SWD_OK;
+        case SWD_OPT_IMAGE_BLOCKS: *value = ctx->image_blocks; return SWD_OK;
         default: return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
 }

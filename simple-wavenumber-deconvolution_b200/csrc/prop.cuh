@@ -670,6 +670,7 @@ struct BwdArgs {
     Wells wells;
     const float *rdata;  // [r_n][nt] preprocessed data injected at the receivers
     double *I, *S, *R;   // FP64 imaging accumulators (R nullable)
+    float *Ip, *Sp, *Rp; // FP32 sums of the current block of IMG_BLOCK steps (nullptr: FP64 every step)
     Batch bt;            // the BATCH instantiations: shot = blockIdx.z
     DpStore ds;          // stored-source backward (k_bwd_rcv_*): dp/dt of forward step it+1
 };
@@ -690,6 +691,8 @@ __device__ __forceinline__ bool bwd_view(BwdArgs &a, int &it)
     a.I += o;
     a.S += o;
     if (a.R) a.R += o;
+    if (a.Ip) { a.Ip += o; a.Sp += o; }
+    if (a.Rp) a.Rp += o;
     a.sx = d.sx; a.sz = d.sz; a.nt = d.nt;
     a.wavsub += d.wav_off;
     a.wells.wcol += (size_t)b * a.g.ntx;
@@ -774,6 +777,87 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
     v_update4<LC, true>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0);
 }
 
+// Imaging condition of one backward step on four cells (sum_image_GPU_kernel_image,
+// acoustic_HLVSPRTMLc.cu:785-817): I += dp/dt * p_r, S += (dp/dt)^2, R += p_r^2.  Without
+// partial buffers every step adds its exact products into the FP64 accumulators.  With them
+// the products are summed in FP32 (one FMA rounding per step) over blocks of IMG_BLOCK steps
+// and each block sum is added into FP64 on the block's last step, it % IMG_BLOCK == 0, which
+// includes the pass's final step it = 0; per step that moves 16 bytes per cell instead of 32.
+constexpr int IMG_BLOCK = 64;
+
+__device__ __forceinline__ void fold4(double *acc, float *part, const bool in[4], float4 v, bool fold)
+{
+    if (fold) {
+        double2 *A2 = reinterpret_cast<double2 *>(acc);
+        double2 a0 = A2[0], a1 = A2[1];
+        double *av[4] = {&a0.x, &a0.y, &a1.x, &a1.y};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (in[k]) *av[k] += (double)elc(v, k);
+        A2[0] = a0;
+        A2[1] = a1;
+        st4(part, make_float4(0.f, 0.f, 0.f, 0.f));
+    } else {
+        st4(part, v);
+    }
+}
+
+__device__ __forceinline__ void image4(const BwdArgs &a, size_t ip, const bool in[4], float4 dp4, float4 pr, int it)
+{
+    if (a.Ip) {
+        const bool fold = it % IMG_BLOCK == 0;
+        float4 pi = ld4(a.Ip + ip), ps = ld4(a.Sp + ip);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (in[k]) {
+                el(pi, k) = fmaf(elc(dp4, k), elc(pr, k), elc(pi, k));
+                el(ps, k) = fmaf(elc(dp4, k), elc(dp4, k), elc(ps, k));
+            }
+        fold4(a.I + ip, a.Ip + ip, in, pi, fold);
+        fold4(a.S + ip, a.Sp + ip, in, ps, fold);
+        if (a.Rp) {
+            float4 pq = ld4(a.Rp + ip);
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (in[k]) el(pq, k) = fmaf(elc(pr, k), elc(pr, k), elc(pq, k));
+            fold4(a.R + ip, a.Rp + ip, in, pq, fold);
+        }
+        return;
+    }
+    double2 *I2 = reinterpret_cast<double2 *>(a.I + ip), *S2 = reinterpret_cast<double2 *>(a.S + ip);
+    double2 i0 = I2[0], i1 = I2[1], s0 = S2[0], s1 = S2[1];
+    double *iv[4] = {&i0.x, &i0.y, &i1.x, &i1.y}, *sv[4] = {&s0.x, &s0.y, &s1.x, &s1.y};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (!in[k]) continue;
+        const double dp = (double)elc(dp4, k);
+        *iv[k] += dp * (double)elc(pr, k);
+        *sv[k] += dp * dp;
+    }
+    I2[0] = i0; I2[1] = i1; S2[0] = s0; S2[1] = s1;
+    if (a.R) {
+        double2 *R2 = reinterpret_cast<double2 *>(a.R + ip);
+        double2 q0 = R2[0], q1 = R2[1];
+        double *rv[4] = {&q0.x, &q0.y, &q1.x, &q1.y};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (in[k]) *rv[k] += (double)elc(pr, k) * (double)elc(pr, k);
+        R2[0] = q0; R2[1] = q1;
+    }
+}
+
+// L2 prefetch of the imaging operands a step will read last
+__device__ __forceinline__ void image_prefetch(const BwdArgs &a, size_t ip, int it)
+{
+    if (a.Ip) {
+        prefetch_l2(a.Ip + ip);
+        prefetch_l2(a.Sp + ip);
+        if (it % IMG_BLOCK != 0) return;
+    }
+    prefetch_l2(a.I + ip);
+    prefetch_l2(a.S + ip);
+}
+
 template <int LC, bool BATCH = false>
 __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_2(const BwdArgs a0)
 {
@@ -793,8 +877,7 @@ __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_2(cons
 #pragma unroll
     for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
     if (any) {   // the imaging operands are read last: start their DRAM reads now
-        prefetch_l2(a.I + ip);
-        prefetch_l2(a.S + ip);
+        image_prefetch(a, ip, it);
         prefetch_l2(a.dpdt + ip);
     }
     // source wavefield velocities, interior only (:488-573)
@@ -842,30 +925,8 @@ __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_2(cons
             if (t[k] >= 0 && z0 + k < g.ntz) { el(pr, k) = a.rdata[(size_t)t[k] * a.nt + it]; wr = true; }
     }
     if (wr) st4(a.r.p + ip, pr);
-    // imaging condition in FP64 (sum_image_GPU_kernel_image :785-817)
-    if (any) {
-        const float4 dp4 = ld4(a.dpdt + ip);
-        double2 *I2 = reinterpret_cast<double2 *>(a.I + ip), *S2 = reinterpret_cast<double2 *>(a.S + ip);
-        double2 i0 = I2[0], i1 = I2[1], s0 = S2[0], s1 = S2[1];
-        double *iv[4] = {&i0.x, &i0.y, &i1.x, &i1.y}, *sv[4] = {&s0.x, &s0.y, &s1.x, &s1.y};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (!in[k]) continue;
-            const double dp = (double)elc(dp4, k);
-            *iv[k] += dp * (double)elc(pr, k);
-            *sv[k] += dp * dp;
-        }
-        I2[0] = i0; I2[1] = i1; S2[0] = s0; S2[1] = s1;
-        if (a.R) {
-            double2 *R2 = reinterpret_cast<double2 *>(a.R + ip);
-            double2 q0 = R2[0], q1 = R2[1];
-            double *rv[4] = {&q0.x, &q0.y, &q1.x, &q1.y};
-#pragma unroll
-            for (int k = 0; k < 4; k++)
-                if (in[k]) *rv[k] += (double)elc(pr, k) * (double)elc(pr, k);
-            R2[0] = q0; R2[1] = q1;
-        }
-    }
+    // imaging condition (sum_image_GPU_kernel_image :785-817)
+    if (any) image4(a, ip, in, ld4(a.dpdt + ip), pr, it);
 }
 
 // ------------------------------------------------------------------------------------
@@ -898,10 +959,7 @@ __global__ void __launch_bounds__(256, 5) k_bwd_rcv_p(const BwdArgs a)
     bool any = false;
 #pragma unroll
     for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
-    if (any) {
-        prefetch_l2(a.I + ip);
-        prefetch_l2(a.S + ip);
-    }
+    if (any) image_prefetch(a, ip, it);
     float4 pr;
     bool upd[4];
     p_update4<LC>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0, pr, upd);
@@ -915,29 +973,7 @@ __global__ void __launch_bounds__(256, 5) k_bwd_rcv_p(const BwdArgs a)
             if (t[k] >= 0 && z0 + k < g.ntz) { el(pr, k) = a.rdata[(size_t)t[k] * a.nt + it]; wr = true; }
     }
     if (wr) st4(a.r.p + ip, pr);
-    if (any) {
-        const float4 dp4 = load_dpdt(a.ds, g, it + 1, x, z0);
-        double2 *I2 = reinterpret_cast<double2 *>(a.I + ip), *S2 = reinterpret_cast<double2 *>(a.S + ip);
-        double2 i0 = I2[0], i1 = I2[1], s0 = S2[0], s1 = S2[1];
-        double *iv[4] = {&i0.x, &i0.y, &i1.x, &i1.y}, *sv[4] = {&s0.x, &s0.y, &s1.x, &s1.y};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (!in[k]) continue;
-            const double dp = (double)elc(dp4, k);
-            *iv[k] += dp * (double)elc(pr, k);
-            *sv[k] += dp * dp;
-        }
-        I2[0] = i0; I2[1] = i1; S2[0] = s0; S2[1] = s1;
-        if (a.R) {
-            double2 *R2 = reinterpret_cast<double2 *>(a.R + ip);
-            double2 q0 = R2[0], q1 = R2[1];
-            double *rv[4] = {&q0.x, &q0.y, &q1.x, &q1.y};
-#pragma unroll
-            for (int k = 0; k < 4; k++)
-                if (in[k]) *rv[k] += (double)elc(pr, k) * (double)elc(pr, k);
-            R2[0] = q0; R2[1] = q1;
-        }
-    }
+    if (any) image4(a, ip, in, load_dpdt(a.ds, g, it + 1, x, z0), pr, it);
 }
 
 // ------------------------------------------------------------------------------------

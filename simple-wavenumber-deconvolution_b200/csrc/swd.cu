@@ -64,7 +64,7 @@ struct swd_ctx {
     int ckpt_every = 50, ckpt_prec = SWD_STRIP_BF16;
     // batched RTM (swd_rtm_batch): every per-shot grid array is one allocation of per-shot slices
     struct BatchBufs {
-        DevBuf w[2][7], dpdt, I, S, strips, scale, rdata, wcol, wmap, desc, wav, reduce;
+        DevBuf w[2][7], dpdt, I, S, Ip, Sp, strips, scale, rdata, wcol, wmap, desc, wav, reduce;
     } bat;
     // the RTM forward pass whose final wavefield and strips are kept for swd_rtm_backward;
     // every other pass that reuses those buffers clears it
@@ -84,6 +84,7 @@ struct swd_ctx {
     // deconvolution scratch kept between swd_decon calls: inputs, taper, window slots,
     // outputs, staged workspaces
     DevBuf dcn[5];
+    DevBuf Ipart, Spart, Rpart;   // FP32 block sums of the imaging condition
     int batch_opt = 0;      // shots per batched launch; 0 = autotune on first use
     int batch_tuned = 0;    // the autotuner's choice (0 = not tuned yet)
     // chunked CUDA-graph execution of the time loops
@@ -94,6 +95,7 @@ struct swd_ctx {
         std::vector<cudaEvent_t> ev;   // probe events: (start, end) per kernel of the probed step
     } gfwd, gbwd, gseg, gadj, gbf, gbb;
     int use_graphs = 1;
+    int image_blocks = 1;   // SWD_OPT_IMAGE_BLOCKS
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -106,11 +108,11 @@ struct swd_ctx {
     {
         DevBuf *all[] = {&vp, &rho, &dpdt, &wcol, &wmap, &seis, &seis2, &rdata, &colbuf, &kzcoef, &tw,
                          &strips, &strip_scale, &I, &S, &R, &stack, &reduce, &stage_in, &stage_out, &ctrl, &wav,
-                         &dk, &gk, &s0, &ckpt, &rbuf, &alias, &dpst, &dpsc, &cig, &cigring};
+                         &dk, &gk, &s0, &ckpt, &rbuf, &alias, &dpst, &dpsc, &cig, &cigring, &Ipart, &Spart, &Rpart};
         for (DevBuf *b : all) bufs.push_back(b);
         for (auto &b : adj) bufs.push_back(&b);
         for (auto &b : dcn) bufs.push_back(&b);
-        DevBuf *ball[] = {&bat.dpdt, &bat.I, &bat.S, &bat.strips, &bat.scale, &bat.rdata, &bat.wcol, &bat.wmap,
+        DevBuf *ball[] = {&bat.dpdt, &bat.I, &bat.S, &bat.Ip, &bat.Sp, &bat.strips, &bat.scale, &bat.rdata, &bat.wcol, &bat.wmap,
                           &bat.desc, &bat.wav, &bat.reduce};
         for (DevBuf *b : ball) bufs.push_back(b);
         for (auto &w : bat.w)
@@ -1482,6 +1484,14 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         CKR(ensure_grid(ctx, ctx->R, sizeof(double)));
         CK(cudaMemsetAsync(ctx->R.p, 0, ctx->R.n, ctx->stream));
     }
+    const bool blocks = ctx->image_blocks && !fz;
+    if (blocks) {
+        DevBuf *pb[3] = {&ctx->Ipart, &ctx->Spart, &ctx->Rpart};
+        for (int i = 0; i < (ctx->have_R ? 3 : 2); i++) {
+            CKR(ensure_grid(ctx, *pb[i], sizeof(float)));
+            CK(cudaMemsetAsync(pb[i]->p, 0, pb[i]->n, ctx->stream));
+        }
+    }
     BwdArgs b;
     memset(&b, 0, sizeof b);
     b.g = make_geo(ctx);
@@ -1506,6 +1516,9 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
     b.I = D(ctx->I);
     b.S = D(ctx->S);
     b.R = ctx->have_R ? D(ctx->R) : nullptr;
+    b.Ip = blocks ? F(ctx->Ipart) : nullptr;
+    b.Sp = blocks ? F(ctx->Spart) : nullptr;
+    b.Rp = blocks && ctx->have_R ? F(ctx->Rpart) : nullptr;
     const dim3 grid = grid_blocks(ctx);
     CKR(ensure(ctx, ctx->ctrl, 64));
     if (fz) {
