@@ -427,33 +427,36 @@ def run_lsrtm(args, rank, world, dist):
     h_grad = torch.empty((w.nx, w.nz), dtype=torch.float32).pin_memory()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def gradient(dd):
+    def gradient(dd, pool=None):
         r = r0.clone().requires_grad_(True)
-        lsrtm.lsrtm_objective(r, ops, dd).backward()
+        lsrtm.lsrtm_objective(r, ops, dd, pool=pool).backward()
         return r.grad
 
-    def timed(K, W, e2e=False, profile=False):
+    engines = [E]
+
+    def timed(K, W, e2e=False, profile=False, pool=None):
         for _ in range(W):
-            gradient(data)
+            gradient(data, pool)
         if profile:
             E.profile(8)
             E.profile_read()
-        n0 = E.launch_count()
+        n0 = sum(e.launch_count() for e in engines)
         torch.cuda.synchronize()
         total = 0.0
         for _ in range(K):
             flush.zero_()
+            torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             if e2e:
                 dd = [hd.to("cuda", non_blocking=True) for hd in h_data]
-                h_grad.copy_(gradient(dd), non_blocking=True)
+                h_grad.copy_(gradient(dd, pool), non_blocking=True)
             else:
-                g = gradient(data)
+                g = gradient(data, pool)
             b.record()
             b.synchronize()
             total += a.elapsed_time(b)
-        launches = E.launch_count() - n0
+        launches = sum(e.launch_count() for e in engines) - n0
         prof = E.profile_read() if profile else None
         E.profile(0)
         return total, launches, prof
@@ -475,9 +478,22 @@ def run_lsrtm(args, rank, world, dist):
     ck_bytes = E.checkpoint_bytes(w.nt)
     full_bytes = w.nt * w.ntx * ((w.ntz + 31) // 32 * 32) * 4
     with ClockSampler(dev) as clk:
-        t_val, launches, prof = timed(args.steps, args.warmup, profile=True)
-        t_e2e, _, _ = timed(args.steps, 1, e2e=True)
-    t_val, t_e2e = max_over_ranks(dist, [t_val, t_e2e], "cuda")
+        t_seq, launches, prof = timed(args.steps, args.warmup, profile=True)
+        t_val, t_e2e = t_seq, None
+        pool = None
+        if args.streams > 1:
+            # engines configured like E; shots spread over them from one host thread each
+            for _ in range(args.streams - 1):
+                Ek = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt, device=dev)
+                Ek.setup_default(vmig, rho)
+                Ek.set_checkpointing(50, prec)
+                engines.append(Ek)
+            pool = lsrtm.EnginePool(engines)
+            t_val, launches, _ = timed(args.steps, args.warmup, pool=pool)
+        t_e2e, _, _ = timed(args.steps, 1, e2e=True, pool=pool)
+        if pool is not None:
+            pool.close()
+    t_val, t_e2e, t_seq = max_over_ranks(dist, [t_val, t_e2e, t_seq], "cuda")
     value = replica_throughput(nshots * args.steps, world, t_val)
     e2e = replica_throughput(nshots * args.steps, world, t_e2e)
     per_launch = {k: ms / n for k, (ms, n) in prof.items() if n}
@@ -497,7 +513,11 @@ def run_lsrtm(args, rank, world, dist):
         "vs_baseline": None, "dtype": f"f32 (FP64 gradient accumulation, {args.ckpt_prec} checkpoints)",
         "data": "synthetic (seeded random-field model, Born data of seeded reflectivity spikes)",
         "config": {"workload": LSRTM_WORKLOAD, "parallelism": f"replicas x{world}", "shots_per_step": nshots,
-                   "checkpoints": f"every 50 steps, {args.ckpt_prec}", "l2": "flushed (256 MiB write) before every timed step"},
+                   "checkpoints": f"every 50 steps, {args.ckpt_prec}", "l2": "flushed (256 MiB write) before every timed step",
+                   "engines": args.streams},
+        "sequential": {"value": replica_throughput(nshots * args.steps, world, t_seq), "unit": "shots/s",
+                       "ms_per_step": t_seq / args.steps,
+                       "what": "one engine, shots one after another (the kernel timings below are from this run)"},
         "gcell_updates_per_s": value * w.nt * 2 * N / 1e9,
         "executed_gcell_updates_per_s": value * w.nt * 4 * N / 1e9,
         "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(nshots * r_n * w.nt * 4),
@@ -833,6 +853,8 @@ def main():
     ap.add_argument("--config", choices=["c2", "c5", "shipped"], default="c2",
                     help="grid of --workload rtm (c2, c5) or decon (c2, c5, shipped: the reference's window geometry)")
     ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
+    ap.add_argument("--streams", type=int, default=3,
+                    help="--workload lsrtm: engines (streams and host threads) the survey's shots are spread over")
     ap.add_argument("--decon-iters", type=int, default=0,
                     help="--workload decon: FISTA iterations of the regularised option (L1 0.02, L2 0.06)")
     ap.add_argument("--ckpt-prec", choices=["f32", "f16", "bf16", "i16"], default="bf16",

@@ -18,8 +18,15 @@ Background checkpoints.  With the engine's checkpointing on (Engine.set_checkpoi
 default every 50 steps in BF16), the Born forward leaves the background state snapshots in
 a device buffer owned by the autograd graph (saved for backward), and the adjoint recomputes
 each 50-step segment from them instead of storing the wavefield of every step.
+
+Concurrent shots.  On grids where one shot's launches do not fill the GPU, an EnginePool of
+identically configured engines (each with its own stream and buffers) runs the shots of a
+survey from one host thread per engine; libswd calls release the GIL, so the engines' kernels
+overlap on the device.  born_survey is the survey-level autograd function over such a pool.
 """
 from __future__ import annotations
+
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
@@ -57,28 +64,31 @@ class BornOperator:
         dk[self.inner] = 2.0 * self.kappa[self.inner] * r
         return dk
 
-    def ckpt_buffer(self):
-        n = self.E.checkpoint_bytes(self.shot.nt)
+    def ckpt_buffer(self, engine: Engine = None):
+        n = (engine or self.E).checkpoint_bytes(self.shot.nt)
         return torch.empty(n, dtype=torch.uint8, device=self.device) if n else None
 
-    def forward(self, r: torch.Tensor, ckpt=None) -> torch.Tensor:
+    def forward(self, r: torch.Tensor, ckpt=None, engine: Engine = None) -> torch.Tensor:
+        """Born data of reflectivity r; `engine` (default: the operator's own) runs it."""
+        E = engine or self.E
         d = torch.empty((len(self.shot.r_ix), self.shot.nt), dtype=torch.float32, device=self.device)
         dk = _dev(self.dkappa(r))
         _sync(self.device)
-        self.E.born(self.shot, self.rick, dk, out=d, ckpt=ckpt)
+        E.born(self.shot, self.rick, dk, out=d, ckpt=ckpt)
         return d
 
-    def adjoint_kappa(self, resid: torch.Tensor, ckpt=None) -> torch.Tensor:
+    def adjoint_kappa(self, resid: torch.Tensor, ckpt=None, engine: Engine = None) -> torch.Tensor:
         """dJ/dkappa on the padded grid, float64."""
-        g = torch.empty((self.E.ntx, self.E.ntz), dtype=torch.float64, device=self.device)
+        E = engine or self.E
+        g = torch.empty((E.ntx, E.ntz), dtype=torch.float64, device=self.device)
         res = _dev(resid.float())
         _sync(self.device)
-        self.E.born_adjoint(self.shot, self.rick, res, out=g, ckpt=ckpt)
+        E.born_adjoint(self.shot, self.rick, res, out=g, ckpt=ckpt)
         return g
 
-    def adjoint(self, resid: torch.Tensor, ckpt=None) -> torch.Tensor:
+    def adjoint(self, resid: torch.Tensor, ckpt=None, engine: Engine = None) -> torch.Tensor:
         """Adjoint with respect to the interior reflectivity, float64."""
-        g = self.adjoint_kappa(resid, ckpt)
+        g = self.adjoint_kappa(resid, ckpt, engine)
         return 2.0 * self.kappa[self.inner].double() * g[self.inner]
 
 
@@ -136,10 +146,71 @@ def modelling(vp_pad: torch.Tensor, engine: Engine, shot: ShotSpec, rick, rho_pa
     return ForwardModelling.apply(vp_pad, engine, shot, rick, rho_pad)
 
 
-def lsrtm_objective(r: torch.Tensor, ops, data) -> torch.Tensor:
-    """J(r) = 1/2 sum_shots ||L_s r - d_s||^2, accumulated in float64."""
+class EnginePool:
+    """n engines configured alike (same grid, model, stencil, CPML, checkpointing) and one host
+    thread per engine.  map(fn, items) calls fn(engine, item) with item i on engine i % n, each
+    engine working through its items in order; results come back in item order."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        self._exec = ThreadPoolExecutor(max_workers=len(self.engines))
+
+    def __len__(self):
+        return len(self.engines)
+
+    def map(self, fn, items):
+        items = list(items)
+        n = len(self.engines)
+
+        def work(k):
+            return [(i, fn(self.engines[k], items[i])) for i in range(k, len(items), n)]
+
+        out = [None] * len(items)
+        for part in self._exec.map(work, range(min(n, len(items)))):
+            for i, v in part:
+                out[i] = v
+        return out
+
+    def close(self):
+        self._exec.shutdown()
+
+
+class BornSurvey(torch.autograd.Function):
+    """(L_1 r, ..., L_S r) for the shots of a survey, the shots spread over an EnginePool;
+    backward sums the shots' adjoints (each from the checkpoints its forward left) in float64."""
+
+    @staticmethod
+    def forward(ctx, r: torch.Tensor, ops, pool: EnginePool):
+        r32 = _dev(r.float())
+
+        def fwd(E, op):
+            ck = op.ckpt_buffer(E)
+            return op.forward(r32, ck, engine=E), ck
+
+        res = pool.map(fwd, ops)
+        ctx.ops, ctx.pool, ctx.ckpts, ctx.dtype = ops, pool, [c for _, c in res], r.dtype
+        return tuple(d for d, _ in res)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        items = [(op, g, ck) for op, g, ck in zip(ctx.ops, grads, ctx.ckpts) if g is not None]
+        parts = ctx.pool.map(lambda E, it: it[0].adjoint(it[1], it[2], engine=E), items)
+        g = parts[0].clone()
+        for q in parts[1:]:
+            g += q
+        return g.to(ctx.dtype), None, None
+
+
+def born_survey(r: torch.Tensor, ops, pool: EnginePool):
+    return BornSurvey.apply(r, ops, pool)
+
+
+def lsrtm_objective(r: torch.Tensor, ops, data, pool: EnginePool = None) -> torch.Tensor:
+    """J(r) = 1/2 sum_shots ||L_s r - d_s||^2, accumulated in float64; with a pool the shots
+    run concurrently on its engines."""
     J = torch.zeros((), dtype=torch.float64, device=r.device)
-    for op, d in zip(ops, data):
-        res = born(r, op) - d
+    preds = born_survey(r, ops, pool) if pool is not None else [born(r, op) for op in ops]
+    for p, d in zip(preds, data):
+        res = p - d
         J = J + 0.5 * (res.double() ** 2).sum()
     return J
