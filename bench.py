@@ -566,11 +566,13 @@ def run_batch(args, rank, world, dist):
     E.set_model(vmig, rho)
     cells = sum(s["nt"] * (2 * w.ntx * w.ntz + w.nx * w.nz) for s in shots_cfg)
 
+    engines = [E]
+
     def timed(fn, K, W):
         for _ in range(W):
             fn()
         torch.cuda.synchronize()
-        n0 = E.launch_count()
+        n0 = sum(e.launch_count() for e in engines)
         total = 0.0
         for _ in range(K):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -579,7 +581,7 @@ def run_batch(args, rank, world, dist):
             b.record(stream)
             b.synchronize()
             total += a.elapsed_time(b)
-        return total, E.launch_count() - n0
+        return total, sum(e.launch_count() for e in engines) - n0
 
     def plain():
         E.stack_reset()
@@ -599,15 +601,29 @@ def run_batch(args, rank, world, dist):
     E.set_option(swd.OPT_GRAPHS, 1)
     E.set_option(swd.OPT_BATCH, 0)
     with ClockSampler(dev) as clk:
-        t_bat, launches = timed(batched, args.steps, args.warmup)
-    st_bat = E.stack(edge_zero=False).astype(np.float64)
+        t_bat, launches_bat = timed(batched, args.steps, args.warmup)
+        st_bat = E.stack(edge_zero=False).astype(np.float64)
+        # engine pool: the survey's shots spread over args.streams engines (own streams, one
+        # host thread each), each migrating its share with swd_rtm_batch
+        from swd_b200 import survey
+        for _ in range(args.streams - 1):
+            Ek = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, ntmax, device=dev)
+            Ek.setup_default(vmig, rho)
+            engines.append(Ek)
+        pool = survey.EnginePool(engines)
+        st_pool = []
+        t_pool, launches = timed(lambda: st_pool.append(survey.rtm_survey(pool, shots, ricks, data, edge_zero=False)),
+                                 args.steps, args.warmup)
+        pool.close()
+    st_pool = st_pool[-1].astype(np.float64)
     # int16 strips: the image error of halving the strip memory
     E.set_strip_precision(swd.STRIP_I16)
     batched()
     st_bat16 = E.stack(edge_zero=False).astype(np.float64)
     E.set_strip_precision(swd.STRIP_F32)
-    t_bat, t_plain = max_over_ranks(dist, [t_bat, t_plain], "cuda")
+    t_bat, t_plain, t_pool = max_over_ranks(dist, [t_bat, t_plain, t_pool], "cuda")
     value = replica_throughput(len(shots) * args.steps, world, t_bat)
+    pool_v = replica_throughput(len(shots) * args.steps, world, t_pool)
     plain_v = replica_throughput(len(shots) * args.steps, world, t_plain)
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     return {
@@ -615,10 +631,15 @@ def run_batch(args, rank, world, dist):
         "warmup": args.warmup, "ms_per_step": t_bat / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP64 imaging)", "data": "synthetic (seeded random-field model)",
         "config": {"workload": BATCH_WORKLOAD, "parallelism": f"replicas x{world}", "shots_per_step": len(shots),
-                   "batch_size": E.get_option(swd.OPT_BATCH_TUNED), "l2": "inputs of one batch exceed L2"},
+                   "batch_size": E.get_option(swd.OPT_BATCH_TUNED),
+                   "what": "swd_rtm_batch on one engine (autotuned batch, CUDA graphs, FP32 strips)",
+                   "l2": "inputs of one batch exceed L2"},
         "gcell_updates_per_s": cells * args.steps / (t_bat / 1e3) / 1e9,
         "plain_engine": {"value": plain_v, "unit": "shots/s", "ms_per_step": t_plain / args.steps,
                          "what": "swd_rtm_shot per shot, host launches (no graphs), FP32 strips"},
+        "engine_pool": {"value": pool_v, "unit": "shots/s", "ms_per_step": t_pool / args.steps, "engines": args.streams,
+                        "what": "rtm_survey: the shots over an engine pool, each engine through swd_rtm_batch",
+                        "stack_rel_l2_vs_plain": rel(st_pool, st_plain)},
         "speedup_vs_plain": value / plain_v,
         "stack_rel_l2_vs_plain": rel(st_bat, st_plain),
         "stack_rel_l2_int16_strips_vs_plain": rel(st_bat16, st_plain),

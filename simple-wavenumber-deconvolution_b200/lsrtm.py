@@ -26,12 +26,11 @@ overlap on the device.  born_survey is the survey-level autograd function over s
 """
 from __future__ import annotations
 
-from concurrent.futures import ThreadPoolExecutor
-
 import numpy as np
 import torch
 
 from . import Engine, ShotSpec
+from .survey import EnginePool
 
 
 def _dev(t: torch.Tensor) -> torch.Tensor:
@@ -144,35 +143,6 @@ class ForwardModelling(torch.autograd.Function):
 
 def modelling(vp_pad: torch.Tensor, engine: Engine, shot: ShotSpec, rick, rho_pad: torch.Tensor) -> torch.Tensor:
     return ForwardModelling.apply(vp_pad, engine, shot, rick, rho_pad)
-
-
-class EnginePool:
-    """n engines configured alike (same grid, model, stencil, CPML, checkpointing) and one host
-    thread per engine.  map(fn, items) calls fn(engine, item) with item i on engine i % n, each
-    engine working through its items in order; results come back in item order."""
-
-    def __init__(self, engines):
-        self.engines = list(engines)
-        self._exec = ThreadPoolExecutor(max_workers=len(self.engines))
-
-    def __len__(self):
-        return len(self.engines)
-
-    def map(self, fn, items):
-        items = list(items)
-        n = len(self.engines)
-
-        def work(k):
-            return [(i, fn(self.engines[k], items[i])) for i in range(k, len(items), n)]
-
-        out = [None] * len(items)
-        for part in self._exec.map(work, range(min(n, len(items)))):
-            for i, v in part:
-                out[i] = v
-        return out
-
-    def close(self):
-        self._exec.shutdown()
 
 
 class BornSurvey(torch.autograd.Function):

@@ -104,3 +104,23 @@ def test_batch_compressed_strips(survey, swd, prec):
 def test_batch_rejects_unsupported_flags(survey, swd):
     with pytest.raises(swd.SwdError):
         survey.E.rtm_batch(survey.shots, survey.ricks, survey.data, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK)
+
+
+def test_survey_on_engine_pool(survey, reference, swd):
+    """rtm_survey over three engines (concurrent host threads and streams, each through
+    swd_rtm_batch) stacks to the sequential image up to the float32 rounding of the per-engine
+    stacks."""
+    from swd_b200 import survey as sv
+    engines = []
+    for _ in range(3):
+        E = swd.Engine(survey.nx, survey.nz, 10, 4, 5.0, 5.0, 5e-4, survey.nt_max)
+        E.setup_default(survey.vp, survey.rho)
+        engines.append(E)
+    pool = sv.EnginePool(engines)
+    try:
+        got = sv.rtm_survey(pool, survey.shots, survey.ricks, survey.data, edge_zero=False)
+        again = sv.rtm_survey(pool, survey.shots, survey.ricks, survey.data, batched=False, edge_zero=False)
+    finally:
+        pool.close()
+    assert rel_l2(got, reference) < 1e-6
+    assert rel_l2(again, reference) < 1e-6
