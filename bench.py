@@ -159,7 +159,7 @@ def algorithmic_bytes(kernel, w, cp, strip_len, r_n, strip_esz=4):
     if kernel == "fwd_p":      # vx, vz; p r/w; ck; phi r/w in the frame; strip save; traces
         return 20 * N + 8 * x_p + strip_esz * strip_len + 4 * r_n
     if kernel == "bwd_1":      # receiver p, v r/w, cbx, cbz (all cells) + psi in the frame;
-        #                        source v, p r/w, vp, rho, dp/dt (interior); strips
+        #                        source v, p r/w, ck, kap, dp/dt (interior); strips
         return 28 * N + 28 * Ni + 8 * x_v + strip_esz * strip_len
     if kernel == "bwd_2":      # receiver v, p r/w, ck (all cells) + phi in the frame; source p, v r/w,
         #                        cbx, cbz (interior); imaging (interior): dp/dt, the FP32 block sums of

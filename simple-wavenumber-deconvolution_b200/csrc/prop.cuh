@@ -746,16 +746,17 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
                 el(dvz, k) += tz.c[ic] * (vw.at(k + ic) - vw.at(k - ic - 1));
             }
         }
-        const float4 v = ldg4(a.vp + ip), r = ldg4(a.rho + ip);
+        // (-dt)*rho*vp*vp = -ck and rho*vp*vp = kap exactly (same products, same order), so
+        // the material coefficients replace vp and rho; ck is also what k_bwd_2 reads
+        const float4 ck = ldg4(a.m.ck + ip), kap = ldg4(a.m.kap + ip);
         float4 p = ld4(a.s.p + ip), dp = make_float4(0.f, 0.f, 0.f, 0.f);
         const int nzb = (g.ntz + 127) / 128;
         const bool band = block_has_strips(g.ntx, g.ntz, g.pmlc, LC);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             if (!in[k]) continue;
-            const float rv = elc(r, k) * elc(v, k) * elc(v, k);
-            el(p, k) = (-g.dt) * elc(r, k) * elc(v, k) * elc(v, k) * (elc(dvx, k) + elc(dvz, k)) + elc(p, k);
-            el(dp, k) = rv * (elc(dvx, k) + elc(dvz, k));
+            el(p, k) = (-elc(ck, k)) * (elc(dvx, k) + elc(dvz, k)) + elc(p, k);
+            el(dp, k) = elc(kap, k) * (elc(dvx, k) + elc(dvz, k));
             if (src_here && a.sz == z0 + k) el(p, k) -= a.wavsub[it + 1];
             // boundary strips overwrite (fdtd_2d_GPU_kernel_borders_backward :575-620)
             if (band) {
