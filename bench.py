@@ -165,6 +165,13 @@ def algorithmic_bytes(kernel, w, cp, strip_len, r_n, strip_esz=4):
         #                        cbx, cbz (interior); imaging (interior): dp/dt, the FP32 block sums of
         #                        I and S r/w every step, the FP64 I and S r/w on one step in 64; traces
         return 20 * N + 28 * Ni + 20 * Ni + Ni // 2 + 8 * x_p + 4 * r_n
+    if kernel == "bwd_v":      # velocities of both wavefields: receiver p, v r/w, cbx, cbz (all cells) + psi
+        #                        in the frame; source p, v r/w (interior; the same cbx, cbz)
+        return 28 * N + 20 * Ni + 8 * x_v
+    if kernel == "bwd_p":      # pressures of both wavefields + imaging: receiver v, p r/w, ck (all cells) +
+        #                        phi in the frame; source v, p r/w, kap (interior); strips; FP32 block sums
+        #                        of I and S r/w, the FP64 fold on one step in 64; traces
+        return 20 * N + 20 * Ni + 16 * Ni + Ni // 2 + 8 * x_p + strip_esz * strip_len + 4 * r_n
     if kernel == "fwd_step":   # one fused launch per forward step: p, vx, vz r/w, vp, rho, CPML, strips
         return 32 * N + 8 * (x_v + x_p) + strip_esz * strip_len + 4 * r_n
     if kernel == "bwd_step":   # one fused launch per backward step: receiver 24N, material 8N, source 24Ni, FP64 image 32Ni
@@ -301,11 +308,14 @@ def run_ours(args, rank, world, dist):
     slen = 2 * w.Lc * w.nx + 2 * w.Lc * (w.nz - 2 * w.Lc)
     # roofline of the dominant kernel (largest total time per step)
     per_launch = {k: ms / n for k, (ms, n) in prof.items() if n}
+    if E.get_option(swd.OPT_BWD_BY_KIND):   # profile slots 2, 3 hold k_bwd_v, k_bwd_p
+        per_launch = {{"bwd_1": "bwd_v", "bwd_2": "bwd_p"}.get(k, k): v for k, v in per_launch.items()}
     # Kernel durations: the whole-pass events (around the graph replays, nothing inside the
     # captured steps) give the time of one forward / backward time step; a probe copy of one
     # chunk brackets the kernels of its middle step, which inflates each by the event-node
     # overhead, so it is only used to split a step's time between its two launches.
-    pairs = {"fwd_pass_step": ("fwd_v", "fwd_p"), "bwd_pass_step": ("bwd_1", "bwd_2")}
+    pairs = {"fwd_pass_step": ("fwd_v", "fwd_p"), "bwd_pass_step": ("bwd_1", "bwd_2") if "bwd_1" in per_launch
+             else ("bwd_v", "bwd_p")}
     live = {}
     for ps, (k1, k2) in pairs.items():
         if ps in per_launch and k1 in per_launch and k2 in per_launch:
@@ -315,7 +325,8 @@ def run_ours(args, rank, world, dist):
         ps = k.replace("_step", "_pass_step")
         if ps in per_launch and k in per_launch:
             live[k] = per_launch[ps]
-    launches_per_shot = {"fwd_v": nt, "fwd_p": nt, "bwd_1": nt - 1, "bwd_2": nt - 1, "fwd_step": nt, "bwd_step": nt - 1}
+    launches_per_shot = {"fwd_v": nt, "fwd_p": nt, "bwd_1": nt - 1, "bwd_2": nt - 1, "bwd_v": nt - 1, "bwd_p": nt - 1,
+                         "fwd_step": nt, "bwd_step": nt - 1}
     dom = max(live, key=lambda k: live[k] * launches_per_shot[k])
     peak, src = peaks()
     ab = algorithmic_bytes(dom, w, cp, slen, r_n, 4 if strips == "f32" else 2)

@@ -179,6 +179,12 @@ int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *
 #define SWD_OPT_BATCH 2
 #define SWD_OPT_BATCH_TUNED 3
 #define SWD_OPT_IMAGE_BLOCKS 4
+/* SWD_OPT_BWD_BY_KIND 1 (default): each RTM backward step runs the two wavefields' velocity
+ *                 phases in one launch and their pressure phases plus the imaging in the other
+ *                 (dp/dt stays in registers; 20 bytes less per interior cell and step; the same
+ *                 images bit for bit); 0: the reference's pairing (source p with receiver v,
+ *                 source v with receiver p).  Angle gathers always use the reference's pairing. */
+#define SWD_OPT_BWD_BY_KIND 5
 int swd_set_option(swd_ctx *ctx, int option, int value);
 int swd_get_option(swd_ctx *ctx, int option, int *value);
 

@@ -23,12 +23,14 @@ static void launch_fwd_batch(const FwdArgs &a, dim3 grid, cudaStream_t s, cudaEv
 }
 
 template <int LC>
-static void launch_bwd_batch(const BwdArgs &a, dim3 grid, cudaStream_t s, cudaEvent_t *ev)
+static void launch_bwd_batch(const BwdArgs &a, dim3 grid, cudaStream_t s, cudaEvent_t *ev, int by_kind)
 {
     if (ev) cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal);
-    k_bwd_1<LC, true><<<grid, dim3(32, 8), 0, s>>>(a);
+    if (by_kind) k_bwd_v<LC, true><<<grid, dim3(32, 8), 0, s>>>(a);
+    else k_bwd_1<LC, true><<<grid, dim3(32, 8), 0, s>>>(a);
     if (ev) { cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal); }
-    k_bwd_2<LC, true><<<grid, dim3(32, 8), 0, s>>>(a);
+    if (by_kind) k_bwd_p<LC, true><<<grid, dim3(32, 8), 0, s>>>(a);
+    else k_bwd_2<LC, true><<<grid, dim3(32, 8), 0, s>>>(a);
     if (ev) cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal);
 }
 
@@ -194,13 +196,16 @@ static int rtm_batch_run(swd_ctx *ctx, const swd_shot *shots, const float *const
     bb.bt = bt;
     const int nbk = probe_steps > 0 ? std::min(probe_steps, ntmax - 1) : ntmax - 1;
     {
+        const int by_kind = ctx->bwd_by_kind;
         auto launch = [&](int k, cudaEvent_t *ev) {
             BwdArgs q = bb;
             q.itoff = -k;
-            LC_DISPATCH(ctx->Lc, launch_bwd_batch, q, grid, ctx->stream, ev);
+            LC_DISPATCH(ctx->Lc, launch_bwd_batch, q, grid, ctx->stream, ev, by_kind);
         };
         const int kid[2] = {2, 3};
-        CKR(run_steps(ctx, ctx->gbb, &bb, sizeof bb, ntmax - 2, -1, nbk, 2, kid, launch));
+        std::vector<char> key((const char *)&bb, (const char *)&bb + sizeof bb);
+        key.insert(key.end(), (const char *)&by_kind, (const char *)&by_kind + sizeof by_kind);
+        CKR(run_steps(ctx, ctx->gbb, key.data(), key.size(), ntmax - 2, -1, nbk, 2, kid, launch));
     }
     if (probe_steps > 0) return SWD_OK;
     // per-shot normalisation, -vp^2 Laplacian and FP64 stack
@@ -304,6 +309,10 @@ int swd_set_option(swd_ctx *ctx, int option, int value)
             if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_IMAGE_BLOCKS takes 0 or 1");
             ctx->image_blocks = value;
             return SWD_OK;
+        case SWD_OPT_BWD_BY_KIND:
+            if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_BWD_BY_KIND takes 0 or 1");
+            ctx->bwd_by_kind = value;
+            return SWD_OK;
         default:
             return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
@@ -317,6 +326,7 @@ int swd_get_option(swd_ctx *ctx, int option, int *value)
         case SWD_OPT_BATCH: *value = ctx->batch_opt; return SWD_OK;
         case SWD_OPT_BATCH_TUNED: *value = ctx->batch_tuned; return SWD_OK;
         case SWD_OPT_IMAGE_BLOCKS: *value = ctx->image_blocks; return SWD_OK;
+        case SWD_OPT_BWD_BY_KIND: *value = ctx->bwd_by_kind; return SWD_OK;
         default: return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
 }

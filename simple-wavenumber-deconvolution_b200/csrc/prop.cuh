@@ -712,25 +712,19 @@ __device__ __forceinline__ float strip_restore(const Strips &st, int it, int si,
     return dec16(((const unsigned short *)st.buf)[(size_t)it * st.slen + si], mx, st.prec);
 }
 
-template <int LC, bool BATCH = false>
-__global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
+// Phases of one RTM backward step on the four cells (x, z0..z0+3), shared by both launch
+// pairings.  in[k]: interior cell; any: some cell of the four is interior.
+//
+// Source wavefield pressure of step it, interior only (fdtd_2d_GPU_kernel_p_backward
+// :434-485, -dt), source subtraction, boundary-strip overwrite (:575-620); returns
+// dp/dt = kap * div v in dp (0 outside the interior).
+template <int LC>
+__device__ __forceinline__ void src_p_phase(const BwdArgs &a, int it, int x, int z0, size_t ip, const bool in[4],
+                                            bool any, float4 &dp)
 {
-    BwdArgs a = a0;
-    int it = *a.itp + a.itoff;
-    if constexpr (BATCH) {
-        if (!bwd_view(a, it)) return;
-    }
-    int x, z0;
-    cell4(x, z0);
     const Geo &g = a.g;
-    if (x >= g.ntx || z0 >= g.ntz) return;
     const int ldz = g.ldz;
-    const size_t ip = (size_t)x * ldz + z0;
-    // source wavefield pressure, interior only (fdtd_2d_GPU_kernel_p_backward :434-485)
-    bool in[4];
-    bool any = false;
-#pragma unroll
-    for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
+    dp = make_float4(0.f, 0.f, 0.f, 0.f);
     const bool src_here = x == a.sx && a.sz >= z0 && a.sz < z0 + 4;
     if (any) {
         float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -747,9 +741,9 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
             }
         }
         // (-dt)*rho*vp*vp = -ck and rho*vp*vp = kap exactly (same products, same order), so
-        // the material coefficients replace vp and rho; ck is also what k_bwd_2 reads
+        // the material coefficients replace vp and rho; ck is also what the receiver p reads
         const float4 ck = ldg4(a.m.ck + ip), kap = ldg4(a.m.kap + ip);
-        float4 p = ld4(a.s.p + ip), dp = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 p = ld4(a.s.p + ip);
         const int nzb = (g.ntz + 127) / 128;
         const bool band = block_has_strips(g.ntx, g.ntz, g.pmlc, LC);
 #pragma unroll
@@ -758,7 +752,6 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
             el(p, k) = (-elc(ck, k)) * (elc(dvx, k) + elc(dvz, k)) + elc(p, k);
             el(dp, k) = elc(kap, k) * (elc(dvx, k) + elc(dvz, k));
             if (src_here && a.sz == z0 + k) el(p, k) -= a.wavsub[it + 1];
-            // boundary strips overwrite (fdtd_2d_GPU_kernel_borders_backward :575-620)
             if (band) {
                 const int si = strip_index(x, z0 + k, g.ntx, g.ntz, g.pmlc, LC);
                 if (si >= 0) el(p, k) = strip_restore(a.strips, it, si, x, z0 + k, nzb);
@@ -770,10 +763,94 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
                 if (a.sz == z0 + k && !in[k]) el(p, k) -= a.wavsub[it + 1];
         }
         st4(a.s.p + ip, p);
-        st4(a.dpdt + ip, dp);
     } else if (src_here) {
         a.s.p[ip + (a.sz - z0)] -= a.wavsub[it + 1];
     }
+}
+
+// Source wavefield velocities, interior only (:488-573, -dt)
+template <int LC>
+__device__ __forceinline__ void src_v_phase(const BwdArgs &a, int x, int z0, size_t ip, const bool in[4])
+{
+    const Geo &g = a.g;
+    const int ldz = g.ldz;
+    const Taps<LC> tx(g, g.odx), tz(g, g.odz);
+    float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int ic = 0; ic < LC; ic++) {
+        const float4 p1 = ld4(a.s.p + ip + (size_t)(ic + 1) * ldz), p2 = ld4(a.s.p + ip - (size_t)ic * ldz);
+#pragma unroll
+        for (int k = 0; k < 4; k++) el(d, k) += tx.c[ic] * (elc(p1, k) - elc(p2, k));
+    }
+    // (-dt)*rcp(...) = -cbx exactly
+    const float4 cbx = ldg4(a.m.cbx + ip);
+    float4 vx = ld4(a.s.vx + ip);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (in[k]) el(vx, k) = (-elc(cbx, k)) * elc(d, k) + elc(vx, k);
+    st4(a.s.vx + ip, vx);
+    ZWin<LC> pw;
+    pw.load(a.s.p + (size_t)x * ldz, z0);
+    d = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int ic = 0; ic < LC; ic++) el(d, k) += tz.c[ic] * (pw.at(k + ic + 1) - pw.at(k - ic));
+    const float4 cbz = ldg4(a.m.cbz + ip);
+    float4 vz = ld4(a.s.vz + ip);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (in[k]) el(vz, k) = (-elc(cbz, k)) * elc(d, k) + elc(vz, k);
+    st4(a.s.vz + ip, vz);
+}
+
+// Receiver wavefield pressure (CPML, -dx/-dz) and hard injection of the data (:717-782)
+template <int LC>
+__device__ __forceinline__ float4 rcv_p_phase(const BwdArgs &a, int it, int x, int z0, size_t ip)
+{
+    const Geo &g = a.g;
+    float4 pr;
+    bool upd[4];
+    p_update4<LC>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0, pr, upd);
+    bool wr = upd[0] || upd[1] || upd[2] || upd[3];
+    const int wc = __ldg(a.wells.wcol + x);
+    if (wc >= 0) {
+        const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * g.ldz + z0));
+        const int t[4] = {tr.x, tr.y, tr.z, tr.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (t[k] >= 0 && z0 + k < g.ntz) { el(pr, k) = a.rdata[(size_t)t[k] * a.nt + it]; wr = true; }
+    }
+    if (wr) st4(a.r.p + ip, pr);
+    return pr;
+}
+
+__device__ __forceinline__ bool interior4(const Geo &g, int x, int z0, bool in[4])
+{
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
+    return any;
+}
+
+template <int LC, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
+{
+    BwdArgs a = a0;
+    int it = *a.itp + a.itoff;
+    if constexpr (BATCH) {
+        if (!bwd_view(a, it)) return;
+    }
+    int x, z0;
+    cell4(x, z0);
+    const Geo &g = a.g;
+    if (x >= g.ntx || z0 >= g.ntz) return;
+    const size_t ip = (size_t)x * g.ldz + z0;
+    bool in[4];
+    const bool any = interior4(g, x, z0, in);
+    float4 dp;
+    src_p_phase<LC>(a, it, x, z0, ip, in, any, dp);
+    if (any) st4(a.dpdt + ip, dp);
     // receiver wavefield velocities (wide guards, negative spacing)
     v_update4<LC, true>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0);
 }
@@ -871,63 +948,70 @@ __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_2(cons
     cell4(x, z0);
     const Geo &g = a.g;
     if (x >= g.ntx || z0 >= g.ntz) return;
-    const int ldz = g.ldz;
-    const size_t ip = (size_t)x * ldz + z0;
+    const size_t ip = (size_t)x * g.ldz + z0;
     bool in[4];
-    bool any = false;
-#pragma unroll
-    for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
+    const bool any = interior4(g, x, z0, in);
     if (any) {   // the imaging operands are read last: start their DRAM reads now
         image_prefetch(a, ip, it);
         prefetch_l2(a.dpdt + ip);
     }
-    // source wavefield velocities, interior only (:488-573)
-    if (any) {
-        const Taps<LC> tx(g, g.odx), tz(g, g.odz);
-        float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int ic = 0; ic < LC; ic++) {
-            const float4 p1 = ld4(a.s.p + ip + (size_t)(ic + 1) * ldz), p2 = ld4(a.s.p + ip - (size_t)ic * ldz);
-#pragma unroll
-            for (int k = 0; k < 4; k++) el(d, k) += tx.c[ic] * (elc(p1, k) - elc(p2, k));
-        }
-        // (-dt)*rcp(...) = -cbx exactly
-        const float4 cbx = ldg4(a.m.cbx + ip);
-        float4 vx = ld4(a.s.vx + ip);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            if (in[k]) el(vx, k) = (-elc(cbx, k)) * elc(d, k) + elc(vx, k);
-        st4(a.s.vx + ip, vx);
-        ZWin<LC> pw;
-        pw.load(a.s.p + (size_t)x * ldz, z0);
-        d = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-#pragma unroll
-            for (int ic = 0; ic < LC; ic++) el(d, k) += tz.c[ic] * (pw.at(k + ic + 1) - pw.at(k - ic));
-        const float4 cbz = ldg4(a.m.cbz + ip);
-        float4 vz = ld4(a.s.vz + ip);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            if (in[k]) el(vz, k) = (-elc(cbz, k)) * elc(d, k) + elc(vz, k);
-        st4(a.s.vz + ip, vz);
-    }
-    // receiver pressure + hard injection (:717-782)
-    float4 pr;
-    bool upd[4];
-    p_update4<LC>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0, pr, upd);
-    bool wr = upd[0] || upd[1] || upd[2] || upd[3];
-    const int wc = __ldg(a.wells.wcol + x);
-    if (wc >= 0) {
-        const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * ldz + z0));
-        const int t[4] = {tr.x, tr.y, tr.z, tr.w};
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            if (t[k] >= 0 && z0 + k < g.ntz) { el(pr, k) = a.rdata[(size_t)t[k] * a.nt + it]; wr = true; }
-    }
-    if (wr) st4(a.r.p + ip, pr);
+    if (any) src_v_phase<LC>(a, x, z0, ip, in);
+    const float4 pr = rcv_p_phase<LC>(a, it, x, z0, ip);
     // imaging condition (sum_image_GPU_kernel_image :785-817)
     if (any) image4(a, ip, in, ld4(a.dpdt + ip), pr, it);
+}
+
+// ------------------------------------------------------------------------------------
+// RTM backward step with the phases paired by kind (default; same per-cell arithmetic and the
+// same images, bit for bit, as k_bwd_1 + k_bwd_2):
+//   BV(it): receiver vx, vz of step it; source vx, vz of step it + 1 (none on the first
+//           backward step, it = nt - 2, which starts from the final forward velocities)
+//   BP(it): source p of step it (strips, source subtraction); receiver p of step it and the
+//           injection; imaging with dp/dt from registers
+// Each launch needs one kind of material coefficient for both wavefields (cbx, cbz; ck, kap)
+// and dp/dt never goes to memory: 20 bytes less per interior cell and step.  The source
+// velocities lag by one step (v of step 0 is never formed), so the angle gathers, which read
+// them after every step, use k_bwd_1 + k_bwd_2.
+// ------------------------------------------------------------------------------------
+template <int LC, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_bwd_v(const BwdArgs a0)
+{
+    BwdArgs a = a0;
+    int it = *a.itp + a.itoff;
+    if constexpr (BATCH) {
+        if (!bwd_view(a, it)) return;
+    }
+    int x, z0;
+    cell4(x, z0);
+    const Geo &g = a.g;
+    if (x >= g.ntx || z0 >= g.ntz) return;
+    const size_t ip = (size_t)x * g.ldz + z0;
+    bool in[4];
+    const bool any = interior4(g, x, z0, in);
+    if (any && it < a.nt - 2) src_v_phase<LC>(a, x, z0, ip, in);
+    v_update4<LC, true>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0);
+}
+
+template <int LC, bool BATCH = false>
+__global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_p(const BwdArgs a0)
+{
+    BwdArgs a = a0;
+    int it = *a.itp + a.itoff;
+    if constexpr (BATCH) {
+        if (!bwd_view(a, it)) return;
+    }
+    int x, z0;
+    cell4(x, z0);
+    const Geo &g = a.g;
+    if (x >= g.ntx || z0 >= g.ntz) return;
+    const size_t ip = (size_t)x * g.ldz + z0;
+    bool in[4];
+    const bool any = interior4(g, x, z0, in);
+    if (any) image_prefetch(a, ip, it);
+    float4 dp;
+    src_p_phase<LC>(a, it, x, z0, ip, in, any, dp);
+    const float4 pr = rcv_p_phase<LC>(a, it, x, z0, ip);
+    if (any) image4(a, ip, in, dp, pr, it);
 }
 
 // ------------------------------------------------------------------------------------

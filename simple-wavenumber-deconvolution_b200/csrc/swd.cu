@@ -96,6 +96,7 @@ struct swd_ctx {
     } gfwd, gbwd, gseg, gadj, gbf, gbb;
     int use_graphs = 1;
     int image_blocks = 1;   // SWD_OPT_IMAGE_BLOCKS
+    int bwd_by_kind = 1;    // SWD_OPT_BWD_BY_KIND
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -653,6 +654,12 @@ static void launch_bwd_1(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_1<
 
 template <int LC>
 static void launch_bwd_2(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_2<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+
+template <int LC>
+static void launch_bwd_v(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_v<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+
+template <int LC>
+static void launch_bwd_p(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_p<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
 
 template <int LC>
 static void launch_bwd_rcv_v(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_rcv_v<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
@@ -1576,13 +1583,24 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
             cg.ring = F(ctx->cigring); cg.cig = F(ctx->cig);
         }
         const dim3 cgrid((ctx->ntz + 31) / 32, (ctx->ntx + 7) / 8);
+        // phases paired by kind (k_bwd_v + k_bwd_p) unless the angle gathers need the source
+        // velocities of every step (k_bwd_1 + k_bwd_2, the reference's pairing)
+        const int by_kind = ctx->bwd_by_kind && !want_cig;
         auto launch = [&](int k, cudaEvent_t *ev) {
             BwdArgs q = b;
             q.itoff = -k;
             if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
-            LC_DISPATCH(ctx->Lc, launch_bwd_1, q, grid, ctx->stream);
+            if (by_kind) {
+                LC_DISPATCH(ctx->Lc, launch_bwd_v, q, grid, ctx->stream);
+            } else {
+                LC_DISPATCH(ctx->Lc, launch_bwd_1, q, grid, ctx->stream);
+            }
             if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
-            LC_DISPATCH(ctx->Lc, launch_bwd_2, q, grid, ctx->stream);
+            if (by_kind) {
+                LC_DISPATCH(ctx->Lc, launch_bwd_p, q, grid, ctx->stream);
+            } else {
+                LC_DISPATCH(ctx->Lc, launch_bwd_2, q, grid, ctx->stream);
+            }
             if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
             if (want_cig) {
                 CigArgs cq = cg;
@@ -1592,9 +1610,10 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         };
         const int kid[2] = {2, 3};
         b.itoff = 0;
-        // the CIG switch is part of the captured graph's identity
+        // the CIG switch and the pairing are part of the captured graph's identity
         std::vector<char> key((const char *)&b, (const char *)&b + sizeof b);
         key.insert(key.end(), (const char *)&cg, (const char *)&cg + sizeof cg);
+        key.insert(key.end(), (const char *)&by_kind, (const char *)&by_kind + sizeof by_kind);
         CKR(run_steps(ctx, ctx->gbwd, key.data(), key.size(), nt - 2, -1, nt - 1, 2, kid, launch));
         if (want_cig) ctx->launches += nt - 1;
         ctx->have_cig = want_cig;

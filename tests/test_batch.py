@@ -124,3 +124,15 @@ def test_survey_on_engine_pool(survey, reference, swd):
         pool.close()
     assert rel_l2(got, reference) < 1e-6
     assert rel_l2(again, reference) < 1e-6
+
+
+def test_batch_pairing_by_kind_same_bits(survey, swd):
+    """Batched launches with the backward phases paired by kind (default) and with the
+    reference's pairing stack to the same image bit for bit."""
+    a = survey.batched(3)
+    survey.E.set_option(swd.OPT_BWD_BY_KIND, 0)
+    try:
+        b = survey.batched(3)
+    finally:
+        survey.E.set_option(swd.OPT_BWD_BY_KIND, 1)
+    assert np.array_equal(a, b)

@@ -458,3 +458,26 @@ def test_image_blocks_against_fp64_every_step(case, swd, orc):
     for a, b in zip(blk, ref):
         assert np.abs(b).max() > 0
         assert rel_l2(a, b) < 1e-6
+
+
+def test_backward_pairing_by_kind_same_bits(case, swd, orc):
+    """The backward step with its phases paired by kind (velocities of both wavefields in one
+    launch, pressures and imaging in the other; the default) against the reference's pairing:
+    the raw images I, S and R are identical bit for bit (same per-cell arithmetic)."""
+    data = orc.forward(case.M, case.G, case.rick)["seis"]
+    flags = swd.RTM_PREPROCESS | swd.RTM_NO_STACK | swd.RTM_ILLUM_RCV
+    path = case.path
+    case.E.set_kernel_path(0)
+    try:
+        assert case.E.get_option(swd.OPT_BWD_BY_KIND) == 1
+        case.E.rtm_shot(case.shot, case.rick, data, flags=flags, want=())
+        a = case.E.rtm_raw(rcv=True)
+        case.E.set_option(swd.OPT_BWD_BY_KIND, 0)
+        case.E.rtm_shot(case.shot, case.rick, data, flags=flags, want=())
+        b = case.E.rtm_raw(rcv=True)
+    finally:
+        case.E.set_option(swd.OPT_BWD_BY_KIND, 1)
+        case.E.set_kernel_path(path)
+    for x, y in zip(a, b):
+        assert np.abs(y).max() > 0
+        assert np.array_equal(x, y)
