@@ -128,11 +128,15 @@ __device__ __forceinline__ bool block_has_strips(int ntx, int ntz, int pmlc, int
 }
 
 // 16-bit codes of a value v relative to its block's max |v| (mx >= |v|): prec 1 IEEE half of
-// v/mx * 32768, prec 2 bfloat16 of v/mx, prec 3 int16 fixed point round(v/mx * 32767).
-// Normalising first keeps |v|/mx <= 1 even for denormal mx.
-__device__ __forceinline__ unsigned short enc16(float v, float mx, int prec)
+// v/mx * 32768, prec 2 bfloat16 of v/mx, prec 3 int16 fixed point round(v/mx * 32767).  The
+// quotient is v times the correctly rounded reciprocal of mx (enc16_inv, once per scale; no
+// division per value), so |q| exceeds 1 by at most a rounding, which the codes absorb; for a
+// subnormal mx, whose reciprocal would overflow, inv is 0 and the quotient is divided out.
+__device__ __forceinline__ float enc16_inv(float mx) { return mx >= 1.17549435e-38f ? __frcp_rn(mx) : 0.f; }
+
+__device__ __forceinline__ unsigned short enc16(float v, float mx, float inv, int prec)
 {
-    const float q = mx > 0.f ? v / mx : 0.f;
+    const float q = inv != 0.f ? v * inv : (mx > 0.f ? v / mx : 0.f);
     if (prec == 1) return __half_as_ushort(__float2half_rn(q * 32768.f));
     if (prec == 2) return __bfloat16_as_ushort(__float2bfloat16_rn(q));
     return (unsigned short)(short)__float2int_rn(q * 32767.f);
@@ -140,9 +144,9 @@ __device__ __forceinline__ unsigned short enc16(float v, float mx, int prec)
 
 __device__ __forceinline__ float dec16(unsigned short u, float mx, int prec)
 {
-    if (prec == 1) return (__half2float(__ushort_as_half(u)) / 32768.f) * mx;
+    if (prec == 1) return (__half2float(__ushort_as_half(u)) * (1.f / 32768.f)) * mx;
     if (prec == 2) return __bfloat162float(__ushort_as_bfloat16(u)) * mx;
-    return ((float)(short)u / 32767.f) * mx;
+    return ((float)(short)u * (1.f / 32767.f)) * mx;
 }
 
 // Index of cell (x, z) in the per-step strip vector, or -1.
@@ -412,11 +416,11 @@ __device__ __forceinline__ void ckpt_save(const Ckpt &ck, const Wave &w, int sna
     if (!in) return;
 #pragma unroll
     for (int i = 0; i < 7; i++) {
-        const float mx = smax[i];
+        const float mx = smax[i], inv = enc16_inv(mx);
         const size_t o = ((size_t)snap * 7 + i) * ck.fstride + ip;
         ushort4 h;
-        h.x = enc16(v[i].x, mx, ck.prec); h.y = enc16(v[i].y, mx, ck.prec);
-        h.z = enc16(v[i].z, mx, ck.prec); h.w = enc16(v[i].w, mx, ck.prec);
+        h.x = enc16(v[i].x, mx, inv, ck.prec); h.y = enc16(v[i].y, mx, inv, ck.prec);
+        h.z = enc16(v[i].z, mx, inv, ck.prec); h.w = enc16(v[i].w, mx, inv, ck.prec);
         *reinterpret_cast<ushort4 *>((unsigned short *)ck.buf + o) = h;
     }
 }
@@ -512,9 +516,10 @@ __device__ __forceinline__ void store_dpdt(const DpStore &ds, const Mat &m, cons
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (threadIdx.x == 0) __stcs(ds.scale + (size_t)it * ds.nwarps + warp_slot(), mx);
     if (off >= 0) {
+        const float inv = enc16_inv(mx);
         ushort4 h;
-        h.x = enc16(dp.x, mx, ds.prec); h.y = enc16(dp.y, mx, ds.prec);
-        h.z = enc16(dp.z, mx, ds.prec); h.w = enc16(dp.w, mx, ds.prec);
+        h.x = enc16(dp.x, mx, inv, ds.prec); h.y = enc16(dp.y, mx, inv, ds.prec);
+        h.z = enc16(dp.z, mx, inv, ds.prec); h.w = enc16(dp.w, mx, inv, ds.prec);
         __stcs(reinterpret_cast<ushort4 *>((unsigned short *)ds.buf + base + off), h);
     }
 }
@@ -637,13 +642,13 @@ __global__ void __launch_bounds__(256, (NW == 1 && MODE != FP_BORN && !BATCH && 
             for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
             if (threadIdx.x == 0 && v > 0.f) atomicMax((int *)&smax, __float_as_int(v));
             __syncthreads();
-            const float mx = smax;
+            const float mx = smax, inv = enc16_inv(mx);
             const int slot = blockIdx.y * gridDim.x + blockIdx.x;
             if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)it * a.strips.nscale + slot] = mx;
 #pragma unroll
             for (int k = 0; k < 4; k++)
                 if (si[k] >= 0)
-                    ((unsigned short *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = enc16(elc(pn[0], k), mx, a.strips.prec);
+                    ((unsigned short *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = enc16(elc(pn[0], k), mx, inv, a.strips.prec);
         }
     }
 }

@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(256) k_fwd_step(FStepArgs a)
         __syncthreads();
         if (lane == 0 && vmax > 0.f) atomicMax((int *)&smax, __float_as_int(vmax));
         __syncthreads();
-        const float mx = smax;
+        const float mx = smax, inv = enc16_inv(mx);
         const int slot = blockIdx.y * gridDim.x + blockIdx.x;
         if (threadIdx.x == 0) a.strips.scale[(size_t)it * a.strips.nscale + slot] = mx;
         for (int k = warp; k < TX * (TZ / 32); k += T::NWARP) {
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(256) k_fwd_step(FStepArgs a)
             if (x >= g.ntx || z >= g.ntz) continue;
             const int si = strip_index(x, z, g.ntx, g.ntz, g.pmlc, LC);
             if (si < 0) continue;
-            ((unsigned short *)a.strips.buf)[(size_t)it * a.strips.slen + si] = enc16(sPn[0][cc * TZ + rr], mx, a.strips.prec);
+            ((unsigned short *)a.strips.buf)[(size_t)it * a.strips.slen + si] = enc16(sPn[0][cc * TZ + rr], mx, inv, a.strips.prec);
         }
     }
 }
