@@ -406,8 +406,8 @@ def adjoint_bytes(kernel, w, cp, r_n):
     x_p = nzc(cp["a_x"]) * w.ntz + nzc(cp["a_z"]) * w.ntx
     if kernel == "adj_v":   # Qx, Qz in; v^x, v^z r/w; rho; Rx, Rz out; psi^ r/w in the frame
         return 36 * N + 8 * x_v
-    if kernel == "adj_p":   # Rx, Rz in; p^ r/w; S0; FP64 grad r/w; vp, rho; Qx, Qz out; phi^ in the frame; traces
-        return 52 * N + 8 * x_p + 4 * r_n
+    if kernel == "adj_p":   # Rx, Rz in; p^ r/w; S0; FP64 grad r/w; ck; Qx, Qz out; phi^ in the frame; traces
+        return 48 * N + 8 * x_p + 4 * r_n
     raise KeyError(kernel)
 
 

@@ -31,6 +31,7 @@ struct AdjArgs {
     Geo g;
     Cpml c;
     const float *vp, *rho;
+    const float *ck;     // dt*rho*vp*vp (the forward pressure coefficient)
     Wave l;              // adjoint state: p^, v^x, v^z, psi^x (ppx), psi^z (ppz), phi^x (pvx), phi^z (pvz)
     float *qx, *qz, *rx, *rz;
     const int *itp;      // step index k = *itp + itoff (counts down)
@@ -188,7 +189,8 @@ __global__ void __launch_bounds__(256) k_adj_p(AdjArgs a)
     // ---- P^T pointwise for the next (earlier) step, on Gp = cols/rows [LC, n-LC]
     float4 Qx = make_float4(0.f, 0.f, 0.f, 0.f), Qz = make_float4(0.f, 0.f, 0.f, 0.f);
     if (colp) {
-        const float4 v = ldg4(a.vp + ip), r = ldg4(a.rho + ip);
+        // dt*rho*vp*vp*p^ = ck*p^ exactly (the same products in the same order)
+        const float4 kc = ldg4(a.ck + ip);
         const float ax = __ldg(a.c.ax + x);
         const float bx = ax != 0.f ? __ldg(a.c.bx + x) : 0.f;
         float4 fx = ax != 0.f ? ld4(a.l.pvx + ip) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(256) k_adj_p(AdjArgs a)
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             if (!in_range(z0 + k, LC, ntz - LC)) continue;
-            const float q = g.dt * elc(r, k) * elc(v, k) * elc(v, k) * elc(p, k);
+            const float q = elc(kc, k) * elc(p, k);
             if (ax != 0.f) {
                 el(Qx, k) = q + ax * (q + elc(fx, k));
                 el(fx, k) = bx * (q + elc(fx, k));

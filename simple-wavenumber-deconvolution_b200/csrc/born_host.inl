@@ -224,6 +224,7 @@ int swd_born_adjoint(swd_ctx *ctx, const swd_shot *shot, const float *rick, cons
     b.c = make_cpml(ctx);
     b.vp = F(ctx->vp);
     b.rho = F(ctx->rho);
+    b.ck = F(ctx->mat[2]);
     b.l = make_wave(ctx, 1);
     b.qx = F(ctx->adj[0]); b.qz = F(ctx->adj[1]); b.rx = F(ctx->adj[2]); b.rz = F(ctx->adj[3]);
     b.itp = I32(ctx->ctrl);
