@@ -185,6 +185,11 @@ int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *
  *                 images bit for bit); 0: the reference's pairing (source p with receiver v,
  *                 source v with receiver p).  Angle gathers always use the reference's pairing. */
 #define SWD_OPT_BWD_BY_KIND 5
+/* SWD_OPT_TMA 1: the velocity launches of the single-wavefield forward pass and of the backward
+ *                 pass paired by kind read the pressure through tiles that the Tensor Memory
+ *                 Accelerator copies into shared memory (persistent CTAs, two stages; the same
+ *                 images bit for bit); 0 (default): per-thread loads, which measure faster */
+#define SWD_OPT_TMA 6
 int swd_set_option(swd_ctx *ctx, int option, int value);
 int swd_get_option(swd_ctx *ctx, int option, int *value);
 

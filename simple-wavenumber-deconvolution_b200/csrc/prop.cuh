@@ -213,11 +213,30 @@ struct ZWin {
     __device__ __forceinline__ float at(int k) const { return v[4 * NB + k]; }   // z0 + k
 };
 
+// Where a velocity update reads the pressure: global memory (PGlobal), or a shared-memory tile
+// staged by TMA (PTile: column x - c0, row z - r0, pr rows per column).  Both give the same
+// values on every cell the update guards let through.
+struct PGlobal {
+    const float *p;
+    int ldz;
+    __device__ __forceinline__ float4 col(int x, int z0) const { return ld4(p + (size_t)x * ldz + z0); }
+    template <int LC>
+    __device__ __forceinline__ void zwin(ZWin<LC> &w, int x, int z0) const { w.load(p + (size_t)x * ldz, z0); }
+};
+
+struct PTile {
+    const float *s;
+    int c0, r0, pr;
+    __device__ __forceinline__ float4 col(int x, int z0) const { return ld4(s + (x - c0) * pr + (z0 - r0)); }
+    template <int LC>
+    __device__ __forceinline__ void zwin(ZWin<LC> &w, int x, int z0) const { w.load(s + (x - c0) * pr - r0, z0); }
+};
+
 // velocity half step (reference kernels _vx/_vz, acoustic_HLVSPRTMLc.cu:24-118; receiver
-// variants with the wider guards and -dx/-dz, :623-715)
-template <int LC, bool WIDE>
-__device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
-                                          int x, int z0)
+// variants with the wider guards and -dx/-dz, :623-715), the pressure read through pl
+template <int LC, bool WIDE, class PL>
+__device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
+                                            int x, int z0, const PL &pl)
 {
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
@@ -237,7 +256,7 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat
             float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int ic = 0; ic < LC; ic++) {
-                const float4 a = ld4(w.p + ip + (size_t)(ic + 1) * ldz), b = ld4(w.p + ip - (size_t)ic * ldz);
+                const float4 a = pl.col(x + ic + 1, z0), b = pl.col(x - ic, z0);
 #pragma unroll
                 for (int k = 0; k < 4; k++) el(d, k) += tx.c[ic] * (elc(a, k) - elc(b, k));
             }
@@ -274,7 +293,7 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat
         }
         if (any) {
             ZWin<LC> pw;
-            pw.load(w.p + (size_t)x * ldz, z0);
+            pl.zwin(pw, x, z0);
             float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int k = 0; k < 4; k++)
@@ -301,6 +320,13 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat
             st4(w.vz + ip, v);
         }
     }
+}
+
+template <int LC, bool WIDE>
+__device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
+                                          int x, int z0)
+{
+    v_update4_l<LC, WIDE>(g, c, m, w, odx, odz, x, z0, PGlobal{w.p, g.ldz});
 }
 
 // pressure step with CPML (reference kernel _p, :121-173) on the four cells; returns the
@@ -773,17 +799,16 @@ __device__ __forceinline__ void src_p_phase(const BwdArgs &a, int it, int x, int
     }
 }
 
-// Source wavefield velocities, interior only (:488-573, -dt)
-template <int LC>
-__device__ __forceinline__ void src_v_phase(const BwdArgs &a, int x, int z0, size_t ip, const bool in[4])
+// Source wavefield velocities, interior only (:488-573, -dt), the source pressure read through pl
+template <int LC, class PL>
+__device__ __forceinline__ void src_v_phase_l(const BwdArgs &a, int x, int z0, size_t ip, const bool in[4], const PL &pl)
 {
     const Geo &g = a.g;
-    const int ldz = g.ldz;
     const Taps<LC> tx(g, g.odx), tz(g, g.odz);
     float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int ic = 0; ic < LC; ic++) {
-        const float4 p1 = ld4(a.s.p + ip + (size_t)(ic + 1) * ldz), p2 = ld4(a.s.p + ip - (size_t)ic * ldz);
+        const float4 p1 = pl.col(x + ic + 1, z0), p2 = pl.col(x - ic, z0);
 #pragma unroll
         for (int k = 0; k < 4; k++) el(d, k) += tx.c[ic] * (elc(p1, k) - elc(p2, k));
     }
@@ -795,7 +820,7 @@ __device__ __forceinline__ void src_v_phase(const BwdArgs &a, int x, int z0, siz
         if (in[k]) el(vx, k) = (-elc(cbx, k)) * elc(d, k) + elc(vx, k);
     st4(a.s.vx + ip, vx);
     ZWin<LC> pw;
-    pw.load(a.s.p + (size_t)x * ldz, z0);
+    pl.zwin(pw, x, z0);
     d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < 4; k++)
@@ -807,6 +832,12 @@ __device__ __forceinline__ void src_v_phase(const BwdArgs &a, int x, int z0, siz
     for (int k = 0; k < 4; k++)
         if (in[k]) el(vz, k) = (-elc(cbz, k)) * elc(d, k) + elc(vz, k);
     st4(a.s.vz + ip, vz);
+}
+
+template <int LC>
+__device__ __forceinline__ void src_v_phase(const BwdArgs &a, int x, int z0, size_t ip, const bool in[4])
+{
+    src_v_phase_l<LC>(a, x, z0, ip, in, PGlobal{a.s.p, a.g.ldz});
 }
 
 // Receiver wavefield pressure (CPML, -dx/-dz) and hard injection of the data (:717-782)

@@ -17,6 +17,7 @@
 #include "../../include/swd.h"
 #include "prop.cuh"
 #include "prop_fused.cuh"
+#include "prop_tma.cuh"
 #include "born.cuh"
 #include "fft.cuh"
 #include "decon.cuh"
@@ -97,6 +98,7 @@ struct swd_ctx {
     int use_graphs = 1;
     int image_blocks = 1;   // SWD_OPT_IMAGE_BLOCKS
     int bwd_by_kind = 1;    // SWD_OPT_BWD_BY_KIND
+    int use_tma = 0;        // SWD_OPT_TMA
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -658,6 +660,97 @@ static void launch_bwd_2(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_2<
 template <int LC>
 static void launch_bwd_v(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_v<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
 
+// ---- TMA-staged velocity kernels (prop_tma.cuh) -----------------------------------------
+typedef CUresult (*TmapEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// the driver's tensor-map encoder, looked up once through the runtime (no libcuda link)
+static TmapEncodeFn tmap_encoder()
+{
+    static const TmapEncodeFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return (TmapEncodeFn)p;
+    }();
+    return fn;
+}
+
+template <int LC>
+static void tma_box(int *rows, int *cols)
+{
+    *rows = VTile<LC>::PR;
+    *cols = VTile<LC>::PC;
+}
+
+// tensor map of a padded grid array (ntx columns of ldz floats) with a box of rows x cols
+// (tma_box of the context's stencil order)
+static bool make_pmap(const swd_ctx *ctx, CUtensorMap *m, const float *base, int rows, int cols)
+{
+    TmapEncodeFn enc = tmap_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)ctx->ldz, (cuuint64_t)ctx->ntx};
+    const cuuint64_t strides[1] = {(cuuint64_t)ctx->ldz * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)rows, (cuuint32_t)cols};
+    const cuuint32_t estride[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, estride,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// launch shape of a TMA velocity kernel with nbox boxes per stage: persistent CTAs, as many as
+// are resident (nblk = 0 when the kernel cannot be used)
+struct TmaShape {
+    int nblk = 0;
+    size_t smem = 0;
+};
+
+template <int LC>
+static void tma_prepare(int dev, int nbox, TmaShape *t)
+{
+    t->nblk = 0;
+    t->smem = vtile_smem<LC>(nbox);
+    const void *fn = nbox == 1 ? (const void *)k_fwd_v_tma<LC> : (const void *)k_bwd_v_tma<LC>;
+    int nsm = 0, occ = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, t->smem) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        return;
+    }
+    t->nblk = nsm * occ;
+}
+
+template <int LC>
+static void launch_fwd_v_tma(const FwdArgs &a, const CUtensorMap &m, int *err, const TmaShape &t, cudaStream_t s)
+{
+    k_fwd_v_tma<LC><<<t.nblk, dim3(32, 8), t.smem, s>>>(a, m, err);
+}
+
+template <int LC>
+static void launch_bwd_v_tma(const BwdArgs &a, const CUtensorMap &mr, const CUtensorMap &ms, int *err, const TmaShape &t,
+                             cudaStream_t s)
+{
+    k_bwd_v_tma<LC><<<t.nblk, dim3(32, 8), t.smem, s>>>(a, mr, ms, err);
+}
+
+// error word of the TMA kernels (set when a wait on a copy gave up), after the step counter
+static int *tma_err(swd_ctx *ctx) { return I32(ctx->ctrl) + 8; }
+
+static int tma_check(swd_ctx *ctx)
+{
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, tma_err(ctx), sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h) return fail(ctx, SWD_ERR_CUDA, "a TMA-staged velocity kernel gave up waiting for its pressure tile");
+    return SWD_OK;
+}
+
 template <int LC>
 static void launch_bwd_p(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_p<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
 
@@ -904,20 +997,38 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     a.wav0 = F(ctx->wav);
     a.wav1 = J.twin ? F(ctx->wav) + nt : F(ctx->wav);
     const int nw = J.twin ? 2 : 1;
+    // one wavefield without checkpoints: the velocity kernel with TMA-staged pressure
+    int use_tma = ctx->use_tma && nw == 1 && !a.ck.every;
+    CUtensorMap pmap;
+    TmaShape tsh;
+    if (use_tma) {
+        int rows = 0, cols = 0;
+        LC_DISPATCH(ctx->Lc, tma_box, &rows, &cols);
+        LC_DISPATCH(ctx->Lc, tma_prepare, ctx->dev, 1, &tsh);
+        use_tma = tsh.nblk > 0 && make_pmap(ctx, &pmap, a.w[0].p, rows, cols);
+        if (use_tma) CK(cudaMemsetAsync(tma_err(ctx), 0, sizeof(int), ctx->stream));
+    }
     auto launch = [&](int k, cudaEvent_t *ev) {
         FwdArgs b = a;
         b.itoff = k;
-        const dim3 blk(32, 8);
         if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
-        LC_DISPATCH(ctx->Lc, launch_fwd_v, b, nw, grid, ctx->stream);
+        if (use_tma) {
+            LC_DISPATCH(ctx->Lc, launch_fwd_v_tma, b, pmap, tma_err(ctx), tsh, ctx->stream);
+        } else {
+            LC_DISPATCH(ctx->Lc, launch_fwd_v, b, nw, grid, ctx->stream);
+        }
         if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
         LC_DISPATCH(ctx->Lc, launch_fwd_p, b, nw, grid, ctx->stream);
         if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
-        (void)blk;
     };
     const int kid[2] = {0, 1};
     a.itoff = 0;
-    return run_steps(ctx, ctx->gfwd, &a, sizeof a, 0, +1, nt, 2, kid, launch);
+    // the TMA choice is part of the captured graph's identity
+    std::vector<char> key((const char *)&a, (const char *)&a + sizeof a);
+    key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
+    CKR(run_steps(ctx, ctx->gfwd, key.data(), key.size(), 0, +1, nt, 2, kid, launch));
+    if (use_tma) CKR(tma_check(ctx));
+    return SWD_OK;
 }
 
 // Fused forward: step it reads copy it%2 and writes copy (it+1)%2 of every double-buffered
@@ -1586,11 +1697,24 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         // phases paired by kind (k_bwd_v + k_bwd_p) unless the angle gathers need the source
         // velocities of every step (k_bwd_1 + k_bwd_2, the reference's pairing)
         const int by_kind = ctx->bwd_by_kind && !want_cig;
+        // velocities of both wavefields with TMA-staged pressures
+        int use_tma = by_kind && ctx->use_tma;
+        CUtensorMap pmap_r, pmap_s;
+        TmaShape tsh;
+        if (use_tma) {
+            int rows = 0, cols = 0;
+            LC_DISPATCH(ctx->Lc, tma_box, &rows, &cols);
+            LC_DISPATCH(ctx->Lc, tma_prepare, ctx->dev, 2, &tsh);
+            use_tma = tsh.nblk > 0 && make_pmap(ctx, &pmap_r, b.r.p, rows, cols) && make_pmap(ctx, &pmap_s, b.s.p, rows, cols);
+            if (use_tma) CK(cudaMemsetAsync(tma_err(ctx), 0, sizeof(int), ctx->stream));
+        }
         auto launch = [&](int k, cudaEvent_t *ev) {
             BwdArgs q = b;
             q.itoff = -k;
             if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
-            if (by_kind) {
+            if (by_kind && use_tma) {
+                LC_DISPATCH(ctx->Lc, launch_bwd_v_tma, q, pmap_r, pmap_s, tma_err(ctx), tsh, ctx->stream);
+            } else if (by_kind) {
                 LC_DISPATCH(ctx->Lc, launch_bwd_v, q, grid, ctx->stream);
             } else {
                 LC_DISPATCH(ctx->Lc, launch_bwd_1, q, grid, ctx->stream);
@@ -1614,7 +1738,9 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         std::vector<char> key((const char *)&b, (const char *)&b + sizeof b);
         key.insert(key.end(), (const char *)&cg, (const char *)&cg + sizeof cg);
         key.insert(key.end(), (const char *)&by_kind, (const char *)&by_kind + sizeof by_kind);
+        key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
         CKR(run_steps(ctx, ctx->gbwd, key.data(), key.size(), nt - 2, -1, nt - 1, 2, kid, launch));
+        if (use_tma) CKR(tma_check(ctx));
         if (want_cig) ctx->launches += nt - 1;
         ctx->have_cig = want_cig;
     }
