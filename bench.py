@@ -214,6 +214,8 @@ def run_ours(args, rank, world, dist):
     E, shot, rick, data, cp = setup(swd, w, dev)
     if args.tma:
         E.set_option(swd.OPT_TMA, 1)
+    if args.pdl:
+        E.set_option(swd.OPT_PDL, 1)
     if args.path is not None:
         E.set_kernel_path(args.path)
     strips = w.extra.get("strips", "f32")
@@ -892,6 +894,7 @@ def main():
                     help="grid of --workload rtm (c2, c5) or decon (c2, c5, shipped: the reference's window geometry)")
     ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
     ap.add_argument("--tma", action="store_true", help="velocity kernels with TMA-staged pressure tiles (SWD_OPT_TMA)")
+    ap.add_argument("--pdl", action="store_true", help="step kernels as programmatic dependent launches (SWD_OPT_PDL)")
     ap.add_argument("--streams", type=int, default=3,
                     help="--workload lsrtm: engines (streams and host threads) the survey's shots are spread over")
     ap.add_argument("--decon-iters", type=int, default=0,

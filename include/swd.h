@@ -190,6 +190,11 @@ int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *
  *                 Accelerator copies into shared memory (persistent CTAs, two stages; the same
  *                 images bit for bit); 0 (default): per-thread loads, which measure faster */
 #define SWD_OPT_TMA 6
+/* SWD_OPT_PDL 1: the RTM step kernels are programmatic dependent launches (the next launch's
+ *                 blocks are placed while this one's last blocks run; each waits for its
+ *                 predecessor before touching memory; the same images bit for bit); 0 (default):
+ *                 plain stream order, which measures the same with CUDA graphs */
+#define SWD_OPT_PDL 7
 int swd_set_option(swd_ctx *ctx, int option, int value);
 int swd_get_option(swd_ctx *ctx, int option, int *value);
 

@@ -562,6 +562,18 @@ __device__ __forceinline__ float4 load_dpdt(const DpStore &ds, const Geo &g, int
     return make_float4(dec16(h.x, mx, ds.prec), dec16(h.y, mx, ds.prec), dec16(h.z, mx, ds.prec), dec16(h.w, mx, ds.prec));
 }
 
+// Programmatic dependent launch.  The RTM step kernels are launched (SWD_OPT_PDL) so that the
+// next launch's CTAs may be scheduled while this launch's last CTAs still run.  Each step kernel
+// first waits until its predecessor grid has completed and its memory is visible, then lets its
+// own dependents be scheduled: they are placed only once every CTA of this grid has started, and
+// they wait in turn, so no CTA waits on one that cannot run.  Without the launch attribute both
+// instructions return at once.
+__device__ __forceinline__ void pdl_begin()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // block (32, 8): lane -> four rows, warp -> one column; a block covers 128 rows x 8 columns
 __device__ __forceinline__ void cell4(int &x, int &z0)
 {
@@ -572,6 +584,7 @@ __device__ __forceinline__ void cell4(int &x, int &z0)
 template <int LC, int NW, bool CKPT, bool BATCH = false>
 __global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
 {
+    pdl_begin();
     FwdArgs a = a0;
     if constexpr (BATCH) {
         if (!fwd_view(a, *a.itp + a.itoff)) return;
@@ -592,6 +605,7 @@ template <int LC, int NW, int MODE, bool BATCH = false>
 __global__ void __launch_bounds__(256, (NW == 1 && MODE != FP_BORN && !BATCH && LC <= 4) ? 5 : 1)
     k_fwd_p(const FwdArgs a0)
 {
+    pdl_begin();
     constexpr bool BORN = MODE == FP_BORN;
     FwdArgs a = a0;
     const int it = *a.itp + a.itoff;
@@ -872,6 +886,7 @@ __device__ __forceinline__ bool interior4(const Geo &g, int x, int z0, bool in[4
 template <int LC, bool BATCH = false>
 __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
 {
+    pdl_begin();
     BwdArgs a = a0;
     int it = *a.itp + a.itoff;
     if constexpr (BATCH) {
@@ -975,6 +990,7 @@ __device__ __forceinline__ void image_prefetch(const BwdArgs &a, size_t ip, int 
 template <int LC, bool BATCH = false>
 __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_2(const BwdArgs a0)
 {
+    pdl_begin();
     BwdArgs a = a0;
     int it = *a.itp + a.itoff;
     if constexpr (BATCH) {
@@ -1012,6 +1028,7 @@ __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_2(cons
 template <int LC, bool BATCH = false>
 __global__ void __launch_bounds__(256) k_bwd_v(const BwdArgs a0)
 {
+    pdl_begin();
     BwdArgs a = a0;
     int it = *a.itp + a.itoff;
     if constexpr (BATCH) {
@@ -1031,6 +1048,7 @@ __global__ void __launch_bounds__(256) k_bwd_v(const BwdArgs a0)
 template <int LC, bool BATCH = false>
 __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_p(const BwdArgs a0)
 {
+    pdl_begin();
     BwdArgs a = a0;
     int it = *a.itp + a.itoff;
     if constexpr (BATCH) {
@@ -1060,6 +1078,7 @@ __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_p(cons
 template <int LC>
 __global__ void __launch_bounds__(256) k_bwd_rcv_v(const BwdArgs a)
 {
+    pdl_begin();
     int x, z0;
     cell4(x, z0);
     if (x >= a.g.ntx || z0 >= a.g.ntz) return;
@@ -1069,6 +1088,7 @@ __global__ void __launch_bounds__(256) k_bwd_rcv_v(const BwdArgs a)
 template <int LC>
 __global__ void __launch_bounds__(256, 5) k_bwd_rcv_p(const BwdArgs a)
 {
+    pdl_begin();
     const int it = *a.itp + a.itoff;
     int x, z0;
     cell4(x, z0);

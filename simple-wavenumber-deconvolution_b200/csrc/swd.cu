@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/swd.h"
@@ -99,6 +100,7 @@ struct swd_ctx {
     int image_blocks = 1;   // SWD_OPT_IMAGE_BLOCKS
     int bwd_by_kind = 1;    // SWD_OPT_BWD_BY_KIND
     int use_tma = 0;        // SWD_OPT_TMA
+    int use_pdl = 0;        // SWD_OPT_PDL
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -624,41 +626,63 @@ __global__ void k_pml_z(float *v, int ntx, int ntz, int pml)
 // ------------------------------------------------------------------------------------
 // the checkpointing and Born variants are separate instantiations, so the plain modelling
 // and RTM kernels keep their register budget
+// Launch of an RTM step kernel (block 32 x 8, no dynamic shared memory); with pdl, as a
+// programmatic dependent launch (the step kernels open with pdl_begin)
+template <typename... P, typename... A>
+static void launch_step(void (*k)(P...), dim3 grid, cudaStream_t s, bool pdl, A &&...args)
+{
+    if (!pdl) {
+        k<<<grid, dim3(32, 8), 0, s>>>(std::forward<A>(args)...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(32, 8);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 template <int LC>
-static void launch_fwd_v(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s)
+static void launch_fwd_v(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bool pdl = false)
 {
     const bool ck = a.ck.every > 0;
     if (nw == 2) {
-        if (ck) k_fwd_v<LC, 2, true><<<grid, dim3(32, 8), 0, s>>>(a);
-        else k_fwd_v<LC, 2, false><<<grid, dim3(32, 8), 0, s>>>(a);
+        if (ck) launch_step(k_fwd_v<LC, 2, true>, grid, s, pdl, a);
+        else launch_step(k_fwd_v<LC, 2, false>, grid, s, pdl, a);
     } else {
-        if (ck) k_fwd_v<LC, 1, true><<<grid, dim3(32, 8), 0, s>>>(a);
-        else k_fwd_v<LC, 1, false><<<grid, dim3(32, 8), 0, s>>>(a);
+        if (ck) launch_step(k_fwd_v<LC, 1, true>, grid, s, pdl, a);
+        else launch_step(k_fwd_v<LC, 1, false>, grid, s, pdl, a);
     }
 }
 
 template <int LC>
-static void launch_fwd_p(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s)
+static void launch_fwd_p(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bool pdl = false)
 {
     const bool born = a.s0_out || a.dkappa;
     if (nw == 2) {
-        if (born) k_fwd_p<LC, 2, FP_BORN><<<grid, dim3(32, 8), 0, s>>>(a);
-        else k_fwd_p<LC, 2, FP_PLAIN><<<grid, dim3(32, 8), 0, s>>>(a);
+        if (born) launch_step(k_fwd_p<LC, 2, FP_BORN>, grid, s, pdl, a);
+        else launch_step(k_fwd_p<LC, 2, FP_PLAIN>, grid, s, pdl, a);
     } else {
-        if (a.ds.buf) k_fwd_p<LC, 1, FP_STORE><<<grid, dim3(32, 8), 0, s>>>(a);
-        else if (born) k_fwd_p<LC, 1, FP_BORN><<<grid, dim3(32, 8), 0, s>>>(a);
-        else k_fwd_p<LC, 1, FP_PLAIN><<<grid, dim3(32, 8), 0, s>>>(a);
+        if (a.ds.buf) launch_step(k_fwd_p<LC, 1, FP_STORE>, grid, s, pdl, a);
+        else if (born) launch_step(k_fwd_p<LC, 1, FP_BORN>, grid, s, pdl, a);
+        else launch_step(k_fwd_p<LC, 1, FP_PLAIN>, grid, s, pdl, a);
     }
 }
 
 template <int LC>
-static void launch_bwd_1(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_1<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+static void launch_bwd_1(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_1<LC>, grid, s, pdl, a); }
 
 template <int LC>
-static void launch_bwd_2(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_2<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+static void launch_bwd_2(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_2<LC>, grid, s, pdl, a); }
 
 template <int LC>
-static void launch_bwd_v(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_v<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+static void launch_bwd_v(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_v<LC>, grid, s, pdl, a); }
 
 // ---- TMA-staged velocity kernels (prop_tma.cuh) -----------------------------------------
 typedef CUresult (*TmapEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -752,13 +776,13 @@ static int tma_check(swd_ctx *ctx)
 }
 
 template <int LC>
-static void launch_bwd_p(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_p<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+static void launch_bwd_p(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_p<LC>, grid, s, pdl, a); }
 
 template <int LC>
-static void launch_bwd_rcv_v(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_rcv_v<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+static void launch_bwd_rcv_v(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_rcv_v<LC>, grid, s, pdl, a); }
 
 template <int LC>
-static void launch_bwd_rcv_p(const BwdArgs &a, dim3 grid, cudaStream_t s) { k_bwd_rcv_p<LC><<<grid, dim3(32, 8), 0, s>>>(a); }
+static void launch_bwd_rcv_p(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_rcv_p<LC>, grid, s, pdl, a); }
 
 template <int LC>
 static void launch_fwd_fused(const FStepArgs &a, int nw, cudaStream_t s)
@@ -1015,10 +1039,10 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
         if (use_tma) {
             LC_DISPATCH(ctx->Lc, launch_fwd_v_tma, b, pmap, tma_err(ctx), tsh, ctx->stream);
         } else {
-            LC_DISPATCH(ctx->Lc, launch_fwd_v, b, nw, grid, ctx->stream);
+            LC_DISPATCH(ctx->Lc, launch_fwd_v, b, nw, grid, ctx->stream, ctx->use_pdl);
         }
         if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
-        LC_DISPATCH(ctx->Lc, launch_fwd_p, b, nw, grid, ctx->stream);
+        LC_DISPATCH(ctx->Lc, launch_fwd_p, b, nw, grid, ctx->stream, ctx->use_pdl);
         if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
     };
     const int kid[2] = {0, 1};
@@ -1026,6 +1050,7 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     // the TMA choice is part of the captured graph's identity
     std::vector<char> key((const char *)&a, (const char *)&a + sizeof a);
     key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
+    key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
     CKR(run_steps(ctx, ctx->gfwd, key.data(), key.size(), 0, +1, nt, 2, kid, launch));
     if (use_tma) CKR(tma_check(ctx));
     return SWD_OK;
@@ -1675,14 +1700,16 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
             BwdArgs q = b;
             q.itoff = -k;
             if (ev) cudaEventRecordWithFlags(ev[0], ctx->stream, cudaEventRecordExternal);
-            LC_DISPATCH(ctx->Lc, launch_bwd_rcv_v, q, grid, ctx->stream);
+            LC_DISPATCH(ctx->Lc, launch_bwd_rcv_v, q, grid, ctx->stream, ctx->use_pdl);
             if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
-            LC_DISPATCH(ctx->Lc, launch_bwd_rcv_p, q, grid, ctx->stream);
+            LC_DISPATCH(ctx->Lc, launch_bwd_rcv_p, q, grid, ctx->stream, ctx->use_pdl);
             if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
         };
         const int kid[2] = {2, 3};
         b.itoff = 0;
-        CKR(run_steps(ctx, ctx->gbwd, &b, sizeof b, nt - 2, -1, nt - 1, 2, kid, launch));
+        std::vector<char> key((const char *)&b, (const char *)&b + sizeof b);
+        key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
+        CKR(run_steps(ctx, ctx->gbwd, key.data(), key.size(), nt - 2, -1, nt - 1, 2, kid, launch));
     } else {
         b.itp = I32(ctx->ctrl);
         b.wavsub = F(ctx->wav);
@@ -1715,15 +1742,15 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
             if (by_kind && use_tma) {
                 LC_DISPATCH(ctx->Lc, launch_bwd_v_tma, q, pmap_r, pmap_s, tma_err(ctx), tsh, ctx->stream);
             } else if (by_kind) {
-                LC_DISPATCH(ctx->Lc, launch_bwd_v, q, grid, ctx->stream);
+                LC_DISPATCH(ctx->Lc, launch_bwd_v, q, grid, ctx->stream, ctx->use_pdl);
             } else {
-                LC_DISPATCH(ctx->Lc, launch_bwd_1, q, grid, ctx->stream);
+                LC_DISPATCH(ctx->Lc, launch_bwd_1, q, grid, ctx->stream, ctx->use_pdl);
             }
             if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
             if (by_kind) {
-                LC_DISPATCH(ctx->Lc, launch_bwd_p, q, grid, ctx->stream);
+                LC_DISPATCH(ctx->Lc, launch_bwd_p, q, grid, ctx->stream, ctx->use_pdl);
             } else {
-                LC_DISPATCH(ctx->Lc, launch_bwd_2, q, grid, ctx->stream);
+                LC_DISPATCH(ctx->Lc, launch_bwd_2, q, grid, ctx->stream, ctx->use_pdl);
             }
             if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
             if (want_cig) {
@@ -1739,6 +1766,7 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         key.insert(key.end(), (const char *)&cg, (const char *)&cg + sizeof cg);
         key.insert(key.end(), (const char *)&by_kind, (const char *)&by_kind + sizeof by_kind);
         key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
+        key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
         CKR(run_steps(ctx, ctx->gbwd, key.data(), key.size(), nt - 2, -1, nt - 1, 2, kid, launch));
         if (use_tma) CKR(tma_check(ctx));
         if (want_cig) ctx->launches += nt - 1;

@@ -505,3 +505,36 @@ def test_tma_velocity_kernels_same_bits(swd, orc, shape):
     assert np.array_equal(seis_t, seis_p)
     for a, b in zip(img_t, img_p):
         assert np.array_equal(a, b)
+
+
+def test_pdl_launches_same_bits(case, swd, orc):
+    """RTM step kernels as programmatic dependent launches (SWD_OPT_PDL = 1) against plain
+    stream order (the default), with CUDA graphs and with host launches, reconstructing and
+    stored-source: the seismograms and raw images are identical bit for bit."""
+    data = orc.forward(case.M, case.G, case.rick)["seis"]
+    flags = swd.RTM_PREPROCESS | swd.RTM_NO_STACK
+    path = case.path
+    case.E.set_kernel_path(0)
+    out = {}
+    try:
+        for pdl in (1, 0):
+            case.E.set_option(swd.OPT_PDL, pdl)
+            for graphs in (1, 0):
+                case.E.set_option(swd.OPT_GRAPHS, graphs)
+                seis = case.E.forward(case.shot, case.rick)
+                case.E.rtm_shot(case.shot, case.rick, data, flags=flags, want=())
+                rec = case.E.rtm_raw()
+                case.E.set_source_storage(1, swd.STRIP_I16)
+                case.E.rtm_shot(case.shot, case.rick, data, flags=flags, want=())
+                st = case.E.rtm_raw()
+                case.E.set_source_storage(0)
+                out[(pdl, graphs)] = (seis, rec[0], rec[1], st[0], st[1])
+    finally:
+        case.E.set_option(swd.OPT_PDL, 0)
+        case.E.set_option(swd.OPT_GRAPHS, 1)
+        case.E.set_kernel_path(path)
+    ref = out[(0, 0)]
+    assert np.abs(ref[0]).max() > 0
+    for key, got in out.items():
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b), key
