@@ -1135,12 +1135,10 @@ struct CigArgs {
     float *cig;          // [ntx*ldz][thetan]
 };
 
-__global__ void __launch_bounds__(256) k_cig(const CigArgs a)
+// one interior cell (x, z) of the gathers after backward step it
+__device__ __forceinline__ void cig_cell(const CigArgs &a, int it, int x, int z)
 {
-    const int it = *a.itp + a.itoff;
     const Geo &g = a.g;
-    const int z = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
-    if (x >= g.ntx || z >= g.ntz || !interior(x, z, g)) return;
     const size_t fs = (size_t)g.ntx * g.ldz, ip = (size_t)x * g.ldz + z;
     const float ps = a.s.p[ip], pr = a.r.p[ip];
     const float fx = __fmul_rn(-ps, a.s.vx[ip]), fz = __fmul_rn(-ps, a.s.vz[ip]);
@@ -1165,6 +1163,42 @@ __global__ void __launch_bounds__(256) k_cig(const CigArgs a)
         const int itheta = (int)ceilf((float)__dsub_rn((double)__fadd_rn(ftheta, (float)ii), 0.5));
         const float betaf = (float)(1.0 * ii * ii / (2.0 * 9.0));
         if (itheta >= 2 && itheta < a.thetan) c[itheta] = __fadd_rn(c[itheta], __fmul_rn(pp, expf(-betaf)));
+    }
+}
+
+// the gathers as a launch of their own, one cell per thread
+__global__ void __launch_bounds__(256) k_cig(const CigArgs a)
+{
+    const int it = *a.itp + a.itoff;
+    const Geo &g = a.g;
+    const int z = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
+    if (x >= g.ntx || z >= g.ntz || !interior(x, z, g)) return;
+    cig_cell(a, it, x, z);
+}
+
+// k_bwd_2 with the gathers fused into its imaging: after the thread's own cells are updated
+// (source v here, source p and receiver v by k_bwd_1, receiver p here), each interior cell's
+// Poynting vectors are formed from the values the thread just wrote or that the previous
+// launch left, so the gathers equal those of the separate launch.
+template <int LC>
+__global__ void __launch_bounds__(256) k_bwd_2_cig(const BwdArgs a, const CigArgs c)
+{
+    pdl_begin();
+    const int it = *a.itp + a.itoff;
+    int x, z0;
+    cell4(x, z0);
+    const Geo &g = a.g;
+    if (x >= g.ntx || z0 >= g.ntz) return;
+    const size_t ip = (size_t)x * g.ldz + z0;
+    bool in[4];
+    const bool any = interior4(g, x, z0, in);
+    if (any) src_v_phase<LC>(a, x, z0, ip, in);
+    const float4 pr = rcv_p_phase<LC>(a, it, x, z0, ip);
+    if (any) {
+        image4(a, ip, in, ld4(a.dpdt + ip), pr, it);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (in[k]) cig_cell(c, it, x, z0 + k);
     }
 }
 

@@ -684,6 +684,12 @@ static void launch_bwd_2(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl =
 template <int LC>
 static void launch_bwd_v(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_v<LC>, grid, s, pdl, a); }
 
+template <int LC>
+static void launch_bwd_2_cig(const BwdArgs &a, const CigArgs &c, dim3 grid, cudaStream_t s, bool pdl = false)
+{
+    launch_step(k_bwd_2_cig<LC>, grid, s, pdl, a, c);
+}
+
 // ---- TMA-staged velocity kernels (prop_tma.cuh) -----------------------------------------
 typedef CUresult (*TmapEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -1720,7 +1726,6 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
             cg.thetan = ctx->cig_thetan; cg.delt = ctx->cig_delt;
             cg.ring = F(ctx->cigring); cg.cig = F(ctx->cig);
         }
-        const dim3 cgrid((ctx->ntz + 31) / 32, (ctx->ntx + 7) / 8);
         // phases paired by kind (k_bwd_v + k_bwd_p) unless the angle gathers need the source
         // velocities of every step (k_bwd_1 + k_bwd_2, the reference's pairing)
         const int by_kind = ctx->bwd_by_kind && !want_cig;
@@ -1749,15 +1754,15 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
             if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
             if (by_kind) {
                 LC_DISPATCH(ctx->Lc, launch_bwd_p, q, grid, ctx->stream, ctx->use_pdl);
+            } else if (want_cig) {
+                // the gathers fused into the imaging launch
+                CigArgs cq = cg;
+                cq.itoff = -k;
+                LC_DISPATCH(ctx->Lc, launch_bwd_2_cig, q, cq, grid, ctx->stream, ctx->use_pdl);
             } else {
                 LC_DISPATCH(ctx->Lc, launch_bwd_2, q, grid, ctx->stream, ctx->use_pdl);
             }
             if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
-            if (want_cig) {
-                CigArgs cq = cg;
-                cq.itoff = -k;
-                k_cig<<<cgrid, dim3(32, 8), 0, ctx->stream>>>(cq);
-            }
         };
         const int kid[2] = {2, 3};
         b.itoff = 0;
@@ -1769,7 +1774,6 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
         CKR(run_steps(ctx, ctx->gbwd, key.data(), key.size(), nt - 2, -1, nt - 1, 2, kid, launch));
         if (use_tma) CKR(tma_check(ctx));
-        if (want_cig) ctx->launches += nt - 1;
         ctx->have_cig = want_cig;
     }
     CK(cudaGetLastError());
