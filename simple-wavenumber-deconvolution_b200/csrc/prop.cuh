@@ -1119,7 +1119,7 @@ __global__ void __launch_bounds__(256, 5) k_bwd_rcv_p(const BwdArgs a)
 
 // ------------------------------------------------------------------------------------
 // Angle-domain common-image gathers (sum_image_GPU_kernel_imageCIG, acoustic_HLVSPRTMLc.cu:
-// 819-905, which the reference never launches), one launch per backward step after k_bwd_2:
+// 819-905, which the reference never launches), formed in each backward step's imaging launch:
 // Poynting vectors -p*v of the source and receiver wavefields, their dot and magnitude
 // products over the last delt steps (a ring of delt slots), the reflection half-angle
 // 0.5*acos(dot/mag) in degrees, and p_s*p_r spread over the five 1-degree bins around it with
