@@ -339,6 +339,8 @@ def run_ours(args, rank, world, dist):
     tj = ROOT / "profiles" / "traffic.json"
     if tj.exists():
         t = json.loads(tj.read_text()).get(dom)
+        if t:
+            t = t.get("by_config", {}).get(args.config, t)   # a capture on this grid when there is one
         if t and "bytes_per_cell" in t:
             traffic = t["bytes_per_cell"] * N
     # the CPU sample: --cpu-steps steps on the 1601x801 grid, fewer on larger grids (same work)
