@@ -289,13 +289,16 @@ long long swd_launch_count(const swd_ctx *ctx);
  * they run: plug-in hosts that own the whole device memory pool and hand their plug-ins only
  * the buffers they pass in, and latency-bound services that reserve memory up front because
  * cudaFree synchronises the whole device and would stall their other streams.
- * Same algorithm and kernels as swd_decon, but all scratch (the per-window result slots and
- * the output taper) lives in one static device array of SWD_DECON_STATIC_SCRATCH_FLOATS
- * floats (16 MiB) that every GPU which loads libswd holds until the process exits.  The call
+ * Same algorithm and kernels as swd_decon, but all scratch (the per-window result slots, the
+ * output taper and, for the workspace or iterative variants, the per-CTA workspaces) lives in
+ * one static device array of SWD_DECON_STATIC_SCRATCH_FLOATS floats (16 MiB) that every GPU
+ * which loads libswd holds until the process exits; those variants run on as many CTAs as
+ * have a workspace that fits.  The call
  * allocates nothing: migreal/migpsf (nx*nz) and mig_dec/mig_coef (nx*nz) must be device
  * memory on the current device, already allocated by the caller.  Work is enqueued on
  * `cuda_stream` (NULL = the default stream); results are ready when that stream reaches it.
- * Returns SWD_ERR_CAPACITY when windows*outwinx*outwinz + outwinx*outwinz exceeds the array,
+ * Returns SWD_ERR_CAPACITY when windows*outwinx*outwinz + outwinx*outwinz exceeds the array
+ * (or leaves no room for one CTA workspace when one is needed),
  * SWD_ERR_ARG for invalid geometry or non-device pointers.  The first call on each device
  * looks up the array's device address (cudaGetSymbolAddress); make that first call before
  * any stream capture.  Every call reuses the same array and leaves its contents behind; each
