@@ -819,6 +819,8 @@ def run_profile_kernels(args):
     E.set_option(swd.OPT_GRAPHS, 0)
     if args.ref_pairing:
         E.set_option(swd.OPT_BWD_BY_KIND, 0)
+    if args.stored:
+        E.set_source_storage(1, swd.STRIP_I16)
     if args.path is not None:
         E.set_kernel_path(args.path)
     E.set_strip_precision({"f32": swd.STRIP_F32, "f16": swd.STRIP_F16}[w.extra.get("strips", "f32")])
@@ -889,6 +891,7 @@ def main():
     ap.add_argument("--profile-kernels", action="store_true", help="one short shot for ncu captures")
     ap.add_argument("--nt", type=int, default=30, help="record length of --profile-kernels")
     ap.add_argument("--path", type=int, default=None, help="kernel path: 0 plain (two launches per step), 1 fused")
+    ap.add_argument("--stored", action="store_true", help="--profile-kernels: stored-source RTM (int16 dp/dt)")
     ap.add_argument("--ref-pairing", action="store_true",
                     help="--profile-kernels: the reference's pairing of the backward phases (k_bwd_1, k_bwd_2)")
     ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch", "decon"], default="rtm")
