@@ -273,3 +273,39 @@ def test_born_survey_on_engine_pool_equals_sequential(bcase, swd):
         assert err < 1e-6
     finally:
         pool.close()
+
+
+def test_born_on_the_lsrtm_grid_vs_fp64_oracle(swd, orc):
+    """Born data and the checkpointed (BF16, every 50 steps) and full-storage adjoint gradients
+    on the LSRTM benchmark grid itself (801x401 with its CPML, stencil and migration model; a
+    300-step record with a shallow receiver line) against the FP64 oracle."""
+    from swd_b200 import configs
+    w = configs.c4()
+    nt, p = 300, w.pmlc
+    vp = swd.pad_model(w.vp_mig, p)
+    rho = np.full_like(vp, 1000.0)
+    rick = swd.ricker_wave(nt, w.f0, w.dt)
+    sx, sz = p + w.nx // 2, p
+    rx = np.full(80, sx + 15, np.int32)
+    rz = (p + 2 + np.arange(80)).astype(np.int32)
+    shot = swd.ShotSpec(sx, sz, rx, rz, nt)
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, nt)
+    E.setup_default(vp, rho)
+    dk = np.zeros_like(vp)
+    dk[p:-p, p:-p] = 2 * 1000.0 * w.vp_mig ** 2 * w.extra["reflectivity"]
+    dk = dk.astype(np.float32)
+    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, p, w.dx, w.dz, w.dt)
+    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), p, w.Lc, nt, w.dx, w.dz, w.dt)
+    G = orc.Geom(sx, sz, rx, rz)
+    d = E.born(shot, rick, dk)
+    ref = orc.born(M, G, rick, dk, np.float64)
+    resid = (0.5 * ref).astype(np.float32)
+    gref = orc.born_adjoint(M, G, rick, resid, np.float64)
+    E.set_checkpointing(0)
+    g_full = E.born_adjoint(shot, rick, resid)
+    E.set_checkpointing(50, swd.STRIP_BF16)
+    g_ck = E.born_adjoint(shot, rick, resid)
+    e_d, e_full, e_ck = rel_l2(d, ref), rel_l2(g_full, gref), rel_l2(g_ck, gref)
+    print(f"LSRTM grid, nt={nt}: Born data {e_d:.2e}, gradient {e_full:.2e} (full), {e_ck:.2e} (BF16 checkpoints)")
+    assert np.abs(ref).max() > 0 and np.abs(gref).max() > 0
+    assert e_d < TOL and e_full < TOL and e_ck < CKPT_TOL["bf16"]
