@@ -1166,20 +1166,10 @@ __device__ __forceinline__ void cig_cell(const CigArgs &a, int it, int x, int z)
     }
 }
 
-// the gathers as a launch of their own, one cell per thread
-__global__ void __launch_bounds__(256) k_cig(const CigArgs a)
-{
-    const int it = *a.itp + a.itoff;
-    const Geo &g = a.g;
-    const int z = blockIdx.x * 32 + threadIdx.x, x = blockIdx.y * 8 + threadIdx.y;
-    if (x >= g.ntx || z >= g.ntz || !interior(x, z, g)) return;
-    cig_cell(a, it, x, z);
-}
-
 // k_bwd_2 with the gathers fused into its imaging: after the thread's own cells are updated
 // (source v here, source p and receiver v by k_bwd_1, receiver p here), each interior cell's
 // Poynting vectors are formed from the values the thread just wrote or that the previous
-// launch left, so the gathers equal those of the separate launch.
+// launch left, i.e. from the state after the whole step.
 template <int LC>
 __global__ void __launch_bounds__(256) k_bwd_2_cig(const BwdArgs a, const CigArgs c)
 {
