@@ -32,6 +32,10 @@ is windows/s with image, PSF image and outputs in HBM, e2e the same call on pinn
 arrays.  The oracle's restatement of the reference's window loop (OpenMP over windows, FP64
 FFTs) on the host cores is the CPU baseline, and its output the parity check.
 
+--workload afor measures the PSF-data modelling stage (AFor) on the same 1601 x 801 shot: a step
+is one forward modelling shot with the Hilbert twin wavefield and the kz up/down split of the
+well column (swd_forward with the Hilbert wavelet and the kz taper), three trace sets out.
+
 --workload lsrtm measures the differentiable LSRTM gradient instead (801 x 401, nt = 4000,
 16 shots, reflectivity spikes at 1 % density): a step is one evaluation of
 J(r) = 1/2 sum_s ||L_s r - d_s||^2 and its gradient through the torch autograd path (Born
@@ -172,6 +176,10 @@ def algorithmic_bytes(kernel, w, cp, strip_len, r_n, strip_esz=4):
         #                        phi in the frame; source v, p r/w, kap (interior); strips; FP32 block sums
         #                        of I and S r/w, the FP64 fold on one step in 64; traces
         return 20 * N + 20 * Ni + 16 * Ni + Ni // 2 + 8 * x_p + strip_esz * strip_len + 4 * r_n
+    if kernel == "fwd_v2":     # velocities of the wavefield and its Hilbert twin (shared cbx, cbz)
+        return 48 * N + 16 * x_v
+    if kernel == "fwd_p2":     # pressures of both (shared ck); both fields' traces; the well columns of both
+        return 36 * N + 16 * x_p + 8 * r_n + 8 * w.extra.get("well_columns", 1) * w.ntz
     if kernel == "fwd_step":   # one fused launch per forward step: p, vx, vz r/w, vp, rho, CPML, strips
         return 32 * N + 8 * (x_v + x_p) + strip_esz * strip_len + 4 * r_n
     if kernel == "bwd_step":   # one fused launch per backward step: receiver 24N, material 8N, source 24Ni, FP64 image 32Ni
@@ -398,6 +406,124 @@ def cpu_baseline(w, samples=1, nsteps=24):
     return {"value": 1.0 / per_shot, "unit": "shots/s", "cores": cores, "kind": "port",
             "sample": f"{nsteps} of {w.nt} time steps (forward + backward) of the same shot on the full grid, "
                       f"extrapolated linearly; {best:.2f} s measured"}
+
+
+AFOR_WORKLOAD = ("c2 PSF-data modelling shot (AFor): 1601x801 @5 m, nt=6000, dt=0.4 ms, 30 Hz, 641 well receivers, "
+                 "pml 30, 8th order, with the Hilbert twin wavefield and the kz up/down split of the well column")
+
+
+def afor_cpu_baseline(w, nsteps):
+    """The oracle's FP32 OpenMP forward with the Hilbert twin and the well-column record on the
+    host cores for nsteps steps of the same shot, extrapolated to nt (the kz split is a per-shot
+    post-process, not included)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as orc
+    swd = sys.modules.get("swd_b200") or load_pkg()
+    pmlc = w.pmlc
+    vp = swd.pad_model(w.vp, pmlc)
+    rho = np.full_like(vp, 1000.0)
+    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
+    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt)
+    rx, rz = w.receivers_padded()
+    sx, sz = w.source_padded()
+    G = orc.Geom(sx, sz, rx, rz)
+    rick = swd.ricker_wave(nsteps, w.f0, w.dt)
+    t = time.perf_counter()
+    orc.forward(M, G, rick, hrick=rick[::-1].copy(), col_ix=sorted(set(int(x) for x in rx)))
+    dt = time.perf_counter() - t
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": 1.0 / (dt * w.nt / nsteps), "unit": "shots/s", "cores": cores, "kind": "port",
+            "sample": f"{nsteps} of {w.nt} time steps of the twin forward on the full grid, extrapolated linearly; "
+                      f"{dt:.2f} s measured"}
+
+
+def run_afor(args, rank, world, dist):
+    import ctypes as C
+    import torch
+    swd = load_pkg()
+    from swd_b200 import configs
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    w = configs.c2()
+    w.extra["well_columns"] = len(set(int(x) for x in w.rec_x))
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt, device=dev)
+    vtrue = swd.pad_model(w.vp, w.pmlc)
+    E.setup_default(vtrue, np.full_like(vtrue, 1000.0))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    E.set_stream(stream.cuda_stream)
+    rick = swd.ricker_wave(w.nt, w.f0, w.dt)
+    hrick = E.hilbert(rick)
+    coef, _ = swd.kz_taper(swd.pow2(w.ntz), w.dz)
+    rx, rz = w.receivers_padded()
+    sx, sz = w.source_padded()
+    shot = swd.ShotSpec(sx, sz, rx, rz, w.nt)
+    sh, keep = E._shot(shot)
+    r_n = len(rx)
+    dev_in = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda() for a in (rick, hrick, coef)]
+    host_in = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory() for a in (rick, hrick, coef)]
+    dev_out = [torch.empty((r_n, w.nt), dtype=torch.float32, device="cuda") for _ in range(3)]
+    host_out = [torch.empty((r_n, w.nt), dtype=torch.float32).pin_memory() for _ in range(3)]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step(ins, outs):
+        E._ck(swd.lib().swd_forward(E._h, C.byref(sh), *[swd._ptr(t) for t in ins], *[swd._ptr(t) for t in outs]))
+
+    def timed(ins, outs, K, W, profile=False):
+        for _ in range(W):
+            step(ins, outs)
+        if profile:
+            E.profile(8)
+            E.profile_read()
+        n0 = E.launch_count()
+        torch.cuda.synchronize()
+        total = 0.0
+        for _ in range(K):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(ins, outs)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        launches = E.launch_count() - n0
+        prof = E.profile_read() if profile else None
+        E.profile(0)
+        return total, launches, prof
+
+    with ClockSampler(dev) as clk:
+        t_val, launches, prof = timed(dev_in, dev_out, args.steps, args.warmup, profile=True)
+        t_e2e, _, _ = timed(host_in, host_out, args.steps, 1)
+    t_val, t_e2e = max_over_ranks(dist, [t_val, t_e2e], "cuda")
+    value = replica_throughput(args.steps, world, t_val)
+    e2e = replica_throughput(args.steps, world, t_e2e)
+    per_launch = {k: ms / n for k, (ms, n) in prof.items() if n}
+    live = {}
+    if all(k in per_launch for k in ("fwd_pass_step", "fwd_v", "fwd_p")):
+        t, a1, a2 = per_launch["fwd_pass_step"], per_launch["fwd_v"], per_launch["fwd_p"]
+        live = {"fwd_v2": t * a1 / (a1 + a2), "fwd_p2": t * a2 / (a1 + a2)}
+    dom = max(live, key=live.get)
+    peak, src = peaks()
+    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, w.pmlc, w.dx, w.dz, w.dt)
+    ab = algorithmic_bytes(dom, w, cp, 0, r_n)
+    achieved = ab / (live[dom] * 1e-3) / 1e9
+    cpu = afor_cpu_baseline(w, max(16, args.cpu_steps // 3))
+    return {
+        "metric": "modelling shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random-field model)",
+        "config": {"workload": AFOR_WORKLOAD, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(sum(t.numel() * 4 for t in host_in)),
+                "d2h_bytes_per_step": int(3 * r_n * w.nt * 4)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": src,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": ab,
+                     "avg_launch_us": live[dom] * 1e3, "kernels_us": {k: v * 1e3 for k, v in live.items()},
+                     "step_us": {"fwd_pass_step": per_launch.get("fwd_pass_step", 0.0) * 1e3}},
+        "gpu_launches": launches,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
 
 
 LSRTM_WORKLOAD = ("c4 LSRTM gradient: 801x401 @5 m, nt=4000, dt=0.4 ms, 16 shots, 321 well receivers, "
@@ -917,7 +1043,7 @@ def main():
     ap.add_argument("--stored", action="store_true", help="--profile-kernels: stored-source RTM (int16 dp/dt)")
     ap.add_argument("--ref-pairing", action="store_true",
                     help="--profile-kernels: the reference's pairing of the backward phases (k_bwd_1, k_bwd_2)")
-    ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch", "decon"], default="rtm")
+    ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch", "decon", "afor"], default="rtm")
     ap.add_argument("--config", choices=["c2", "c5", "shipped"], default="c2",
                     help="grid of --workload rtm (c2, c5) or decon (c2, c5, shipped: the reference's window geometry)")
     ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
@@ -948,7 +1074,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = td
-    runner = {"rtm": run_ours, "lsrtm": run_lsrtm, "batch": run_batch, "decon": run_decon}[args.workload]
+    runner = {"rtm": run_ours, "lsrtm": run_lsrtm, "batch": run_batch, "decon": run_decon, "afor": run_afor}[args.workload]
     out = runner(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(out), flush=True)
