@@ -514,6 +514,7 @@ def run_afor(args, rank, world, dist):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random-field model)",
         "config": {"workload": AFOR_WORKLOAD, "parallelism": f"replicas x{world}",
                    "l2": "flushed (256 MiB write) before every timed step"},
+        "gcell_updates_per_s": value * 2 * w.nt * w.ntx * w.ntz / 1e9,   # the wavefield and its twin
         "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(sum(t.numel() * 4 for t in host_in)),
                 "d2h_bytes_per_step": int(3 * r_n * w.nt * 4)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": src,
