@@ -152,6 +152,8 @@ class BornSurvey(torch.autograd.Function):
     @staticmethod
     def forward(ctx, r: torch.Tensor, ops, pool: EnginePool):
         r32 = _dev(r.float())
+        # the pool's threads wait on their own (default) streams: finish this thread's work first
+        _sync(r32.device)
 
         def fwd(E, op):
             ck = op.ckpt_buffer(E)
@@ -164,6 +166,8 @@ class BornSurvey(torch.autograd.Function):
     @staticmethod
     def backward(ctx, *grads):
         items = [(op, g, ck) for op, g, ck in zip(ctx.ops, grads, ctx.ckpts) if g is not None]
+        if items:
+            _sync(items[0][1].device)   # the incoming gradients are complete before other threads read them
         parts = ctx.pool.map(lambda E, it: it[0].adjoint(it[1], it[2], engine=E), items)
         g = parts[0].clone()
         for q in parts[1:]:
