@@ -187,6 +187,19 @@ def algorithmic_bytes(kernel, w, cp, strip_len, r_n, strip_esz=4):
     raise KeyError(kernel)
 
 
+def measured_traffic(kernel, config, cells):
+    """DRAM bytes (read + written) of one launch of `kernel` on a grid of `cells` cells, from the
+    ncu captures summarised in profiles/traffic.json (a capture on this grid when there is one);
+    None without a capture."""
+    tj = ROOT / "profiles" / "traffic.json"
+    if not tj.exists():
+        return None
+    t = json.loads(tj.read_text()).get(kernel)
+    if t:
+        t = t.get("by_config", {}).get(config, t)
+    return t["bytes_per_cell"] * cells if t and "bytes_per_cell" in t else None
+
+
 def setup(swd, w, device):
     import torch
     E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt, device=device)
@@ -343,14 +356,7 @@ def run_ours(args, rank, world, dist):
     peak, src = peaks()
     ab = algorithmic_bytes(dom, w, cp, slen, r_n, 4 if strips == "f32" else 2)
     achieved = ab / (live[dom] * 1e-3) / 1e9
-    traffic = None
-    tj = ROOT / "profiles" / "traffic.json"
-    if tj.exists():
-        t = json.loads(tj.read_text()).get(dom)
-        if t:
-            t = t.get("by_config", {}).get(args.config, t)   # a capture on this grid when there is one
-        if t and "bytes_per_cell" in t:
-            traffic = t["bytes_per_cell"] * N
+    traffic = measured_traffic(dom, args.config, N)
     # the CPU sample: --cpu-steps steps on the 1601x801 grid, fewer on larger grids (same work)
     cpu = cpu_baseline(w, samples=1, nsteps=max(32, int(args.cpu_steps * 1669 * 869 / N)))
     return {
@@ -518,7 +524,8 @@ def run_afor(args, rank, world, dist):
         "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(sum(t.numel() * 4 for t in host_in)),
                 "d2h_bytes_per_step": int(3 * r_n * w.nt * 4)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": src,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": ab,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": measured_traffic(dom, "c2", w.ntx * w.ntz),
+                     "algorithmic_bytes_per_launch": ab,
                      "avg_launch_us": live[dom] * 1e3, "kernels_us": {k: v * 1e3 for k, v in live.items()},
                      "step_us": {"fwd_pass_step": per_launch.get("fwd_pass_step", 0.0) * 1e3}},
         "gpu_launches": launches,
@@ -669,7 +676,8 @@ def run_lsrtm(args, rank, world, dist):
         "gradient_vs_fp32_full_storage": {"rel_l2": err, "full_storage_ms_per_step": t_full,
                                           "checkpoint_bytes_per_shot": ck_bytes, "full_storage_bytes_per_shot": full_bytes},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": src, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": ab,
+                     "frac": achieved / peak, "traffic": measured_traffic(dom, "c4", w.ntx * w.ntz),
+                     "algorithmic_bytes_per_launch": ab,
                      "avg_launch_us": live[dom] * 1e3, "kernels_us": {k: v * 1e3 for k, v in live.items()},
                      "step_us": {k: per_launch[k] * 1e3 for k in ("fwd_pass_step", "adj_pass_step") if k in per_launch}},
         "gpu_launches": launches,
@@ -959,6 +967,10 @@ def run_profile_kernels(args):
     kernels are the same ones the graphs replay), which keeps ncu's per-launch handling fast.
     Prints per-kernel event timings."""
     import ctypes as C
+    if args.workload == "afor":
+        return run_profile_afor(args)
+    if args.workload == "lsrtm":
+        return run_profile_lsrtm(args)
     swd = load_pkg()
     from swd_b200 import configs
     w = configs.CONFIGS[args.config]()
@@ -983,6 +995,65 @@ def run_profile_kernels(args):
     E.rtm_shot(shot, rick, data, want=())
     prof = E.profile_read()
     print(json.dumps({"mode": "profile-kernels", "grid": [w.ntx, w.ntz], "nt": w.nt, "launches": E.launch_count(),
+                      "kernels_us": {k: ms / n * 1e3 for k, (ms, n) in prof.items() if n}}))
+
+
+def run_profile_afor(args):
+    """--profile-kernels of the modelling workload: one forward of the 1601x801 shot with the
+    Hilbert twin and the kz split of the well column, --nt steps, kernels launched directly."""
+    import ctypes as C
+    import torch
+    swd = load_pkg()
+    from swd_b200 import configs
+    w = configs.c2()
+    w.nt = args.nt
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt)
+    vtrue = swd.pad_model(w.vp, w.pmlc)
+    E.setup_default(vtrue, np.full_like(vtrue, 1000.0))
+    E.set_option(swd.OPT_GRAPHS, 0)
+    rick = swd.ricker_wave(w.nt, w.f0, w.dt)
+    coef, _ = swd.kz_taper(swd.pow2(w.ntz), w.dz)
+    rx, rz = w.receivers_padded()
+    sx, sz = w.source_padded()
+    sh, keep = E._shot(swd.ShotSpec(sx, sz, rx, rz, w.nt))
+    ins = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda() for a in (rick, E.hilbert(rick), coef)]
+    outs = [torch.empty((len(rx), w.nt), dtype=torch.float32, device="cuda") for _ in range(3)]
+    torch.cuda.synchronize()
+    E.profile(1)
+    E._ck(swd.lib().swd_forward(E._h, C.byref(sh), *[swd._ptr(t) for t in ins], *[swd._ptr(t) for t in outs]))
+    torch.cuda.synchronize()
+    prof = E.profile_read()
+    print(json.dumps({"mode": "profile-kernels", "workload": "afor", "grid": [w.ntx, w.ntz], "nt": w.nt,
+                      "launches": E.launch_count(),
+                      "kernels_us": {k: ms / n * 1e3 for k, (ms, n) in prof.items() if n}}))
+
+
+def run_profile_lsrtm(args):
+    """--profile-kernels of the LSRTM workload: the Born data and the gradient of one 801x401
+    shot (BF16 checkpoints every 50 steps), --nt steps, kernels launched directly."""
+    import torch
+    swd = load_pkg()
+    from swd_b200 import configs, lsrtm
+    w = configs.c4()
+    w.nt = args.nt
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt)
+    vmig = swd.pad_model(w.vp_mig, w.pmlc)
+    rho = np.full_like(vmig, 1000.0)
+    E.setup_default(vmig, rho)
+    E.set_option(swd.OPT_GRAPHS, 0)
+    E.set_checkpointing(50, swd.STRIP_BF16)
+    rick = swd.ricker_wave(w.nt, w.f0, w.dt)
+    rx, rz = w.receivers_padded()
+    op = lsrtm.BornOperator(E, swd.ShotSpec(w.sx[0] + w.pmlc, w.pmlc, rx, rz, w.nt), rick, vmig, rho)
+    r = torch.tensor(w.extra["reflectivity"], device="cuda").requires_grad_(True)
+    torch.cuda.synchronize()
+    E.profile(1)
+    d = lsrtm.born(r, op)
+    (0.5 * (d.double() ** 2).sum()).backward()
+    torch.cuda.synchronize()
+    prof = E.profile_read()
+    print(json.dumps({"mode": "profile-kernels", "workload": "lsrtm", "grid": [w.ntx, w.ntz], "nt": w.nt,
+                      "launches": E.launch_count(),
                       "kernels_us": {k: ms / n * 1e3 for k, (ms, n) in prof.items() if n}}))
 
 

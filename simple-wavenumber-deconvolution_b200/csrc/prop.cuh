@@ -601,8 +601,20 @@ __global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
     for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.m, a.w[k], a.g.odx, a.g.odz, x, z0);
 }
 
+// Blocks per SM asked of the register allocator: 5 (48 registers) for one wavefield and for the
+// twin of the modelling forward (4 bytes of spill there), 4 (64 registers, no spill) for the Born
+// twin; left free for LC > 4 and the batched kernels.  The twin at its free 80 registers ran 3
+// blocks per SM and its launches took 8% longer.
+template <int LC, int NW, int MODE, bool BATCH>
+constexpr int fwd_p_min_blocks()
+{
+    if (BATCH || LC > 4) return 1;
+    if (NW == 1) return MODE == FP_BORN ? 1 : 5;
+    return MODE == FP_PLAIN ? 5 : 4;
+}
+
 template <int LC, int NW, int MODE, bool BATCH = false>
-__global__ void __launch_bounds__(256, (NW == 1 && MODE != FP_BORN && !BATCH && LC <= 4) ? 5 : 1)
+__global__ void __launch_bounds__(256, (fwd_p_min_blocks<LC, NW, MODE, BATCH>()))
     k_fwd_p(const FwdArgs a0)
 {
     pdl_begin();
