@@ -971,6 +971,8 @@ def run_profile_kernels(args):
         return run_profile_afor(args)
     if args.workload == "lsrtm":
         return run_profile_lsrtm(args)
+    if args.workload == "batch":
+        return run_profile_batch(args)
     swd = load_pkg()
     from swd_b200 import configs
     w = configs.CONFIGS[args.config]()
@@ -1054,6 +1056,31 @@ def run_profile_lsrtm(args):
     prof = E.profile_read()
     print(json.dumps({"mode": "profile-kernels", "workload": "lsrtm", "grid": [w.ntx, w.ntz], "nt": w.nt,
                       "launches": E.launch_count(),
+                      "kernels_us": {k: ms / n * 1e3 for k, (ms, n) in prof.items() if n}}))
+
+
+def run_profile_batch(args):
+    """--profile-kernels of the batched RTM: the first two shots of the 1201x601 survey as one
+    batch (B = 2), --nt steps each, seeded random data, kernels launched directly."""
+    swd = load_pkg()
+    from swd_b200 import configs
+    w = configs.c3()
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, args.nt)
+    vmig = swd.pad_model(w.vp_mig, w.pmlc)
+    E.setup_default(vmig, np.full_like(vmig, 1000.0))
+    E.set_option(swd.OPT_GRAPHS, 0)
+    E.set_option(swd.OPT_BATCH, 2)
+    rng = np.random.default_rng(0)
+    shots, ricks, data = [], [], []
+    for s in w.extra["shots"][:2]:
+        shots.append(swd.ShotSpec(s["sx"] + w.pmlc, s["sz"] + w.pmlc, s["rec_x"] + w.pmlc, s["rec_z"] + w.pmlc, args.nt))
+        ricks.append(swd.ricker_wave(args.nt, s["f0"], w.dt))
+        data.append(rng.standard_normal((len(s["rec_x"]), args.nt)).astype(np.float32) * 1e-6)
+    E.profile(1)
+    E.rtm_batch(shots, ricks, data)
+    prof = E.profile_read()
+    print(json.dumps({"mode": "profile-kernels", "workload": "batch", "grid": [w.ntx, w.ntz], "nt": args.nt,
+                      "batch": E.get_option(swd.OPT_BATCH_TUNED), "launches": E.launch_count(),
                       "kernels_us": {k: ms / n * 1e3 for k, (ms, n) in prof.items() if n}}))
 
 
