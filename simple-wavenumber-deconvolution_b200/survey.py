@@ -5,7 +5,8 @@ the GPU on grids where one shot's launches are latency-bound (a few hundred thou
 million cells), and it composes with swd_rtm_batch, which each engine may use for its share.
 
 The reference migrates its shots one after another on each GPU (acoustic_HLVSPRTMC.cpp:576-745)
-and sums the images with MPI_Allreduce (:750-752); rtm_survey sums the engines' FP64 stacks.
+and sums the images with MPI_Allreduce (:750-752); rtm_survey reads each engine's stack (FP64 on
+the device, float32 out, like the reference's image) and sums the parts in float64.
 """
 from __future__ import annotations
 
@@ -43,7 +44,6 @@ class EnginePool:
 
     def close(self):
         self._exec.shutdown()
-
 
 
 def rtm_survey(pool: EnginePool, shots, ricks, datas, flags=RTM_PREPROCESS, batched=True, edge_zero=True):
