@@ -276,6 +276,10 @@ int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *
         return fail(ctx, SWD_ERR_ARG, "swd_rtm_batch stacks every shot; ILLUM_RCV / NO_STACK apply to swd_rtm_shot");
     for (int i = 0; i < nshots; i++)
         if (!ricks[i] || !data[i]) return fail(ctx, SWD_ERR_ARG, "shot %d has no wavelet or data", i);
+    {   // every shot checked before any device work: an argument error leaves the stack as it was
+        ShotPlan P;
+        for (int i = 0; i < nshots; i++) CKR(plan_shot_host(ctx, &shots[i], P));
+    }
     if (nshots == 0) return SWD_OK;
     // longest records first, so each batch's records end close together
     std::vector<int> order(nshots);

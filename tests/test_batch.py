@@ -106,6 +106,23 @@ def test_batch_rejects_unsupported_flags(survey, swd):
         survey.E.rtm_batch(survey.shots, survey.ricks, survey.data, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK)
 
 
+def test_batch_checks_every_shot_before_migrating(survey, reference, swd):
+    """A shot with its source outside the grid, behind shots that would batch first: the call
+    fails on the host and the stack is left as it was (no shot of the call is stacked)."""
+    E = survey.E
+    E.set_option(swd.OPT_GRAPHS, 1)
+    E.set_option(swd.OPT_BATCH, 1)
+    E.stack_reset()
+    E.rtm_batch(survey.shots[:1], survey.ricks[:1], survey.data[:1])
+    before = E.stack(edge_zero=False)
+    bad = survey.shots[1]
+    bad = swd.ShotSpec(E.ntx + 5, bad.s_iz, bad.r_ix, bad.r_iz, bad.nt)
+    shots = survey.shots[2:] + [bad]
+    with pytest.raises(swd.SwdError, match="source cell"):
+        E.rtm_batch(shots, survey.ricks[2:] + [survey.ricks[1]], survey.data[2:] + [survey.data[1]])
+    assert np.array_equal(E.stack(edge_zero=False), before)
+
+
 def test_survey_on_engine_pool(survey, reference, swd):
     """rtm_survey over three engines (concurrent host threads and streams, each through
     swd_rtm_batch) stacks to the sequential image up to the float32 rounding of the per-engine
