@@ -162,7 +162,8 @@ int swd_stack_reset(swd_ctx *ctx);
  * to the FP64 stack exactly as swd_rtm_shot adds it.  B = swd_set_option(SWD_OPT_BATCH), or
  * chosen by timing probes of B = 1, 2, 4, 8 on the first call (SWD_OPT_BATCH_TUNED reads the
  * choice).  flags: SWD_RTM_PREPROCESS only (the batch always stacks).  The context's current
- * strip precision applies. */
+ * strip precision applies.  Every shot is validated before any device work: a bad shot returns
+ * SWD_ERR_ARG and leaves the stack unchanged. */
 int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *const *ricks,
                   const float *const *data, unsigned flags);
 
