@@ -358,7 +358,7 @@ def run_ours(args, rank, world, dist):
     achieved = ab / (live[dom] * 1e-3) / 1e9
     traffic = measured_traffic(dom, args.config, N)
     # the CPU sample: --cpu-steps steps on the 1601x801 grid, fewer on larger grids (same work)
-    cpu = cpu_baseline(w, samples=1, nsteps=max(32, int(args.cpu_steps * 1669 * 869 / N)))
+    cpu = rank0_single(rank, world, lambda: cpu_baseline(w, samples=1, nsteps=rtm_cpu_steps(args, w)))
     return {
         "metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -383,6 +383,18 @@ def run_ours(args, rank, world, dist):
         "clocks": clk.summary(),
         "stored_source": stored,
     }
+
+
+def rank0_single(rank, world, sample):
+    """The CPU baseline is timed on rank 0 of a one-GPU run only (None otherwise), so that
+    ranks of a multi-GPU run do not time the host cores against one another."""
+    return sample() if rank == 0 and world == 1 else None
+
+
+def rtm_cpu_steps(args, w):
+    """Time steps of the RTM CPU sample: --cpu-steps on the 1601x801 grid, fewer on larger
+    grids (the same host work)."""
+    return max(32, int(args.cpu_steps * 1669 * 869 / (w.ntx * w.ntz)))
 
 
 def cpu_baseline(w, samples=1, nsteps=24):
@@ -513,7 +525,7 @@ def run_afor(args, rank, world, dist):
     cp = swd.get_absorbing_parameters(w.ntx, w.ntz, w.pmlc, w.dx, w.dz, w.dt)
     ab = algorithmic_bytes(dom, w, cp, 0, r_n)
     achieved = ab / (live[dom] * 1e-3) / 1e9
-    cpu = afor_cpu_baseline(w, max(16, args.cpu_steps // 3))
+    cpu = rank0_single(rank, world, lambda: afor_cpu_baseline(w, max(16, args.cpu_steps // 3)))
     return {
         "metric": "modelling shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -657,7 +669,7 @@ def run_lsrtm(args, rank, world, dist):
     ab = adjoint_bytes(dom, w, cp, r_n)
     achieved = ab / (live[dom] * 1e-3) / 1e9
     N, Ni = w.ntx * w.ntz, w.nx * w.nz
-    cpu = lsrtm_cpu_baseline(w, nsteps=args.cpu_steps // 3)
+    cpu = rank0_single(rank, world, lambda: lsrtm_cpu_baseline(w, nsteps=args.cpu_steps // 3))
     return {
         "metric": "LSRTM gradient shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -933,6 +945,33 @@ def run_decon(args, rank, world, dist):
     return out
 
 
+def survey_cpu_baseline(w, nsteps):
+    """The oracle's FP32 OpenMP RTM of the survey's first shot for nsteps steps on the full grid;
+    its time per step, times the survey's total steps (every shot's nt), gives the survey's
+    shots/s."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as orc
+    swd = sys.modules.get("swd_b200") or load_pkg()
+    pmlc = w.pmlc
+    vp = swd.pad_model(w.vp_mig, pmlc)
+    rho = np.full_like(vp, 1000.0)
+    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
+    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt)
+    shots = w.extra["shots"]
+    s = shots[0]
+    G = orc.Geom(int(s["sx"]) + pmlc, int(s["sz"]) + pmlc, s["rec_x"] + pmlc, s["rec_z"] + pmlc)
+    rick = swd.ricker_wave(nsteps, s["f0"], w.dt)
+    data = np.random.default_rng(0).standard_normal((len(s["rec_x"]), nsteps)).astype(np.float32)
+    t = time.perf_counter()
+    orc.rtm_shot(M, G, rick, data)
+    dt = time.perf_counter() - t
+    total = dt / nsteps * sum(int(x["nt"]) for x in shots)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": len(shots) / total, "unit": "shots/s", "cores": cores, "kind": "port",
+            "sample": f"{nsteps} steps (forward + backward) of the survey's first shot on the full grid; the time "
+                      f"per step times the survey's {sum(int(x['nt']) for x in shots)} steps; {dt:.2f} s measured"}
+
+
 def lsrtm_cpu_baseline(w, nsteps=100):
     """The oracle's Born modelling + adjoint (FP32, OpenMP stencils, serial adjoint scatters)
     for one shot over nsteps steps on the full grid, extrapolated to nt."""
@@ -1108,23 +1147,41 @@ def run_reference_decon(args):
 
 
 def run_reference(args):
+    """The reference arm: the oracle's restatement of the reference's loops on the host cores,
+    for the metric, unit and workload of our arm (--workload, --config); each step a bounded
+    sample of that workload."""
     if args.workload == "decon":
         return run_reference_decon(args)
-    from swd_b200 import configs  # noqa: F401  (package already loaded by caller)
-    w = sys.modules["swd_b200"].configs.c2()
+    configs = sys.modules["swd_b200"].configs
+    if args.workload == "afor":
+        w = configs.c2()
+        metric, workload = "modelling shots/s", AFOR_WORKLOAD
+        sample = lambda: afor_cpu_baseline(w, max(16, args.cpu_steps // 3))
+    elif args.workload == "lsrtm":
+        w = configs.c4()
+        metric, workload = "LSRTM gradient shots/s", LSRTM_WORKLOAD
+        sample = lambda: lsrtm_cpu_baseline(w, nsteps=max(8, args.cpu_steps // 3))
+    elif args.workload == "batch":
+        w = configs.c3()
+        metric, workload = "RTM shots/s", BATCH_WORKLOAD
+        sample = lambda: survey_cpu_baseline(w, max(8, args.cpu_steps))
+    else:
+        w = configs.CONFIGS[args.config]()
+        metric, workload = "RTM shots/s", WORKLOADS[args.config]
+        sample = lambda: cpu_baseline(w, samples=1, nsteps=rtm_cpu_steps(args, w))
     t0 = time.perf_counter()
     vals = []
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(w, samples=1, nsteps=args.cpu_steps)
+        cb = sample()
         if i >= args.warmup:
             vals.append(1.0 / cb["value"])
     mean = float(np.mean(vals))
     value = 1.0 / mean
     cb["value"] = value
-    return {"metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": 1, "steps": args.steps,
+    return {"metric": metric, "value": value, "unit": "shots/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "parallelism": "host OpenMP"},
+            "config": {"workload": workload, "parallelism": "host OpenMP"},
             "cpu_baseline": cb, "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": time.perf_counter() - t0}
 
