@@ -831,6 +831,7 @@ def run_batch(args, rank, world, dist):
         "stack_rel_l2_vs_plain": rel(st_bat, st_plain),
         "stack_rel_l2_int16_strips_vs_plain": rel(st_bat16, st_plain),
         "gpu_launches": launches,
+        "cpu_baseline": rank0_single(rank, world, lambda: survey_cpu_baseline(w, max(8, args.cpu_steps // 3))),
         "clocks": clk.summary(),
     }
 
