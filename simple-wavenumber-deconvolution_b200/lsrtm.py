@@ -38,7 +38,9 @@ def _dev(t: torch.Tensor) -> torch.Tensor:
 
 
 def _sync(device):
-    torch.cuda.current_stream(device).synchronize()
+    """Wait for the calling thread's current stream on `device` (nothing to wait for on the CPU)."""
+    if torch.device(device).type == "cuda":
+        torch.cuda.current_stream(device).synchronize()
 
 
 class BornOperator:
