@@ -11,7 +11,8 @@
 //     %dsource_seismogram_scatter{,up,down}.bin.  The reference perturbs density
 //     (rho += 1e-3*vp, :697-705); `swd.perturb = velocity` in parameter.txt multiplies vp by
 //     (1 + swd.perturb_amp, default 0.01) instead.
-// Extensions (parameter.txt lines `swd.key = value`): device, perturb, perturb_amp.
+// Extensions (parameter.txt lines `swd.key = value`): device, perturb (density|velocity; an
+// unknown value is an error), perturb_amp.
 #include <math.h>
 #include "common.h"
 
@@ -27,7 +28,8 @@ int main(int, char **)
     }
     auto ext = extensions((up + "/parameter.txt").c_str());
     const int device = ext_int(ext, "device", 0);
-    const std::string perturb = ext_str(ext, "perturb", "density");
+    std::string perturb;
+    if (!ext_choice(ext, "perturb", {"density", "velocity"}, perturb)) return 1;
     const float perturb_amp = (float)atof(ext_str(ext, "perturb_amp", "0.01").c_str());
     printf("Number of MPI thread is 1\n");
     printf("The simulation time step is %d\n", m.itmax);

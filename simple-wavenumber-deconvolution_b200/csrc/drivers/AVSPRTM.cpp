@@ -10,8 +10,9 @@
 // end the stacked, edge-zeroed migration_pp.bin / migration_psf.bin.
 // The final forward wavefield stays in GPU memory; the reference's wavefield%d_itmax%d.dat
 // disk round trip is not needed.
-// Extensions (parameter.txt lines `swd.key = value`): device, strip_precision (f32|f16|bf16),
-// data (up|full|down: which AFor record to migrate; the reference always uses up).
+// Extensions (parameter.txt lines `swd.key = value`): device, strip_precision
+// (f32|f16|bf16|i16), data (up|full|down: which AFor record to migrate; the reference always
+// uses up).  An unknown value of either is an error.
 #include <math.h>
 #include "common.h"
 
@@ -26,8 +27,10 @@ int main(int, char **)
     }
     auto ext = extensions("./parameter.txt");
     const int device = ext_int(ext, "device", 0);
-    const std::string sp = ext_str(ext, "strip_precision", "f32");
-    const std::string which = ext_str(ext, "data", "up");
+    std::string sp, which;
+    if (!ext_choice(ext, "strip_precision", {"f32", "f16", "bf16", "i16"}, sp) ||
+        !ext_choice(ext, "data", {"up", "full", "down"}, which))
+        return 1;
     printf("Number of MPI thread is 1\n");
     printf("The simulation time step is %d\n", m.itmax);
 
@@ -47,6 +50,7 @@ int main(int, char **)
     swd_ctx *ctx = make_context(m, device);
     if (sp == "f16") die_on(ctx, swd_set_strip_precision(ctx, SWD_STRIP_F16), "strip precision");
     else if (sp == "bf16") die_on(ctx, swd_set_strip_precision(ctx, SWD_STRIP_BF16), "strip precision");
+    else if (sp == "i16") die_on(ctx, swd_set_strip_precision(ctx, SWD_STRIP_I16), "strip precision");
 
     std::vector<float> rick(m.itmax);
     swd_prep_ricker(m.itmax, m.f0, m.dt, rick.data());

@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 #include <map>
+#include <initializer_list>
 #include "swd.h"
 
 namespace drv {
@@ -77,6 +78,22 @@ inline std::string ext_str(const std::map<std::string, std::string> &kv, const c
 {
     auto it = kv.find(k);
     return it == kv.end() ? std::string(def) : it->second;
+}
+// An extension whose value must be one of `choices` (the first is the default).  An unknown
+// value is reported and the caller stops before any device work, instead of running with a
+// silent default.
+inline bool ext_choice(const std::map<std::string, std::string> &kv, const char *k,
+                       std::initializer_list<const char *> choices, std::string &out)
+{
+    auto it = kv.find(k);
+    out = it == kv.end() ? std::string(*choices.begin()) : it->second;
+    std::string all;
+    for (const char *c : choices) {
+        if (out == c) return true;
+        all += (all.empty() ? "" : "|") + std::string(c);
+    }
+    printf("swd.%s = %s: expected %s\n", k, out.c_str(), all.c_str());
+    return false;
 }
 
 inline bool write_f32(const std::string &path, const float *a, size_t n)

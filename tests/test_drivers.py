@@ -50,6 +50,26 @@ def test_truncated_parameter_file_is_an_error():
         assert r.returncode != 0
 
 
+@pytest.mark.parametrize("prog,line,msg", [
+    ("AVSPRTM", "swd.data = sideways", "swd.data = sideways: expected up|full|down"),
+    ("AVSPRTM", "swd.strip_precision = fp16", "swd.strip_precision = fp16: expected f32|f16|bf16|i16"),
+    ("AFor", "swd.perturb = pressure", "swd.perturb = pressure: expected density|velocity"),
+])
+def test_unknown_extension_value_is_an_error(prog, line, msg):
+    """An extension value the program does not know stops it before any device work, instead
+    of running with the default."""
+    mk = _mkg("make_golden_ref_gpu")
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        mk.write_params(d / "parameter.txt", mk.CASE, 0)
+        with open(d / "parameter.txt", "a") as f:
+            f.write(line + "\n")
+        cwd = d / "forward" if prog == "AFor" else d
+        r = subprocess.run([str(PKG_DIR / prog)], cwd=cwd, capture_output=True, text=True)
+        assert r.returncode != 0
+        assert msg in r.stdout
+
+
 def test_decon_rejects_even_windows():
     mk = _mkg("make_golden")
     with tempfile.TemporaryDirectory() as d:
