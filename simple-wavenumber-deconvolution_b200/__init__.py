@@ -24,7 +24,7 @@ import numpy as np
 PKG_DIR = Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "libswd.so"
 
-SWD_OK, SWD_ERR_ARG, SWD_ERR_CUDA, SWD_ERR_ALLOC, SWD_ERR_STATE, SWD_ERR_DEVICE = range(6)
+SWD_OK, SWD_ERR_ARG, SWD_ERR_CUDA, SWD_ERR_ALLOC, SWD_ERR_STATE, SWD_ERR_DEVICE, SWD_ERR_CAPACITY = range(7)
 STRIP_F32, STRIP_F16, STRIP_BF16, STRIP_I16 = 0, 1, 2, 3
 PATH_PLAIN, PATH_FUSED = 0, 1
 RTM_PREPROCESS, RTM_ILLUM_RCV, RTM_NO_STACK, RTM_CIG = 1, 2, 4, 8

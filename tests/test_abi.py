@@ -36,6 +36,21 @@ def test_version_and_error_paths(swd):
     assert L.swd_last_error(None) == b"null context"
 
 
+def test_python_constants_equal_the_header(swd):
+    """The Python view's status codes, strip precisions, RTM flags, kernel paths and option ids
+    are the values include/swd.h defines."""
+    defs = {m.group(1): int(m.group(2)) for m in
+            re.finditer(r"^#define (SWD_\w+) (\d+)u?\b", (ROOT / "include" / "swd.h").read_text(), re.M)}
+    pairs = {k: getattr(swd, k) for k in dir(swd) if k.startswith("SWD_")}
+    pairs.update({"SWD_" + k: getattr(swd, k) for k in dir(swd)
+                  if k.split("_")[0] in ("STRIP", "RTM", "PATH", "OPT") and isinstance(getattr(swd, k), int)})
+    assert len(pairs) >= 24
+    for name, value in pairs.items():
+        assert name in defs, name
+        assert defs[name] == value, (name, defs[name], value)
+    assert len(swd.Engine.PROFILE_NAMES) == defs["SWD_NKERNELS"]
+
+
 def test_decon_geometry(swd, orc):
     for args in [((845, 702), (31, 31), (71, 71), (11, 11)), ((120, 100), (11, 11), (21, 21), (5, 5)),
                  ((130, 97), (11, 9), (25, 21), (5, 4))]:
