@@ -36,6 +36,31 @@ def test_version_and_error_paths(swd):
     assert L.swd_last_error(None) == b"null context"
 
 
+def declared_arity():
+    """{function: number of parameters} of every prototype in include/swd.h."""
+    src = (ROOT / "include" / "swd.h").read_text()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(?:int|long long|const char|unsigned|size_t|void)\s*\**\s*(swd_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", src):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_python_signatures_match_the_header(swd):
+    """Every ctypes signature the Python view declares has the header's parameter count."""
+    arity = declared_arity()
+    assert sorted(arity) == declared_functions()
+    L = swd.lib()
+    checked = 0
+    for name, n in arity.items():
+        f = getattr(L, name)
+        if f.argtypes is not None:
+            assert len(f.argtypes) == n, (name, len(f.argtypes), n)
+            checked += 1
+    assert checked >= 30
+
+
 def test_python_constants_equal_the_header(swd):
     """The Python view's status codes, strip precisions, RTM flags, kernel paths and option ids
     are the values include/swd.h defines."""
