@@ -61,6 +61,31 @@ def test_python_signatures_match_the_header(swd):
     assert checked >= 30
 
 
+def test_python_structures_have_the_c_layout(swd, tmp_path):
+    """The ctypes structures of the Python view (Grid, Shot, DeconParams) have the size and
+    field offsets that a C compiler gives swd_grid, swd_shot and swd_decon_params."""
+    import subprocess
+    structs = {"swd_grid": swd.Grid, "swd_shot": swd.Shot, "swd_decon_params": swd.DeconParams}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "swd.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, field, value = line.split()
+        got[(cname, field)] = int(value)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
 def test_python_constants_equal_the_header(swd):
     """The Python view's status codes, strip precisions, RTM flags, kernel paths and option ids
     are the values include/swd.h defines."""
