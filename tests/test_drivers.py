@@ -164,6 +164,22 @@ def test_decon2d_mine_iterative_option(orc):
 REF_ON_SWD = ROOT / "oracle" / "_ref"
 
 
+@pytest.mark.parametrize("which,nrows", [("rtm", 33), ("fwd", 46)])
+def test_compat_layouts_match_the_reference_structs(which, nrows):
+    """The compat libraries read the reference's struct Source and struct MultiGPU through
+    their own restatement of the layouts; every named member sits at the reference's offset
+    and both structs have the reference's size (checker compiled from the reference's own
+    headers by oracle/Makefile)."""
+    exe = REF_ON_SWD / f"layout_{which}"
+    if not exe.exists():
+        pytest.skip("layout checker not built (reference sources absent)")
+    rows = [line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                    check=True).stdout.splitlines()]
+    assert len(rows) == nrows
+    bad = [r for r in rows if r[2] != r[3]]
+    assert not bad, bad
+
+
 @pytest.mark.gpu
 @pytest.mark.skipif(not (REF_ON_SWD / "AVSPRTM_on_swd").exists(), reason="reference hosts on libswd not built")
 def test_reference_host_programs_on_libswd():
