@@ -114,6 +114,32 @@ def test_decon_geometry(swd, orc):
         swd.decon_geometry(100, 100, (10, 11), (21, 21), (5, 5))   # even PSF window
 
 
+def test_decon_geometry_random_cases(swd, orc):
+    """Window lattices of random images and window sizes: wherever the engine accepts the
+    geometry, the oracle accepts it too and gives the same window count and transform size
+    (integer work: exact)."""
+    from hypothesis import given, settings, strategies as st
+
+    odd = lambda lo, hi: st.integers(lo // 2, hi // 2).map(lambda k: 2 * k + 1)
+    accepted = []
+
+    @settings(max_examples=300, derandomize=True, deadline=None)
+    @given(nx=st.integers(40, 1400), nz=st.integers(40, 1400), px=odd(5, 41), pz=odd(5, 41),
+           fx_extra=st.integers(0, 30), fz_extra=st.integers(0, 30), sx=st.integers(2, 15), sz=st.integers(2, 15))
+    def check(nx, nz, px, pz, fx_extra, fz_extra, sx, sz):
+        psf, flt, snap = (px, pz), (px + 2 * fx_extra, pz + 2 * fz_extra), (sx, sz)
+        try:
+            w, fx, fz = swd.decon_geometry(nx, nz, psf, flt, snap)
+        except swd.SwdError:
+            return                      # outside the engine's limits (e.g. transform > 512)
+        g = orc.decon_geometry(nx, nz, psf, flt, snap)
+        assert (w, fx, fz) == (g["totalnum"], g["FX"], g["FZ"])
+        accepted.append(w)
+
+    check()
+    assert len(accepted) > 100          # most draws are valid geometries
+
+
 def test_host_prep_equals_oracle(swd, orc):
     for Lc in range(1, 9):
         assert np.array_equal(swd.cal_xishu(Lc).view(np.uint32), orc.cal_xishu(Lc).view(np.uint32))
