@@ -165,6 +165,39 @@ def test_host_prep_equals_oracle(swd, orc):
         assert np.array_equal(ra, rb) and np.array_equal(za, zb)
 
 
+def test_host_prep_random_cases_equal_oracle(swd, orc):
+    """The host preparation on random grids, spacings, time steps and acquisitions: CPML
+    profiles, Ricker wavelets, kz tapers and well geometries equal the oracle's bit for bit."""
+    from hypothesis import given, settings, strategies as st
+
+    bits = lambda a: np.asarray(a, np.float32).view(np.uint32)
+
+    @settings(max_examples=120, derandomize=True, deadline=None)
+    @given(nx=st.integers(20, 900), nz=st.integers(20, 900), pml=st.integers(5, 40), Lc=st.integers(1, 8),
+           dx=st.sampled_from([2.0, 2.5, 4.0, 5.0, 10.0, 12.5]), dt=st.floats(2.0 ** -13, 2.0 ** -10, width=32),
+           nt=st.integers(16, 9000), f0=st.floats(5.0, 60.0, width=32),
+           shotdep=st.floats(0.0, 200.0, width=32), offsetz=st.floats(1.0, 6000.0, width=32))
+    def check(nx, nz, pml, Lc, dx, dt, nt, f0, shotdep, offsetz):
+        pmlc = pml + Lc
+        ntx, ntz = nx + 2 * pmlc, nz + 2 * pmlc
+        a, b = swd.get_absorbing_parameters(ntx, ntz, pmlc, dx, dx, dt), orc.cpml(ntx, ntz, pmlc, dx, dx, dt)
+        for k in a:
+            assert np.array_equal(bits(a[k]), bits(b[k])), k
+        assert np.array_equal(bits(swd.ricker_wave(nt, f0, dt)), bits(orc.ricker(nt, f0, dt)))
+        nf = swd.pow2(ntz)
+        assert nf == orc.pow2_len(ntz)
+        ta, la = swd.kz_taper(nf, dx)
+        tb, lb = orc.kz_taper(nf, dx)
+        assert la == lb
+        if la >= 0:
+            assert np.array_equal(bits(ta), bits(tb))
+        ra, za = swd.well_geometry(nx, nz, pmlc, dx, shotdep, offsetz)
+        rb, zb = orc.well_geometry(nx, nz, pmlc, dx, shotdep, offsetz)
+        assert np.array_equal(ra, rb) and np.array_equal(za, zb)
+
+    check()
+
+
 def test_synthetic_configs_are_seeded(swd):
     from swd_b200 import configs
     a, b = configs.c1(), configs.c1()
