@@ -64,6 +64,36 @@ def test_host_prep_bit_exact_vs_reference(orc):
         assert np.array_equal(s.view(np.uint32), Fw.smooth(vp, 12, w).view(np.uint32))
 
 
+def test_host_prep_random_cases_vs_reference(orc):
+    """The oracle's CPML profiles and Gaussian smoothing on random grids, spacings, time steps,
+    frames and windows equal the reference's own host functions (built from its sources) bit
+    for bit, beyond the fixed cases above."""
+    from hypothesis import given, settings, strategies as st
+    R, Fw = orc.RefHost("rtm"), orc.RefHost("fwd")
+
+    @settings(max_examples=60, derandomize=True, deadline=None)
+    @given(ntx=st.integers(40, 1200), ntz=st.integers(40, 1200), pmlc=st.integers(6, 48),
+           dx=st.sampled_from([2.0, 2.5, 4.0, 5.0, 10.0]), dz=st.sampled_from([2.0, 4.0, 5.0, 7.5]),
+           dt=st.floats(2.0 ** -13, 2.0 ** -10, width=32))
+    def cpml(ntx, ntz, pmlc, dx, dz, dt):
+        a, b = orc.cpml(ntx, ntz, pmlc, dx, dz, dt), R.cpml(ntx, ntz, pmlc, dx, dz, dt)
+        for k in a:
+            assert np.array_equal(a[k].view(np.uint32), b[k].view(np.uint32)), k
+
+    @settings(max_examples=20, derandomize=True, deadline=None)
+    @given(nx=st.integers(20, 90), nz=st.integers(20, 90), pmlc=st.integers(9, 20), w=st.integers(1, 6),
+           seed=st.integers(0, 2 ** 16))
+    def smooth(nx, nz, pmlc, w, seed):
+        v = np.random.default_rng(seed).uniform(1500, 4500, (nx, nz)).astype(np.float32)
+        vp = orc.pad_model(v, pmlc)
+        s = orc.smooth(vp, pmlc, w)
+        assert np.array_equal(s.view(np.uint32), R.smooth(vp, pmlc, w).view(np.uint32))
+        assert np.array_equal(s.view(np.uint32), Fw.smooth(vp, pmlc, w).view(np.uint32))
+
+    cpml()
+    smooth()
+
+
 def test_decon_oracle_matches_reference_golden(orc):
     """Oracle decon vs the reference decon2d_mine (built from its source) on the committed
     cases; both use the same FFT, so they agree bit for bit."""
