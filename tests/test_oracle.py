@@ -122,6 +122,39 @@ def test_decon_oracle_live_vs_reference_build(orc):
     assert np.array_equal(dec.view(np.uint32), ref_dec.view(np.uint32))
 
 
+@pytest.mark.skipif(not REF_DECON.exists(), reason="reference decon not built")
+def test_decon_oracle_random_cases_vs_reference_build(orc):
+    """The oracle's deconvolution on random image sizes, window sizes and damping equals the
+    reference's decon2d_mine (built from its source, same FFT shim) bit for bit."""
+    import importlib.util
+    from hypothesis import assume, given, settings, strategies as st
+    spec = importlib.util.spec_from_file_location("mkg", GOLDEN / "make_golden.py")
+    mkg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mkg)
+    odd = lambda lo, hi: st.integers(lo // 2, hi // 2).map(lambda k: 2 * k + 1)
+    done = []
+
+    @settings(max_examples=10, derandomize=True, deadline=None)
+    @given(nx=st.integers(60, 130), nz=st.integers(60, 130), px=odd(5, 13), pz=odd(5, 13),
+           kx=st.integers(2, 7), kz=st.integers(2, 7), sx=st.integers(3, 6), sz=st.integers(3, 6),
+           eps=st.sampled_from([1e-3, 2e-3, 5e-3]), seed=st.integers(0, 1000))
+    def check(nx, nz, px, pz, kx, kz, sx, sz, eps, seed):
+        psf, flt, snap = (px, pz), (px + 2 * kx, pz + 2 * kz), (sx, sz)
+        try:
+            orc.decon_geometry(nx, nz, psf, flt, snap)
+        except ValueError:
+            assume(False)
+        mig, p, vp = mkg.synthetic_decon_inputs(nx, nz, psf, seed)
+        ref_dec, ref_coef = mkg.run_ref_decon(nx, nz, mig, p, vp, psf, flt, snap, eps)
+        dec, coef = orc.decon(nx, nz, mig, p, psf, flt, snap, eps)
+        assert np.array_equal(coef, ref_coef)
+        assert np.array_equal(dec.view(np.uint32), ref_dec.view(np.uint32))
+        done.append(1)
+
+    check()
+    assert len(done) >= 5
+
+
 def _small_model(orc, nt=300, nx=60, nz=44, pml=8, Lc=4):
     rng = np.random.default_rng(5)
     v = np.full((nx, nz), 2000.0, np.float32)
