@@ -65,9 +65,9 @@ def test_host_prep_bit_exact_vs_reference(orc):
 
 
 def test_host_prep_random_cases_vs_reference(orc):
-    """The oracle's CPML profiles and Gaussian smoothing on random grids, spacings, time steps,
-    frames and windows equal the reference's own host functions (built from its sources) bit
-    for bit, beyond the fixed cases above."""
+    """The oracle's CPML profiles, Gaussian smoothing and Ricker wavelets on random grids,
+    spacings, time steps, frames, windows and frequencies equal the reference's own host
+    functions (built from its sources) bit for bit, beyond the fixed cases above."""
     from hypothesis import given, settings, strategies as st
     R, Fw = orc.RefHost("rtm"), orc.RefHost("fwd")
 
@@ -90,8 +90,15 @@ def test_host_prep_random_cases_vs_reference(orc):
         assert np.array_equal(s.view(np.uint32), R.smooth(vp, pmlc, w).view(np.uint32))
         assert np.array_equal(s.view(np.uint32), Fw.smooth(vp, pmlc, w).view(np.uint32))
 
+    @settings(max_examples=20, derandomize=True, deadline=None)
+    @given(nt=st.integers(16, 9000), f0=st.floats(5.0, 60.0, width=32), dt=st.floats(2.0 ** -13, 2.0 ** -10, width=32))
+    def ricker(nt, f0, dt):
+        with tempfile.TemporaryDirectory() as d:
+            assert np.array_equal(orc.ricker(nt, f0, dt).view(np.uint32), R.ricker(nt, f0, dt, d).view(np.uint32))
+
     cpml()
     smooth()
+    ricker()
 
 
 def test_decon_oracle_matches_reference_golden(orc):
