@@ -18,7 +18,12 @@ step, no collective in the data path): value = all ranks' shots / the slowest ra
 --impl reference times the CPU implementation of the same shot on the host cores: the
 reference has no CPU propagator, so this is the project's OpenMP restatement of the
 reference's stencil, imaging and preprocessing loops (oracle/, kind "port"), run for a
-bounded number of time steps per sample and extrapolated to the full record.
+bounded number of time steps per sample and extrapolated to the full record.  With
+--workload / --config it times that workload's CPU restatement instead, with the same
+metric and unit.  The cpu_baseline of our own lines is timed on rank 0 of a one-GPU run.
+
+--profile-kernels [--workload afor|lsrtm|batch] [--config c5] --nt N runs one short shot of
+the workload with kernels launched directly (no graphs), for ncu captures.
 
 --workload batch measures batched multi-shot RTM on the 96-shot walkaway survey (1201 x 601,
 nt ~ U[3000, 6000], 200-600 receivers, 20-35 Hz): a step is the whole survey migrated and
