@@ -114,6 +114,22 @@ def test_decon_geometry(swd, orc):
         swd.decon_geometry(100, 100, (10, 11), (21, 21), (5, 5))   # even PSF window
 
 
+def test_decon_layout_of_the_bench_cases(swd, orc):
+    """The benchmark's window lattice (configs.decon_layout, from which its byte and FLOP counts
+    come) equals the oracle's and the engine's for the three decon workloads."""
+    from swd_b200 import configs
+    expect = {"shipped": 2484, "c2": 1222, "c5": 1593}
+    for name, windows in expect.items():
+        case = configs.decon_case(name)
+        lay = configs.decon_layout(case)
+        g = orc.decon_geometry(case.nx, case.nz, case.psfwin, case.filterwin, case.snapwin)
+        assert lay["windows"] == g["totalnum"] == windows
+        assert (lay["fullx"], lay["fullz"]) == (g["fullwx"], g["fullwz"])
+        assert (lay["outwinx"], lay["outwinz"]) == (g["outwinx"], g["outwinz"])
+        assert (lay["nxp"], lay["nzp"]) == (g["nxp"], g["nzp"])
+        assert swd.decon_geometry(case.nx, case.nz, case.psfwin, case.filterwin, case.snapwin)[0] == windows
+
+
 def test_decon_geometry_random_cases(swd, orc):
     """Window lattices of random images and window sizes: wherever the engine accepts the
     geometry, the oracle accepts it too and gives the same window count and transform size
