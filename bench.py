@@ -72,6 +72,38 @@ def load_pkg():
     return mod
 
 
+def load_configs():
+    """The seeded workload definitions (configs.py).  Taken from the package when it is loaded;
+    otherwise configs.py is loaded on its own (it needs only numpy), so the reference arm runs
+    without mapping libswd."""
+    if "swd_b200" in sys.modules:
+        return sys.modules["swd_b200"].configs
+    if "swd_configs" not in sys.modules:
+        spec = importlib.util.spec_from_file_location("swd_configs", PKG / "configs.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["swd_configs"] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules["swd_configs"]
+
+
+def load_oracle():
+    """The CPU oracle (oracle/pyoracle.py), the checker and the CPU baseline; nothing of the
+    product path goes through it."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    return pyoracle
+
+
+def oracle_model(orc, w, vp_int, nsteps):
+    """An oracle model of workload w on the migration or true velocity vp_int (interior), set up
+    with the oracle's own restatement of the reference's host preparation (padding, CPML
+    profiles, stencil coefficients), so the CPU legs use nothing of libswd."""
+    vp = orc.pad_model(vp_int, w.pmlc)
+    rho = np.full_like(vp, 1000.0)
+    cp = orc.cpml(w.ntx, w.ntz, w.pmlc, w.dx, w.dz, w.dt)
+    return orc.Model(vp, rho, cp, orc.cal_xishu(w.Lc), w.pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt), vp
+
+
 def max_over_ranks(dist, values, device):
     """Element-wise max over ranks of per-rank device timings: the slowest rank sets the job
     time of a replica run.  dist is torch.distributed (or None for one process)."""
@@ -364,6 +396,11 @@ def run_ours(args, rank, world, dist):
     traffic = measured_traffic(dom, args.config, N)
     # the CPU sample: --cpu-steps steps on the 1601x801 grid, fewer on larger grids (same work)
     cpu = rank0_single(rank, world, lambda: cpu_baseline(w, samples=1, nsteps=rtm_cpu_steps(args, w)))
+    # the accuracy condition of the metric, once, after every timed region (one-GPU runs)
+    parity = None
+    if not args.no_parity:
+        pnt = args.parity_nt or (None if args.config == "c2" else 1500)
+        parity = rank0_single(rank, world, lambda: fp64_parity(swd, E, w, shot, rick, data, nt=pnt))
     return {
         "metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -387,7 +424,41 @@ def run_ours(args, rank, world, dist):
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "stored_source": stored,
+        "parity": parity,
     }
+
+
+PARITY_TOL = 1e-3   # the metric's accuracy condition: image rel-L2 against FP64
+
+
+def fp64_parity(swd, E, w, shot, rick, data, nt=None):
+    """The metric's accuracy condition, checked outside every timed region: one more RTM shot of
+    the benchmark (same engine, options and inputs; imaging without stacking) against the FP64
+    CPU oracle's restatement of the reference's method (strip reconstruction, imaging,
+    illumination normalisation and -vp^2 Laplacian, all in double) on the host cores.  Relative
+    L2 errors of the raw image I, the source illumination S and the filtered image.  nt < the
+    shot's record runs both on the first nt steps (stated in the result)."""
+    orc = load_oracle()
+    nt = shot.nt if nt is None else min(nt, shot.nt)
+    sh = swd.ShotSpec(shot.s_ix, shot.s_iz, shot.r_ix, shot.r_iz, nt)
+    rk = np.ascontiguousarray(rick[:nt])
+    dd = np.ascontiguousarray(data[:, :nt])
+    out = E.rtm_shot(sh, rk, dd, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK, want=("fimage",))
+    I, S, _ = E.rtm_raw()
+    t = time.perf_counter()
+    M, _ = oracle_model(orc, w, w.vp_mig, nt)
+    G = orc.Geom(sh.s_ix, sh.s_iz, sh.r_ix, sh.r_iz)
+    ref = orc.rtm_shot(M, G, rk, dd, dtype=np.float64)
+    _, fim = orc.rtm_post(M, ref["img"], ref["illum"], np.float64)
+    t = time.perf_counter() - t
+    rel = lambda a, b: float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+    res = {"reference": "FP64 CPU oracle (oracle/), the reference's reconstruction and imaging in double",
+           "nt": nt, "record": "full" if nt == shot.nt else f"first {nt} of {shot.nt} steps",
+           "receivers": len(sh.r_ix), "image_rel_l2": rel(I, ref["img"]), "illum_rel_l2": rel(S, ref["illum"]),
+           "fimage_rel_l2": rel(out["fimage"], fim), "tolerance": PARITY_TOL,
+           "oracle_s": round(t, 1), "oracle_threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))}
+    res["pass"] = max(res["image_rel_l2"], res["illum_rel_l2"], res["fimage_rel_l2"]) <= PARITY_TOL
+    return res
 
 
 def rank0_single(rank, world, sample):
@@ -405,18 +476,12 @@ def rtm_cpu_steps(args, w):
 def cpu_baseline(w, samples=1, nsteps=24):
     """OpenMP FP32 restatement of the reference loops (oracle/) on the host cores, for a
     bounded number of time steps of the same shot, extrapolated to nt."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle as orc
-    swd = sys.modules.get("swd_b200") or load_pkg()
-    pmlc = w.pmlc
-    vp = swd.pad_model(w.vp_mig, pmlc)
-    rho = np.full_like(vp, 1000.0)
-    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
-    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt)
+    orc = load_oracle()
+    M, _ = oracle_model(orc, w, w.vp_mig, nsteps)
     rx, rz = w.receivers_padded()
     sx, sz = w.source_padded()
     G = orc.Geom(sx, sz, rx, rz)
-    rick = swd.ricker_wave(nsteps, w.f0, w.dt)
+    rick = orc.ricker(nsteps, w.f0, w.dt)
     data = np.random.default_rng(0).standard_normal((len(rx), nsteps)).astype(np.float32)
     best = None
     for _ in range(samples):
@@ -426,7 +491,7 @@ def cpu_baseline(w, samples=1, nsteps=24):
         best = dt if best is None else min(best, dt)
     per_shot = best * w.nt / nsteps
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": 1.0 / per_shot, "unit": "shots/s", "cores": cores, "kind": "port",
+    return {"value": 1.0 / per_shot, "unit": "shots/s", "cores": cores, "kind": "port", "sample_s": best,
             "sample": f"{nsteps} of {w.nt} time steps (forward + backward) of the same shot on the full grid, "
                       f"extrapolated linearly; {best:.2f} s measured"}
 
@@ -439,23 +504,17 @@ def afor_cpu_baseline(w, nsteps):
     """The oracle's FP32 OpenMP forward with the Hilbert twin and the well-column record on the
     host cores for nsteps steps of the same shot, extrapolated to nt (the kz split is a per-shot
     post-process, not included)."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle as orc
-    swd = sys.modules.get("swd_b200") or load_pkg()
-    pmlc = w.pmlc
-    vp = swd.pad_model(w.vp, pmlc)
-    rho = np.full_like(vp, 1000.0)
-    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
-    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt)
+    orc = load_oracle()
+    M, _ = oracle_model(orc, w, w.vp, nsteps)
     rx, rz = w.receivers_padded()
     sx, sz = w.source_padded()
     G = orc.Geom(sx, sz, rx, rz)
-    rick = swd.ricker_wave(nsteps, w.f0, w.dt)
+    rick = orc.ricker(nsteps, w.f0, w.dt)
     t = time.perf_counter()
     orc.forward(M, G, rick, hrick=rick[::-1].copy(), col_ix=sorted(set(int(x) for x in rx)))
     dt = time.perf_counter() - t
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": 1.0 / (dt * w.nt / nsteps), "unit": "shots/s", "cores": cores, "kind": "port",
+    return {"value": 1.0 / (dt * w.nt / nsteps), "unit": "shots/s", "cores": cores, "kind": "port", "sample_s": dt,
             "sample": f"{nsteps} of {w.nt} time steps of the twin forward on the full grid, extrapolated linearly; "
                       f"{dt:.2f} s measured"}
 
@@ -855,8 +914,7 @@ def decon_flops(lay):
 
 def decon_cpu(case, mig, psf):
     """The oracle's restatement of the reference's window loop on all host cores."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle as orc
+    orc = load_oracle()
     cores = os.cpu_count() or 1
     t = time.perf_counter()
     dec, coef = orc.decon(case.nx, case.nz, mig, psf, case.psfwin, case.filterwin, case.snapwin, case.epsilon,
@@ -955,25 +1013,20 @@ def survey_cpu_baseline(w, nsteps):
     """The oracle's FP32 OpenMP RTM of the survey's first shot for nsteps steps on the full grid;
     its time per step, times the survey's total steps (every shot's nt), gives the survey's
     shots/s."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle as orc
-    swd = sys.modules.get("swd_b200") or load_pkg()
+    orc = load_oracle()
     pmlc = w.pmlc
-    vp = swd.pad_model(w.vp_mig, pmlc)
-    rho = np.full_like(vp, 1000.0)
-    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
-    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt)
+    M, _ = oracle_model(orc, w, w.vp_mig, nsteps)
     shots = w.extra["shots"]
     s = shots[0]
     G = orc.Geom(int(s["sx"]) + pmlc, int(s["sz"]) + pmlc, s["rec_x"] + pmlc, s["rec_z"] + pmlc)
-    rick = swd.ricker_wave(nsteps, s["f0"], w.dt)
+    rick = orc.ricker(nsteps, s["f0"], w.dt)
     data = np.random.default_rng(0).standard_normal((len(s["rec_x"]), nsteps)).astype(np.float32)
     t = time.perf_counter()
     orc.rtm_shot(M, G, rick, data)
     dt = time.perf_counter() - t
     total = dt / nsteps * sum(int(x["nt"]) for x in shots)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": len(shots) / total, "unit": "shots/s", "cores": cores, "kind": "port",
+    return {"value": len(shots) / total, "unit": "shots/s", "cores": cores, "kind": "port", "sample_s": dt,
             "sample": f"{nsteps} steps (forward + backward) of the survey's first shot on the full grid; the time "
                       f"per step times the survey's {sum(int(x['nt']) for x in shots)} steps; {dt:.2f} s measured"}
 
@@ -981,17 +1034,12 @@ def survey_cpu_baseline(w, nsteps):
 def lsrtm_cpu_baseline(w, nsteps=100):
     """The oracle's Born modelling + adjoint (FP32, OpenMP stencils, serial adjoint scatters)
     for one shot over nsteps steps on the full grid, extrapolated to nt."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle as orc
-    swd = sys.modules.get("swd_b200") or load_pkg()
+    orc = load_oracle()
     pmlc = w.pmlc
-    vp = swd.pad_model(w.vp_mig, pmlc)
-    rho = np.full_like(vp, 1000.0)
-    cp = swd.get_absorbing_parameters(w.ntx, w.ntz, pmlc, w.dx, w.dz, w.dt)
-    M = orc.Model(vp, rho, cp, swd.cal_xishu(w.Lc), pmlc, w.Lc, nsteps, w.dx, w.dz, w.dt)
+    M, vp = oracle_model(orc, w, w.vp_mig, nsteps)
     rx, rz = w.receivers_padded()
     G = orc.Geom(w.sx[0] + pmlc, pmlc, rx, rz)
-    rick = swd.ricker_wave(nsteps, w.f0, w.dt)
+    rick = orc.ricker(nsteps, w.f0, w.dt)
     dk = np.zeros_like(vp)
     dk[pmlc:-pmlc, pmlc:-pmlc] = 2 * 1000.0 * w.vp_mig ** 2 * w.extra["reflectivity"]
     t = time.perf_counter()
@@ -1000,7 +1048,7 @@ def lsrtm_cpu_baseline(w, nsteps=100):
     dt = time.perf_counter() - t
     per_shot = dt * w.nt / nsteps
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": 1.0 / per_shot, "unit": "shots/s", "cores": cores, "kind": "port",
+    return {"value": 1.0 / per_shot, "unit": "shots/s", "cores": cores, "kind": "port", "sample_s": dt,
             "sample": f"Born + adjoint of 1 shot, {nsteps} of {w.nt} steps on the full grid, extrapolated; "
                       f"{dt:.2f} s measured"}
 
@@ -1130,7 +1178,7 @@ def run_profile_batch(args):
 
 
 def run_reference_decon(args):
-    configs = sys.modules["swd_b200"].configs
+    configs = load_configs()
     case = configs.decon_case(args.config)
     lay = configs.decon_layout(case)
     mig, psf = configs.decon_inputs(case)
@@ -1146,6 +1194,7 @@ def run_reference_decon(args):
             "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 FFTs", "data": "synthetic", "impl": "reference",
             "config": {"workload": case.name, "parallelism": "host OpenMP"},
+            "step": f"the whole image ({lay['windows']} windows)",
             "cpu_baseline": {"value": value, "unit": "windows/s", "cores": cores, "kind": "port",
                              "sample": f"the whole image ({lay['windows']} windows) per step"},
             "e2e": {"value": value, "unit": "windows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -1154,11 +1203,13 @@ def run_reference_decon(args):
 
 def run_reference(args):
     """The reference arm: the oracle's restatement of the reference's loops on the host cores,
-    for the metric, unit and workload of our arm (--workload, --config); each step a bounded
-    sample of that workload."""
+    for the metric, unit and workload of our arm (--workload, --config).  Each step is one
+    bounded sample of that workload (a few hundred time steps of the shot on the full grid, the
+    oracle's own host preparation, nothing of libswd); `steps` and `ms_per_step` are those
+    samples as timed, and `value` is the shot rate they extrapolate to."""
     if args.workload == "decon":
         return run_reference_decon(args)
-    configs = sys.modules["swd_b200"].configs
+    configs = load_configs()
     if args.workload == "afor":
         w = configs.c2()
         metric, workload = "modelling shots/s", AFOR_WORKLOAD
@@ -1176,18 +1227,20 @@ def run_reference(args):
         metric, workload = "RTM shots/s", WORKLOADS[args.config]
         sample = lambda: cpu_baseline(w, samples=1, nsteps=rtm_cpu_steps(args, w))
     t0 = time.perf_counter()
-    vals = []
+    per_unit, sample_s = [], []
     for i in range(args.warmup + args.steps):
         cb = sample()
         if i >= args.warmup:
-            vals.append(1.0 / cb["value"])
-    mean = float(np.mean(vals))
-    value = 1.0 / mean
+            per_unit.append(1.0 / cb["value"])
+            sample_s.append(cb["sample_s"])
+    value = 1.0 / float(np.mean(per_unit))
     cb["value"] = value
     return {"metric": metric, "value": value, "unit": "shots/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "warmup": args.warmup, "ms_per_step": float(np.mean(sample_s)) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": workload, "parallelism": "host OpenMP"},
+            "step": "one bounded sample of the workload: " + cb["sample"].split(";")[0]
+                    + "; value extrapolates the samples to whole shots",
             "cpu_baseline": cb, "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": time.perf_counter() - t0}
 
@@ -1209,6 +1262,10 @@ def main():
     ap.add_argument("--config", choices=["c2", "c5", "shipped"], default="c2",
                     help="grid of --workload rtm (c2, c5) or decon (c2, c5, shipped: the reference's window geometry)")
     ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the image-error check against the FP64 oracle (a few minutes of host time)")
+    ap.add_argument("--parity-nt", type=int, default=0,
+                    help="record length of the FP64 check (0: the whole record on c2, 1500 steps on c5)")
     ap.add_argument("--tma", action="store_true", help="velocity kernels with TMA-staged pressure tiles (SWD_OPT_TMA)")
     ap.add_argument("--pdl", action="store_true", help="step kernels as programmatic dependent launches (SWD_OPT_PDL)")
     ap.add_argument("--streams", type=int, default=3,
@@ -1220,13 +1277,14 @@ def main():
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        # the CPU restatement only: the package (and with it libswd) is not loaded
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
     load_pkg()
     if args.profile_kernels:
         run_profile_kernels(args)
-        return
-    if args.impl == "reference":
-        if rank == 0:
-            print(json.dumps(run_reference(args)), flush=True)
         return
     dist = None
     if world > 1:

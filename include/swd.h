@@ -300,9 +300,12 @@ long long swd_launch_count(const swd_ctx *ctx);
  * `cuda_stream` (NULL = the default stream); results are ready when that stream reaches it.
  * Returns SWD_ERR_CAPACITY when windows*outwinx*outwinz + outwinx*outwinz exceeds the array
  * (or leaves no room for one CTA workspace when one is needed),
- * SWD_ERR_ARG for invalid geometry or non-device pointers.  The first call on each device
- * looks up the array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  Every call reuses the same array and leaves its contents behind; each
+ * SWD_ERR_ARG for invalid geometry or for pointers that are not device memory of the current
+ * device (host memory, or another GPU's memory, which the kernels could not dereference),
+ * SWD_ERR_CUDA for a failed launch or query.  Each call looks up the array's device address
+ * on the current device (cudaGetSymbolAddress, which allocates nothing); the first lookup on a
+ * device loads the library's kernels there, so make the first call on each device before any
+ * stream capture.  Every call reuses the same array and leaves its contents behind; each
  * call writes every scratch word it reads, so nothing needs clearing, but calls that overlap
  * on the GPU (other streams or host threads) race on the shared array. */
 #define SWD_ERR_CAPACITY 6

@@ -16,7 +16,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_DIR = HERE / "_ref"
-REFERENCE_SRC = Path(os.environ.get("SWD_REFERENCE", "/root/reference"))
+# the reference tree, for building oracle/_ref: the SWD_REFERENCE environment variable
+REFERENCE_SRC = Path(os.environ["SWD_REFERENCE"]) if os.environ.get("SWD_REFERENCE") else None
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -26,7 +27,7 @@ _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 def build(reference: bool = False) -> None:
     """Build liboracle.so (and, if asked and the reference sources exist, oracle/_ref)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    if reference and REFERENCE_SRC.exists():
+    if reference and REFERENCE_SRC is not None and REFERENCE_SRC.exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REFERENCE_SRC}"], check=True)
 
 

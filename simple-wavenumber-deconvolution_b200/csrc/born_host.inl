@@ -130,7 +130,7 @@ int swd_checkpoint_bytes(swd_ctx *ctx, int nt, size_t *bytes)
 static int check_ckpt(swd_ctx *ctx, const swd_shot *shot, const void *ckpt, size_t bytes)
 {
     if (!ckpt || ctx->ckpt_every == 0) return SWD_OK;
-    if (!is_device_ptr(ckpt)) return fail(ctx, SWD_ERR_ARG, "ckpt must be device memory");
+    if (!is_device_ptr_on(ckpt, ctx->dev)) return fail(ctx, SWD_ERR_ARG, "ckpt must be device memory of the context's GPU");
     if (!shot || shot->nt < 1) return fail(ctx, SWD_ERR_ARG, "shot is NULL or empty");
     const size_t need = ckpt_layout(ctx, shot->nt, nullptr, nullptr);
     if (bytes < need) return fail(ctx, SWD_ERR_ARG, "ckpt holds %zu bytes, %zu needed", bytes, need);

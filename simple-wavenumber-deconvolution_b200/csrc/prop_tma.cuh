@@ -93,16 +93,28 @@ __device__ __forceinline__ bool vtile_loop(const Geo &g, const CUtensorMap *cons
             const int t = blockIdx.x + s * gridDim.x;
             if (t < ntile) issue(t, s);
         }
+    // bounded wait for use k of a stage; true when it completed
+    auto wait_use = [&](int kk) {
+        long long tries = 0;
+        while (!mbar_try_wait(&bar[kk % T::STAGES], (kk / T::STAGES) & 1))
+            if (++tries > T::WAIT_TRIES) return false;
+        return true;
+    };
     int k = 0;
     for (int t = blockIdx.x; t < ntile; t += gridDim.x, k++) {
         const int s = k % T::STAGES;
-        const unsigned parity = (k / T::STAGES) & 1;
-        long long tries = 0;
-        while (!mbar_try_wait(&bar[s], parity)) {
-            if (++tries > T::WAIT_TRIES) {
+        // The decision to give up is the whole CTA's: every thread waits (bounded), then the
+        // block agrees.  On giving up no further tile is issued, and thread 0 waits (bounded
+        // again) for the copies still in flight into this CTA's stages before all threads return
+        // together, so the CTA does not exit under its own bulk copies.
+        if (__syncthreads_or(!wait_use(k))) {
+            if (tid == 0) {
                 atomicExch(err, 1);
-                return false;
+                for (int j = 0; j < T::STAGES; j++)
+                    if (t + j * gridDim.x < ntile) wait_use(k + j);
             }
+            __syncthreads();
+            return false;
         }
         body((t / ntz_t) * T::TX, (t % ntz_t) * T::TZ, vt_sm + (size_t)s * NBOX * T::SLOT);
         __syncthreads();   // every thread is done with stage s before it is refilled

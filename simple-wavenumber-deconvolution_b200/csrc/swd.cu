@@ -187,6 +187,20 @@ static bool is_device_ptr(const void *p)
     return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
+// Whether a kernel running on device dev may dereference p: managed memory, or device memory
+// allocated on dev.  Device memory of another GPU is not (it would need peer access); copies
+// (cudaMemcpyAsync) still reach it, so the copy paths use is_device_ptr.
+static bool is_device_ptr_on(const void *p, int dev)
+{
+    if (!p) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeManaged || (at.type == cudaMemoryTypeDevice && at.device == dev);
+}
+
 // copy n elements of host-or-device src into device buffer dst
 static int to_dev(swd_ctx *ctx, void *dst, const void *src, size_t bytes)
 {
@@ -1197,14 +1211,17 @@ static const void *decon_ws_kernel(const DeconGeo &g)
 {
     return g.staged ? (const void *)k_decon_window_ws<true> : (const void *)k_decon_window_ws<false>;
 }
+// CTAs of the persistent window kernel, or -1 when a CUDA query fails (the error is cleared).
 static int decon_ws_blocks(const DeconGeo &g, int dev)
 {
     int nsm = 0, occ = 0;
     const size_t sm = decon_ws_smem(g);
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    if (cudaFuncSetAttribute(decon_ws_kernel(g), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decon_ws_kernel(g), 512, sm) != cudaSuccess)
-        return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(decon_ws_kernel(g), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decon_ws_kernel(g), 512, sm) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
     return std::max(1, std::min(g.totalnum, nsm * std::max(occ, 1)));
 }
 
@@ -1997,8 +2014,10 @@ int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, 
             }
         // device arrays are read and written in place; host arrays go through the scratch
         const size_t np = (size_t)g.nx * g.nz, nout = coefr.size();
-        const bool din = is_device_ptr(migreal) && is_device_ptr(migpsf);
-        const bool dout = is_device_ptr(mig_dec) && is_device_ptr(mig_coef);
+        // the kernels read and write only memory of this device; anything else (host memory,
+        // another GPU's memory) goes through the context's scratch with copies
+        const bool din = is_device_ptr_on(migreal, ctx->dev) && is_device_ptr_on(migpsf, ctx->dev);
+        const bool dout = is_device_ptr_on(mig_dec, ctx->dev) && is_device_ptr_on(mig_coef, ctx->dev);
         DevBuf &bin = ctx->dcn[0], &bcoef = ctx->dcn[1], &bwin = ctx->dcn[2], &bout = ctx->dcn[3], &bws = ctx->dcn[4];
         const int nblk = decon_persistent(g) ? decon_ws_blocks(g, ctx->dev) : 0;
         if (decon_persistent(g) && nblk < 1) { rc = fail(ctx, SWD_ERR_CUDA, "decon: no launch shape for the window kernel"); break; }
@@ -2037,9 +2056,6 @@ int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, 
 int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const float *migpsf, float *mig_dec,
                       float *mig_coef, void *cuda_stream)
 {
-    // device address of the static scratch, looked up once per device with that device
-    // current; the lookup allocates nothing
-    static float *scratch_addr[64] = {nullptr};
     DeconGeo g;
     if (!p || decon_geo(p, g) != SWD_OK) return SWD_ERR_ARG;
     const size_t nout = (size_t)g.outwinx * g.outwinz;
@@ -2047,29 +2063,42 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
     // aligned offset; that kernel runs on as many CTAs as have a workspace that fits
     const size_t used = (size_t)g.totalnum * nout + nout, wsoff = (used + 63) & ~(size_t)63;
     if (used > SWD_DECON_STATIC_SCRATCH_FLOATS) return SWD_ERR_CAPACITY;
-    int nblk = 0;
+    // a launch error left over from the caller's own work is not this call's: clear it, so the
+    // checks below see only this call's launches
+    cudaGetLastError();
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return SWD_ERR_CUDA;
+    }
+    // the kernels dereference the four arrays on this device: memory of another GPU would be an
+    // illegal access without peer mappings, so it is refused here
     const void *ptrs[4] = {migreal, migpsf, mig_dec, mig_coef};
     for (const void *q : ptrs)
-        if (!is_device_ptr(q)) return SWD_ERR_ARG;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWD_ERR_CUDA;
-    if (!scratch_addr[dev]) {
-        void *a = nullptr;
-        if (cudaGetSymbolAddress(&a, g_decon_scratch) != cudaSuccess || !a) {
-            cudaGetLastError();
-            return SWD_ERR_CUDA;
-        }
-        scratch_addr[dev] = (float *)a;
+        if (!is_device_ptr_on(q, dev)) return SWD_ERR_ARG;
+    // Device address of the static scratch on this device.  It is looked up on every call (the
+    // lookup allocates nothing) rather than cached: a cache would have to be shared between host
+    // threads and would go stale if the caller reset the device, which reloads the module.  The
+    // first lookup on a device loads the module there, so the first call should come before any
+    // stream capture.
+    void *sa = nullptr;
+    if (cudaGetSymbolAddress(&sa, g_decon_scratch) != cudaSuccess || !sa) {
+        cudaGetLastError();
+        return SWD_ERR_CUDA;
     }
+    int nblk = 0;
     if (decon_persistent(g)) {
         const size_t per = decon_ws_floats(g);
         const size_t fit = wsoff < SWD_DECON_STATIC_SCRATCH_FLOATS ? (SWD_DECON_STATIC_SCRATCH_FLOATS - wsoff) / per : 0;
-        nblk = std::min<long long>(decon_ws_blocks(g, dev), (long long)fit);
+        const int occ = decon_ws_blocks(g, dev);
+        if (occ < 0) return SWD_ERR_CUDA;
+        nblk = (int)std::min<long long>(occ, (long long)fit);
         if (nblk < 1) return SWD_ERR_CAPACITY;
     }
-    float *coefr = scratch_addr[dev], *winout = coefr + nout;
+    float *coefr = (float *)sa, *winout = coefr + nout;
     cudaStream_t st = (cudaStream_t)cuda_stream;
     k_decon_taper<<<(int)((nout + 255) / 256), 256, 0, st>>>(coefr, g.outwinx, g.outwinz, p->snapwinx, p->snapwinz);
+    if (cudaGetLastError() != cudaSuccess) return SWD_ERR_CUDA;
     if (launch_decon_windows(g, migreal, migpsf, winout, coefr + wsoff, nblk, st) != cudaSuccess)
         return SWD_ERR_CUDA;
     k_decon_gather<<<592, 256, 0, st>>>(g, winout, coefr, mig_dec, mig_coef);

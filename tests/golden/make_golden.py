@@ -8,7 +8,7 @@
                    images, two window geometries (square and non-square)
 
 Run from the repository root in a container where the reference tree is mounted
-(SWD_REFERENCE, default /root/reference) after `make -C oracle ref`.
+(its location in the SWD_REFERENCE environment variable) after `make -C oracle ref`.
 """
 import os
 import subprocess
@@ -19,7 +19,7 @@ from pathlib import Path
 import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
-REF = Path(os.environ.get("SWD_REFERENCE", "/root/reference"))
+REF = Path(os.environ["SWD_REFERENCE"]) if os.environ.get("SWD_REFERENCE") else None
 OUT = Path(__file__).resolve().parent
 
 
@@ -75,6 +75,8 @@ DECON_CASES = [  # (nx, nz, psfwin, filterwin, snapwin, epsilon, seed)
 
 
 def main():
+    if REF is None:
+        raise SystemExit("set SWD_REFERENCE to the reference tree")
     # smoothing known-answer test: crops with a 5-cell halo
     acc = np.fromfile(REF / "input" / "acc_vp.bin", np.float32).reshape(845, 702)
     ini = np.fromfile(REF / "kkdecon_acoustic" / "input" / "ini_vp.bin", np.float32).reshape(845, 702)

@@ -2,7 +2,7 @@
 sm_100a by oracle/Makefile into oracle/_ref) on a small seeded model and saves their outputs
 as tests/golden/ref_gpu_small.npz.  Needs a GPU; run on the B200 box:
 
-    python tests/golden/make_golden_ref_gpu.py gpurun_out/ref_gpu_small.npz
+    python tests/golden/make_golden_ref_gpu.py <output dir>/ref_gpu_small.npz
 
 Geometry is chosen so the reference kernels stay inside their arrays: the padded width
 ntx = 100 + 2*14 = 128 is a multiple of 16 (the RTM kernels' block) and of 8 (AFor's), so
