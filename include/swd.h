@@ -118,6 +118,24 @@ int swd_set_kernel_path(swd_ctx *ctx, int path);
 int swd_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *hrick,
                 const float *kz_coef, float *seis, float *seis_up, float *seis_down);
 
+/* ---- scatter (PSF) data as an exact scattered field ------------------------------------
+ * Replaces the scatter mode's two forward runs and their difference
+ * (forward/acoustic_hilbert_fftkz_HLForC.cpp:620-795: background and perturbed records,
+ * scatter data = perturbed - background, :733-794).  The difference of two FP32 records of
+ * nearly equal size loses the digits the scatter points carry (about 1e-3 relative error of the
+ * difference for the reference's 1e-3 * vp density scatterers); here the difference field
+ * u(m1) - u(m) itself is propagated in FP32 beside the background field, in the perturbed model
+ * with the exact secondary sources (coefficient differences formed in double), so its error
+ * is relative to the scatter data, not to the record.
+ * swd_set_scatter_model: the perturbed model (padded ntx*ntz, like swd_set_model, which must
+ * come first; setting a new background clears it); NULL, NULL clears it.
+ * swd_forward_scatter: arguments as swd_forward; seis receives the scatter record and, with
+ * hrick and kz_coef, seis_up / seis_down its kz-separated traces (a second pass propagates the
+ * Hilbert wavelet's fields). */
+int swd_set_scatter_model(swd_ctx *ctx, const float *vp1, const float *rho1);
+int swd_forward_scatter(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *hrick,
+                        const float *kz_coef, float *seis, float *seis_up, float *seis_down);
+
 /* ---- RTM of one shot ---------------------------------------------------------------
  * Replaces the fdtd_2d_GPU_forward(inv_flag=1) + fdtd_2d_GPU_backward pair and the per-shot
  * host steps of AVSPRTM (acoustic_HLVSPRTMC.cpp:576-745; acoustic_HLVSPRTMLc.cu:239-432,
@@ -298,7 +316,8 @@ long long swd_launch_count(const swd_ctx *ctx);
  * allocates nothing: migreal/migpsf (nx*nz) and mig_dec/mig_coef (nx*nz) must be device
  * memory on the current device, already allocated by the caller.  Work is enqueued on
  * `cuda_stream` (NULL = the default stream); results are ready when that stream reaches it.
- * Returns SWD_ERR_CAPACITY when windows*outwinx*outwinz + outwinx*outwinz exceeds the array
+ * Returns SWD_ERR_CAPACITY when windows*outwinx*outwinz + outwinx*outwinz floats (plus the
+ * transform tables, a few thousand floats) exceed the array
  * (or leaves no room for one CTA workspace when one is needed),
  * SWD_ERR_ARG for invalid geometry or for pointers that are not device memory of the current
  * device (host memory, or another GPU's memory, which the kernels could not dereference),

@@ -90,6 +90,8 @@ def lib():
         L.swd_set_cig.argtypes = [vp, C.c_int, C.c_int]
         L.swd_rtm_cig.argtypes = [vp, vp]
         L.swd_forward.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, vp, vp]
+        L.swd_set_scatter_model.argtypes = [vp, vp, vp]
+        L.swd_forward_scatter.argtypes = [vp, C.POINTER(Shot), vp, vp, vp, vp, vp, vp]
         L.swd_rtm_shot.argtypes = [vp, C.POINTER(Shot), vp, vp, C.c_uint, vp, vp, vp, vp]
         L.swd_rtm_raw.argtypes = [vp, vp, vp, vp]
         L.swd_rtm_forward.argtypes = [vp, C.POINTER(Shot), vp, vp]
@@ -332,6 +334,31 @@ class Engine:
         kc = None if kz_coef is None else _f32(kz_coef)
         self._ck(lib().swd_forward(self._h, C.byref(sh), _ptr(rk), _ptr(hr), _ptr(kc), _ptr(seis), _ptr(up), _ptr(dn)))
         return (seis, up, dn) if twin else seis
+
+    def set_scatter_model(self, vp1, rho1):
+        """Perturbed model of forward_scatter (padded like set_model, which must come first);
+        None, None clears it."""
+        if vp1 is None and rho1 is None:
+            self._ck(lib().swd_set_scatter_model(self._h, None, None))
+            return
+        vp1, rho1 = _f32(vp1), _f32(rho1)
+        self._ck(lib().swd_set_scatter_model(self._h, _ptr(vp1), _ptr(rho1)))
+
+    def forward_scatter(self, shot: ShotSpec, rick, hrick=None, kz_coef=None):
+        """Scatter record u(perturbed) - u(background) at the receivers, propagated as an exact
+        scattered field; with hrick and kz_coef also its up/down traces: (seis, up, down)."""
+        sh, keep = self._shot(shot)
+        r_n, nt = sh.r_n, sh.nt
+        seis = np.zeros((r_n, nt), np.float32)
+        split = hrick is not None and kz_coef is not None
+        up = np.zeros((r_n, nt), np.float32) if split else None
+        dn = np.zeros((r_n, nt), np.float32) if split else None
+        rk = _f32(rick)
+        hr = None if hrick is None else _f32(hrick)
+        kc = None if kz_coef is None else _f32(kz_coef)
+        self._ck(lib().swd_forward_scatter(self._h, C.byref(sh), _ptr(rk), _ptr(hr), _ptr(kc), _ptr(seis), _ptr(up),
+                                           _ptr(dn)))
+        return (seis, up, dn) if split else seis
 
     def rtm_shot(self, shot: ShotSpec, rick, data, flags=RTM_PREPROCESS, want=("image_pp", "image_src", "fimage")):
         sh, keep = self._shot(shot)

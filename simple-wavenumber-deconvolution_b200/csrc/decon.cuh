@@ -27,12 +27,15 @@
 // The buffer index is ixx*FZ + izz and the 2D transform is taken over (n0 rows x n1
 // columns) of that linear buffer, which is how the reference plans it
 // (fftw_plan_dft_2d(fullwz, fullwx) on an x-major buffer, :490-493).  Transforms are FP32
-// DFTs over shared-memory twiddle tables (any length up to 512, prime 101 included).
+// FFTs, one warp per row or column (wfft.cuh): radix 2 for power-of-two lengths, Bluestein's
+// chirp-z through a power-of-two FFT for every other length up to 512 (the reference's 101 is
+// prime), with tables built in double by k_wfft_tables and copied into shared memory.
 // The L1 norms are accumulated serially in the reference's order with the reference's
 // float-through-double rounding, so the normalisation matches it exactly.
 #pragma once
 #include <cuda_runtime.h>
 #include "fft.cuh"
+#include "wfft.cuh"
 
 namespace swd {
 
@@ -80,47 +83,16 @@ __device__ __forceinline__ float img_at(const float *__restrict__ im, int nx, in
     return __ldg(im + (size_t)ix * nz + iz);
 }
 
-// Batched direct DFTs of length L over B transforms of the linear buffer s:
-// element j of transform t at s[t*str + j*sin].  sign -1 forward, +1 inverse; tw[m] =
-// exp(-2*pi*i*m/L).  Whole transforms are processed per round so the in-place
-// write-back never overwrites inputs still being read.
-__device__ void dft_pass(float2 *s, const float2 *tw, int L, int B, int sin, int str, int sign)
+__device__ void dft2(float2 *s, const WfftPlan &P0, const WfftPlan &P1, int n0, int n1, int sign)
 {
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const int per = nthr / L;   // transforms per round (L <= nthr)
-    for (int t0 = 0; t0 < B; t0 += per) {
-        const int t = t0 + tid / L, k = tid % L;
-        const bool act = (tid / L) < per && t < B;
-        float2 y = make_float2(0.f, 0.f);
-        if (act) {
-            const float2 *x = s + (size_t)t * str;
-            int m = 0;
-            for (int j = 0; j < L; j++) {
-                const float2 w = tw[m];
-                const float wi = sign < 0 ? w.y : -w.y;
-                const float2 v = x[(size_t)j * sin];
-                y.x = fmaf(v.x, w.x, fmaf(-v.y, wi, y.x));
-                y.y = fmaf(v.x, wi, fmaf(v.y, w.x, y.y));
-                m += k;
-                if (m >= L) m -= L;
-            }
-        }
-        __syncthreads();
-        if (act) s[(size_t)t * str + (size_t)k * sin] = y;
-        __syncthreads();
-    }
-}
-
-__device__ void dft2(float2 *s, const float2 *tw0, const float2 *tw1, int n0, int n1, int sign)
-{
-    dft_pass(s, tw1, n1, n0, 1, n1, sign);   // rows (length n1)
-    dft_pass(s, tw0, n0, n1, n1, 1, sign);   // columns (length n0)
+    fft_pass(s, P1, n0, 1, n1, sign);   // rows (length n1)
+    fft_pass(s, P0, n1, n1, 1, sign);   // columns (length n0)
 }
 
 // dft2 on a buffer Zg in global memory: row transforms (length n1, contiguous) and then column
 // transforms (length n0, stride n1) are copied cap elements at a time into the shared chunk,
-// transformed by dft_pass and written back.  cap >= max(n0, n1).
-__device__ void dft2_staged(float2 *Zg, float2 *chunk, int cap, const float2 *tw0, const float2 *tw1, int n0, int n1,
+// transformed by fft_pass and written back.  cap >= max(n0, n1).
+__device__ void dft2_staged(float2 *Zg, float2 *chunk, int cap, const WfftPlan &P0, const WfftPlan &P1, int n0, int n1,
                             int sign)
 {
     const int tid = threadIdx.x, nthr = blockDim.x;
@@ -130,7 +102,7 @@ __device__ void dft2_staged(float2 *Zg, float2 *chunk, int cap, const float2 *tw
         float2 *src = Zg + (size_t)r0 * n1;
         for (int j = tid; j < m; j += nthr) chunk[j] = src[j];
         __syncthreads();
-        dft_pass(chunk, tw1, n1, nr, 1, n1, sign);
+        fft_pass(chunk, P1, nr, 1, n1, sign);
         for (int j = tid; j < m; j += nthr) src[j] = chunk[j];
         __syncthreads();
     }
@@ -139,40 +111,44 @@ __device__ void dft2_staged(float2 *Zg, float2 *chunk, int cap, const float2 *tw
         const int nc = min(Cc, n1 - c0), m = n0 * nc;
         for (int j = tid; j < m; j += nthr) chunk[j] = Zg[(size_t)(j / nc) * n1 + c0 + j % nc];
         __syncthreads();
-        dft_pass(chunk, tw0, n0, nc, nc, 1, sign);
+        fft_pass(chunk, P0, nc, nc, 1, sign);
         for (int j = tid; j < m; j += nthr) Zg[(size_t)(j / nc) * n1 + c0 + j % nc] = chunk[j];
         __syncthreads();
     }
 }
 
-__device__ __forceinline__ void decon_twiddles(const DeconGeo &g, float2 *tw0, float2 *tw1)
+// Floats2 of transform tables of a window geometry: lengths n0 and n1 (one copy when equal).
+__host__ __device__ inline size_t decon_tab_len(const DeconGeo &g)
 {
-    for (int j = threadIdx.x; j < g.n0; j += blockDim.x) {
-        float s, c;
-        sincospi(-2.0f * (float)j / (float)g.n0, &s, &c);
-        tw0[j] = make_float2(c, s);
-    }
-    for (int j = threadIdx.x; j < g.n1; j += blockDim.x) {
-        float s, c;
-        sincospi(-2.0f * (float)j / (float)g.n1, &s, &c);
-        tw1[j] = make_float2(c, s);
-    }
+    return wfft_table_len(g.n0) + (g.n1 != g.n0 ? wfft_table_len(g.n1) : 0);
+}
+
+// Copies the transform tables (built by k_wfft_tables into tabs: length n0, then length n1
+// unless equal) into shared memory at sm and returns the two plans over that copy.
+__device__ __forceinline__ void decon_plans(const DeconGeo &g, const float2 *__restrict__ tabs, float2 *sm,
+                                            WfftPlan &P0, WfftPlan &P1)
+{
+    const int n = (int)decon_tab_len(g);
+    for (int j = threadIdx.x; j < n; j += blockDim.x) sm[j] = tabs[j];
+    P0 = wfft_plan(g.n0, sm);
+    P1 = g.n1 != g.n0 ? wfft_plan(g.n1, sm + wfft_table_len(g.n0)) : P0;
+    __syncthreads();
 }
 
 // One window w on the buffer Z (shared memory, or global memory when STAGED with the shared
 // chunk of cap elements); the twiddle tables are filled by the caller.
 template <bool STAGED>
-__device__ __forceinline__ void window_dft2(float2 *Z, float2 *chunk, int cap, const float2 *tw0, const float2 *tw1,
+__device__ __forceinline__ void window_dft2(float2 *Z, float2 *chunk, int cap, const WfftPlan &P0, const WfftPlan &P1,
                                             const DeconGeo &g, int sign)
 {
-    if (STAGED) dft2_staged(Z, chunk, cap, tw0, tw1, g.n0, g.n1, sign);
-    else dft2(Z, tw0, tw1, g.n0, g.n1, sign);
+    if (STAGED) dft2_staged(Z, chunk, cap, P0, P1, g.n0, g.n1, sign);
+    else dft2(Z, P0, P1, g.n0, g.n1, sign);
 }
 
 // FISTA refinement of the window solution held (unnormalised) in Z.x; leaves n*x in Z.x.
 template <bool STAGED>
-__device__ void decon_iterate(const DeconGeo &g, float2 *Z, const DeconIter &it, float fmax, const float2 *tw0,
-                              const float2 *tw1, float2 *chunk, int cap)
+__device__ void decon_iterate(const DeconGeo &g, float2 *Z, const DeconIter &it, float fmax, const WfftPlan &P0,
+                              const WfftPlan &P1, float2 *chunk, int cap)
 {
     __shared__ unsigned s_xmax;
     const int n = g.FX * g.FZ, tid = threadIdx.x, nthr = blockDim.x;
@@ -196,14 +172,14 @@ __device__ void decon_iterate(const DeconGeo &g, float2 *Z, const DeconIter &it,
         t = tn;
         for (int j = tid; j < n; j += nthr) Z[j] = make_float2(it.X[j] + beta * (it.X[j] - it.XP[j]), 0.f);
         __syncthreads();
-        window_dft2<STAGED>(Z, chunk, cap, tw0, tw1, g, -1);
+        window_dft2<STAGED>(Z, chunk, cap, P0, P1, g, -1);
         for (int j = tid; j < n; j += nthr) {
             const float2 y = Z[j], b = it.B[j];
             const float q = it.P[j] + mu;
             Z[j] = make_float2(q * y.x - b.x, q * y.y - b.y);
         }
         __syncthreads();
-        window_dft2<STAGED>(Z, chunk, cap, tw0, tw1, g, +1);
+        window_dft2<STAGED>(Z, chunk, cap, P0, P1, g, +1);
         for (int j = tid; j < n; j += nthr) {
             const float x = it.X[j], y = x + beta * (x - it.XP[j]);
             const float v = y - tau * (Z[j].x * invn);
@@ -216,9 +192,31 @@ __device__ void decon_iterate(const DeconGeo &g, float2 *Z, const DeconIter &it,
     __syncthreads();
 }
 
+// Sum of |Z[(ox + ixx)*FZ + oz + izz]| (component x, or y when Y) over ixx < nxw, izz < nzw,
+// in that order, into a float through double additions (the reference's accumulation).  The
+// chain of additions is serial; loads are issued eight at a time ahead of it.
+template <bool Y>
+__device__ float l1_serial(const float2 *Z, int FZ, int ox, int oz, int nxw, int nzw)
+{
+    float acc = 0.f;
+    for (int ixx = 0; ixx < nxw; ixx++) {
+        const float2 *row = Z + (size_t)(ox + ixx) * FZ + oz;
+        int izz = 0;
+        for (; izz + 8 <= nzw; izz += 8) {
+            float v[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) v[k] = Y ? row[izz + k].y : row[izz + k].x;
+#pragma unroll
+            for (int k = 0; k < 8; k++) acc = (float)((double)acc + fabs((double)v[k]));
+        }
+        for (; izz < nzw; izz++) acc = (float)((double)acc + fabs((double)(Y ? row[izz].y : row[izz].x)));
+    }
+    return acc;
+}
+
 template <bool STAGED>
 __device__ void decon_window(const DeconGeo &g, const float *__restrict__ mig, const float *__restrict__ psf,
-                             float *__restrict__ winout, int w, float2 *Z, const float2 *tw0, const float2 *tw1,
+                             float *__restrict__ winout, int w, float2 *Z, const WfftPlan &P0, const WfftPlan &P1,
                              float2 *chunk, int cap, const DeconIter &itr)
 {
     const int n = g.FX * g.FZ;
@@ -253,42 +251,44 @@ __device__ void decon_window(const DeconGeo &g, const float *__restrict__ mig, c
     };
 
     for (int j = tid; j < n; j += nthr) Z[j] = make_float2(0.f, 0.f);
-    // L1 norms in the reference's order and rounding (:554-576, :618-620): thread 0 sums
-    // the image patch, thread 32 the PSF, while the rest of the block fills the buffer
+    if (tid == 64) s_fmax = 0u;
+    __syncthreads();
+    // raw image patch (centred) and PSF patch (corner) into the buffer
+    for (int j = tid; j < g.filterwinx * g.filterwinz; j += nthr) {
+        const int ixx = j / g.filterwinz, izz = j % g.filterwinz;
+        const int iix = ix - g.halfltwx + ixx, iiz = iz - g.halfltwz + izz;
+        if (iix >= 0 && iix < g.nxp && iiz >= 0 && iiz < g.nzp)
+            Z[(g.midpx - g.halfltwx + ixx) * g.FZ + g.midpz - g.halfltwz + izz].x = img_at(mig, g.nx, g.nz, iix, iiz);
+    }
+    for (int j = tid; j < g.psfwinx * g.psfwinz; j += nthr) {
+        const int ixx = j / g.psfwinz, izz = j % g.psfwinz;
+        Z[ixx * g.FZ + izz].y = psf_val(ixx, izz);
+    }
+    __syncthreads();
+    // L1 norms in the reference's order and rounding (:554-576, :618-620), from the buffer:
+    // thread 0 sums the image patch, thread 32 the PSF (cells outside the expanded image are
+    // zero there and add nothing)
     if (tid == 0) {
-        float pp = 0.0f;
-        for (int ixx = 0; ixx < g.filterwinx; ixx++)
-            for (int izz = 0; izz < g.filterwinz; izz++) {
-                const int iix = ix - g.halfltwx + ixx, iiz = iz - g.halfltwz + izz;
-                if (iix >= 0 && iix < g.nxp && iiz >= 0 && iiz < g.nzp)
-                    pp = (float)((double)pp + fabs((double)img_at(mig, g.nx, g.nz, iix, iiz)));
-            }
+        float pp = l1_serial<false>(Z, g.FZ, g.midpx - g.halfltwx, g.midpz - g.halfltwz, g.filterwinx, g.filterwinz);
         if ((double)pp <= 1.0e-15) pp = 1.0e-10f;
         s_ppmax = pp;
     } else if (tid == 32) {
-        float ps = 0.0f;
-        for (int ixx = 0; ixx < g.psfwinx; ixx++)
-            for (int izz = 0; izz < g.psfwinz; izz++)
-                ps = (float)((double)ps + fabs((double)psf_val(ixx, izz)));
-        s_psfmax = ps;
+        s_psfmax = l1_serial<true>(Z, g.FZ, 0, 0, g.psfwinx, g.psfwinz);
     }
-    if (tid == 64) s_fmax = 0u;
     __syncthreads();
     const double ppm = (double)s_ppmax, psm = (double)s_psfmax;
     for (int j = tid; j < g.filterwinx * g.filterwinz; j += nthr) {
         const int ixx = j / g.filterwinz, izz = j % g.filterwinz;
-        const int iix = ix - g.halfltwx + ixx, iiz = iz - g.halfltwz + izz;
-        if (iix >= 0 && iix < g.nxp && iiz >= 0 && iiz < g.nzp) {
-            const int ip = (g.midpx - g.halfltwx + ixx) * g.FZ + g.midpz - g.halfltwz + izz;
-            Z[ip].x = (float)((double)img_at(mig, g.nx, g.nz, iix, iiz) / ppm);
-        }
+        float2 &z = Z[(g.midpx - g.halfltwx + ixx) * g.FZ + g.midpz - g.halfltwz + izz];
+        z.x = (float)((double)z.x / ppm);
     }
     for (int j = tid; j < g.psfwinx * g.psfwinz; j += nthr) {
         const int ixx = j / g.psfwinz, izz = j % g.psfwinz;
-        Z[ixx * g.FZ + izz].y = (float)((double)psf_val(ixx, izz) / psm);
+        float2 &z = Z[ixx * g.FZ + izz];
+        z.y = (float)((double)z.y / psm);
     }
     __syncthreads();
-    window_dft2<STAGED>(Z, chunk, cap, tw0, tw1, g, -1);
+    window_dft2<STAGED>(Z, chunk, cap, P0, P1, g, -1);
     // |S^|^2 maximum over all bins (float compare of the double square, :625-633)
     float fm = 0.f;
     for (int j = tid; j < n; j += nthr) {
@@ -327,9 +327,9 @@ __device__ void decon_window(const DeconGeo &g, const float *__restrict__ mig, c
         }
     }
     __syncthreads();
-    window_dft2<STAGED>(Z, chunk, cap, tw0, tw1, g, +1);
+    window_dft2<STAGED>(Z, chunk, cap, P0, P1, g, +1);
     if (g.iters > 0 && __uint_as_float(s_fmax) > 0.0f)
-        decon_iterate<STAGED>(g, Z, itr, __uint_as_float(s_fmax), tw0, tw1, chunk, cap);
+        decon_iterate<STAGED>(g, Z, itr, __uint_as_float(s_fmax), P0, P1, chunk, cap);
     const int nout = g.outwinx * g.outwinz;
     float *o = winout + (size_t)w * nout;
     for (int j = tid; j < nout; j += nthr) {
@@ -339,14 +339,16 @@ __device__ void decon_window(const DeconGeo &g, const float *__restrict__ mig, c
     }
 }
 
-// One CTA per window, the whole buffer and the twiddles in shared memory.
+// One CTA per window, the whole buffer and the transform tables in shared memory.
 __global__ void __launch_bounds__(512) k_decon_window(DeconGeo g, const float *__restrict__ mig,
-                                                      const float *__restrict__ psf, float *__restrict__ winout)
+                                                      const float *__restrict__ psf, float *__restrict__ winout,
+                                                      const float2 *__restrict__ tabs)
 {
     extern __shared__ float2 sm[];
-    float2 *Z = sm, *tw0 = Z + (size_t)g.FX * g.FZ, *tw1 = tw0 + g.n0;
-    decon_twiddles(g, tw0, tw1);
-    decon_window<false>(g, mig, psf, winout, blockIdx.x, Z, tw0, tw1, nullptr, 0, DeconIter{});
+    float2 *Z = sm;
+    WfftPlan P0, P1;
+    decon_plans(g, tabs, Z + (size_t)g.FX * g.FZ, P0, P1);
+    decon_window<false>(g, mig, psf, winout, blockIdx.x, Z, P0, P1, nullptr, 0, DeconIter{});
 }
 
 // Floats of global workspace one persistent CTA of k_decon_window_ws needs: the staged
@@ -364,22 +366,21 @@ __host__ __device__ inline size_t decon_ws_floats(const DeconGeo &g)
 template <bool STAGED>
 __global__ void __launch_bounds__(512) k_decon_window_ws(DeconGeo g, const float *__restrict__ mig,
                                                          const float *__restrict__ psf, float *__restrict__ winout,
-                                                         float *__restrict__ ws, int cap)
+                                                         float *__restrict__ ws, int cap, const float2 *__restrict__ tabs)
 {
     extern __shared__ float2 sm[];
     const size_t n = (size_t)g.FX * g.FZ;
     float *mine = ws + (size_t)blockIdx.x * decon_ws_floats(g);
-    float2 *Z, *tw0, *chunk = nullptr;
+    float2 *Z, *tsm, *chunk = nullptr;
     if (STAGED) {
         Z = (float2 *)mine;
         mine += 2 * n;
-        tw0 = sm;
-        chunk = sm + g.n0 + g.n1;
+        tsm = sm;
+        chunk = sm + decon_tab_len(g);
     } else {
         Z = sm;
-        tw0 = sm + n;
+        tsm = sm + n;
     }
-    float2 *tw1 = tw0 + g.n0;
     DeconIter itr{};
     if (g.iters > 0) {
         itr.B = (float2 *)mine;
@@ -387,9 +388,10 @@ __global__ void __launch_bounds__(512) k_decon_window_ws(DeconGeo g, const float
         itr.X = itr.P + n;
         itr.XP = itr.X + n;
     }
-    decon_twiddles(g, tw0, tw1);
+    WfftPlan P0, P1;
+    decon_plans(g, tabs, tsm, P0, P1);
     for (int w = blockIdx.x; w < g.totalnum; w += gridDim.x) {
-        decon_window<STAGED>(g, mig, psf, winout, w, Z, tw0, tw1, chunk, cap, itr);
+        decon_window<STAGED>(g, mig, psf, winout, w, Z, P0, P1, chunk, cap, itr);
         __syncthreads();   // the next window's fill overwrites Z and the shared scalars
     }
 }

@@ -12,7 +12,12 @@
 //     (rho += 1e-3*vp, :697-705); `swd.perturb = velocity` in parameter.txt multiplies vp by
 //     (1 + swd.perturb_amp, default 0.01) instead.
 // Extensions (parameter.txt lines `swd.key = value`): device, perturb (density|velocity; an
-// unknown value is an error), perturb_amp.
+// unknown value is an error), perturb_amp, scatter_field (difference|exact): `difference`, the
+// default, forms the scatter records as the reference does, perturbed run minus background run;
+// `exact` propagates the difference field itself (swd_forward_scatter), whose FP32 error is
+// relative to the scatter data instead of to the records.
+// Per-shot receivers: ../input/%dsource_receivers.txt, when present, gives that shot its own
+// receiver list (count, then "ix iz" interior cells); its records then hold that many traces.
 #include <math.h>
 #include "common.h"
 
@@ -28,8 +33,10 @@ int main(int, char **)
     }
     auto ext = extensions((up + "/parameter.txt").c_str());
     const int device = ext_int(ext, "device", 0);
-    std::string perturb;
-    if (!ext_choice(ext, "perturb", {"density", "velocity"}, perturb)) return 1;
+    std::string perturb, sfield;
+    if (!ext_choice(ext, "perturb", {"density", "velocity"}, perturb) ||
+        !ext_choice(ext, "scatter_field", {"difference", "exact"}, sfield))
+        return 1;
     const float perturb_amp = (float)atof(ext_str(ext, "perturb_amp", "0.01").c_str());
     printf("Number of MPI thread is 1\n");
     printf("The simulation time step is %d\n", m.itmax);
@@ -39,15 +46,15 @@ int main(int, char **)
     const size_t ntp = (size_t)ntz * ntx;
     Operator op = make_operator(m, ntx, ntz, pmlc);
 
-    // shots and the two edge wells (forward/...HLForC.cpp:144-191)
-    const int r_n = swd_prep_wells(m.nx, m.nz, pmlc, m.dz, m.shotdep, m.offsetz, nullptr, nullptr);
-    std::vector<int> r_ix(r_n), r_iz(r_n);
-    swd_prep_wells(m.nx, m.nz, pmlc, m.dz, m.shotdep, m.offsetz, r_ix.data(), r_iz.data());
-    printf("The maximum trace number for source is %d\n", r_n);
-    if (r_n < 2) {
-        printf("No receiver depth lies within the maximum offset\n");
-        return 1;
+    // shots and their receivers: the two edge wells (forward/...HLForC.cpp:144-191) or the
+    // shot's own list; every file is checked before any device work
+    std::vector<Receivers> recv(m.ns);
+    int rnmax = 0;
+    for (int is = 0; is < m.ns; is++) {
+        if (!shot_receivers(up, is, m, recv[is])) return 1;
+        rnmax = (int)recv[is].ix.size() > rnmax ? (int)recv[is].ix.size() : rnmax;
     }
+    printf("The maximum trace number for source is %d\n", rnmax);
 
     // kz taper (forward/...HLForC.cpp:354-377)
     const int nfftz = swd_prep_pow2(ntz);
@@ -93,22 +100,30 @@ int main(int, char **)
                              op.bxh.data(), op.bz.data(), op.bzh.data()), "swd_set_cpml");
     printf("ABC parameters are done\n");
 
-    const size_t ntr = (size_t)r_n * m.itmax;
-    std::vector<float> obs(ntr), obsup(ntr), obsdown(ntr);
+    std::vector<float> obs, obsup, obsdown;
     auto shot_of = [&](int is) {
         swd_shot s;
         s.s_ix = pmlc + (int)(m.sx0 / m.dx) + (int)(m.shotdx / m.dx) * is;
         s.s_iz = pmlc + (int)(m.shotdep / m.dz);
         s.nt = m.itmax;
-        s.r_n = r_n;
-        s.r_ix = r_ix.data();
-        s.r_iz = r_iz.data();
+        s.r_n = (int)recv[is].ix.size();
+        s.r_ix = recv[is].ix.data();
+        s.r_iz = recv[is].iz.data();
         return s;
     };
-    auto run = [&](int is, std::vector<float> &a, std::vector<float> &b, std::vector<float> &c) {
+    // records of shot is, sized for its receivers
+    auto run = [&](int is, std::vector<float> &a, std::vector<float> &b, std::vector<float> &c, bool scat = false) {
         swd_shot s = shot_of(is);
-        die_on(ctx, swd_forward(ctx, &s, rick.data(), hrick.data(), coef.data(), a.data(), b.data(), c.data()),
-               "swd_forward");
+        const size_t n = (size_t)s.r_n * m.itmax;
+        a.resize(n);
+        b.resize(n);
+        c.resize(n);
+        if (scat)
+            die_on(ctx, swd_forward_scatter(ctx, &s, rick.data(), hrick.data(), coef.data(), a.data(), b.data(), c.data()),
+                   "swd_forward_scatter");
+        else
+            die_on(ctx, swd_forward(ctx, &s, rick.data(), hrick.data(), coef.data(), a.data(), b.data(), c.data()),
+                   "swd_forward");
     };
     auto shotfile = [&](int is, const char *kind) {
         char name[64];
@@ -122,9 +137,9 @@ int main(int, char **)
         die_on(ctx, swd_set_model(ctx, vp.data(), rho.data()), "swd_set_model");
         for (int is = 0; is < m.ns; is++) {
             run(is, obs, obsup, obsdown);
-            write_f32(shotfile(is, "obs"), obs.data(), ntr);
-            write_f32(shotfile(is, "obsup"), obsup.data(), ntr);
-            write_f32(shotfile(is, "obsdown"), obsdown.data(), ntr);
+            write_f32(shotfile(is, "obs"), obs.data(), obs.size());
+            write_f32(shotfile(is, "obsup"), obsup.data(), obsup.size());
+            write_f32(shotfile(is, "obsdown"), obsdown.data(), obsdown.size());
         }
     } else {
         printf("    The Scatter Flag == %d--- PSF\n====================\n", m.scatter_flag);
@@ -135,9 +150,9 @@ int main(int, char **)
         std::vector<std::vector<float>> bg(3 * (size_t)m.ns);
         for (int is = 0; is < m.ns; is++) {
             run(is, obs, obsup, obsdown);
-            write_f32(shotfile(is, "sobs"), obs.data(), ntr);
-            write_f32(shotfile(is, "sobsup"), obsup.data(), ntr);
-            write_f32(shotfile(is, "sobsdown"), obsdown.data(), ntr);
+            write_f32(shotfile(is, "sobs"), obs.data(), obs.size());
+            write_f32(shotfile(is, "sobsup"), obsup.data(), obsup.size());
+            write_f32(shotfile(is, "sobsdown"), obsdown.data(), obsdown.size());
             bg[3 * is] = obs;
             bg[3 * is + 1] = obsup;
             bg[3 * is + 2] = obsdown;
@@ -154,17 +169,21 @@ int main(int, char **)
         write_f32(up + "/output/ini_scatter_vp.bin", interior(vps, ntx, ntz, pmlc).data(), (size_t)m.nx * m.nz);
         write_f32(up + "/output/rho_scatter.bin", interior(rhos, ntx, ntz, pmlc).data(), (size_t)m.nx * m.nz);
         printf("Obtain the observed scatter seismogram !\n");
-        die_on(ctx, swd_set_model(ctx, vps.data(), rhos.data()), "swd_set_model");
+        const bool exact = sfield == "exact";
+        // exact: the background stays and the perturbed model drives the scattered field
+        if (exact) die_on(ctx, swd_set_scatter_model(ctx, vps.data(), rhos.data()), "swd_set_scatter_model");
+        else die_on(ctx, swd_set_model(ctx, vps.data(), rhos.data()), "swd_set_model");
         for (int is = 0; is < m.ns; is++) {
-            run(is, obs, obsup, obsdown);
-            for (size_t ip = 0; ip < ntr; ip++) {
-                obs[ip] -= bg[3 * is][ip];
-                obsup[ip] -= bg[3 * is + 1][ip];
-                obsdown[ip] -= bg[3 * is + 2][ip];
-            }
-            write_f32(shotfile(is, "scatter"), obs.data(), ntr);
-            write_f32(shotfile(is, "scatterup"), obsup.data(), ntr);
-            write_f32(shotfile(is, "scatterdown"), obsdown.data(), ntr);
+            run(is, obs, obsup, obsdown, exact);
+            if (!exact)
+                for (size_t ip = 0; ip < obs.size(); ip++) {
+                    obs[ip] -= bg[3 * is][ip];
+                    obsup[ip] -= bg[3 * is + 1][ip];
+                    obsdown[ip] -= bg[3 * is + 2][ip];
+                }
+            write_f32(shotfile(is, "scatter"), obs.data(), obs.size());
+            write_f32(shotfile(is, "scatterup"), obsup.data(), obsup.size());
+            write_f32(shotfile(is, "scatterdown"), obsdown.data(), obsdown.size());
         }
     }
     printf("====================\n      THE END\n====================\n");

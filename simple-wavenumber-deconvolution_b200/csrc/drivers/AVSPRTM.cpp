@@ -13,6 +13,10 @@
 // Extensions (parameter.txt lines `swd.key = value`): device, strip_precision
 // (f32|f16|bf16|i16), data (up|full|down: which AFor record to migrate; the reference always
 // uses up).  An unknown value of either is an error.
+// Per-shot receivers: ./input/%dsource_receivers.txt, when present, gives that shot its own
+// receiver list (count, then "ix iz" interior cells; AFor reads the same file); every record
+// must hold exactly r_n x itmax floats of its shot.  All shots' geometry and record files are
+// checked before any device work.
 #include <math.h>
 #include "common.h"
 
@@ -38,14 +42,22 @@ int main(int, char **)
     const int ntz = m.nz + 2 * pmlc, ntx = m.nx + 2 * pmlc;
     const size_t ntp = (size_t)ntz * ntx, np = (size_t)m.nx * m.nz;
     Operator op = make_operator(m, ntx, ntz, pmlc);
-    const int r_n = swd_prep_wells(m.nx, m.nz, pmlc, m.dz, m.shotdep, m.offsetz, nullptr, nullptr);
-    std::vector<int> r_ix(r_n), r_iz(r_n);
-    swd_prep_wells(m.nx, m.nz, pmlc, m.dz, m.shotdep, m.offsetz, r_ix.data(), r_iz.data());
-    printf("The maximum trace number for source is %d\n", r_n);
-    if (r_n < 2) {
-        printf("No receiver depth lies within the maximum offset\n");
-        return 1;
+    // every shot's receivers and record, checked before any device work
+    const char *suffix = which == "full" ? "" : (which == "down" ? "down" : "up");
+    std::vector<Receivers> recv(m.ns);
+    std::vector<std::string> files(m.ns);
+    int rnmax = 0;
+    for (int is = 0; is < m.ns; is++) {
+        if (!shot_receivers(".", is, m, recv[is])) return 1;
+        const int r_n = (int)recv[is].ix.size();
+        rnmax = r_n > rnmax ? r_n : rnmax;
+        char name[128];
+        snprintf(name, sizeof name, "./output/%dsource_seismogram_%s%s.bin", is + 1, m.scatter_flag ? "scatter" : "obs",
+                 suffix);
+        files[is] = name;
+        if (!check_record(files[is], r_n, m.itmax)) return 1;
     }
+    printf("The maximum trace number for source is %d\n", rnmax);
 
     swd_ctx *ctx = make_context(m, device);
     if (sp == "f16") die_on(ctx, swd_set_strip_precision(ctx, SWD_STRIP_F16), "strip precision");
@@ -79,23 +91,24 @@ int main(int, char **)
     printf("ABC parameters are done\n");
     printf("====================\n%s\n====================\n", m.scatter_flag ? " PSF RTM BEGIN" : " NORMAL RTM BEGIN");
 
-    const size_t ntr = (size_t)r_n * m.itmax;
-    std::vector<float> data(ntr), syn(ntr), rms(ntr), img(np), src(np), fim(np);
+    std::vector<float> data, syn, rms, img(np), src(np), fim(np);
     const char *tag = m.scatter_flag ? "psf" : "pp";
-    const char *suffix = which == "full" ? "" : (which == "down" ? "down" : "up");
     die_on(ctx, swd_stack_reset(ctx), "swd_stack_reset");
     for (int is = 0; is < m.ns; is++) {
         char name[128];
-        snprintf(name, sizeof name, "./output/%dsource_seismogram_%s%s.bin", is + 1, m.scatter_flag ? "scatter" : "obs",
-                 suffix);
-        if (!read_f32(name, data.data(), ntr)) return 1;
+        const int r_n = (int)recv[is].ix.size();
+        const size_t ntr = (size_t)r_n * m.itmax;
+        data.resize(ntr);
+        syn.resize(ntr);
+        rms.resize(ntr);
+        if (!read_f32(files[is], data.data(), ntr)) return 1;
         swd_shot s;
         s.s_ix = pmlc + (int)(m.sx0 / m.dx) + (int)(m.shotdx / m.dx) * is;
         s.s_iz = pmlc + (int)(m.shotdep / m.dz);
         s.nt = m.itmax;
         s.r_n = r_n;
-        s.r_ix = r_ix.data();
-        s.r_iz = r_iz.data();
+        s.r_ix = recv[is].ix.data();
+        s.r_iz = recv[is].iz.data();
         die_on(ctx, swd_rtm_shot(ctx, &s, rick.data(), data.data(), SWD_RTM_PREPROCESS, syn.data(), img.data(),
                                  src.data(), fim.data()), "swd_rtm_shot");
         if (is % 20 == 0) {

@@ -159,6 +159,89 @@ inline bool read_model_params(const char *path, ModelParams &m)
     return r.ok;
 }
 
+// Size of a file in bytes, or -1 when it cannot be opened.
+inline long long file_bytes(const std::string &path)
+{
+    FILE *fp = fopen(path.c_str(), "rb");
+    if (!fp) return -1;
+    fseek(fp, 0, SEEK_END);
+    const long long n = ftell(fp);
+    fclose(fp);
+    return n;
+}
+
+// A seismogram record [r_n][itmax] (trace-major float32, the layout AFor writes): the file must
+// hold exactly r_n * itmax floats.  The reference freads r_n*itmax floats without looking
+// (acoustic_HLVSPRTMC.cpp:598-604), so a record of another receiver count or length would be
+// migrated silently as garbage; here the mismatch is reported with both shapes.
+inline bool check_record(const std::string &path, int r_n, int itmax)
+{
+    const long long n = file_bytes(path);
+    if (n < 0) {
+        printf("Cannot Open the File: %s\n", path.c_str());
+        return false;
+    }
+    const long long want = (long long)r_n * itmax * (long long)sizeof(float);
+    if (n != want) {
+        printf("The file %s holds %lld floats; r_n x itmax = %d x %d = %lld expected\n", path.c_str(),
+               n / (long long)sizeof(float), r_n, itmax, want / (long long)sizeof(float));
+        return false;
+    }
+    return true;
+}
+
+// Receivers of shot `is` (0-based).  The optional file <root>/input/<is+1>source_receivers.txt
+// gives the shot its own receiver list: the count r_n, then r_n lines "ix iz" of interior cell
+// indices (0 <= ix < nx, 0 <= iz < nz).  Without it the shot has the reference's two edge wells
+// (acoustic_HLVSPRTMC.cpp:153-200), the same for every shot.  Returns false, with a message,
+// for a malformed file.
+struct Receivers {
+    std::vector<int> ix, iz;   // padded-grid cells
+    bool from_file = false;
+};
+
+inline bool shot_receivers(const std::string &root, int is, const ModelParams &m, Receivers &R)
+{
+    const int pmlc = m.pml + m.Lc;
+    char name[256];
+    snprintf(name, sizeof name, "%s/input/%dsource_receivers.txt", root.c_str(), is + 1);
+    FILE *fp = fopen(name, "r");
+    R.ix.clear();
+    R.iz.clear();
+    R.from_file = fp != nullptr;
+    if (!fp) {
+        const int r_n = swd_prep_wells(m.nx, m.nz, pmlc, m.dz, m.shotdep, m.offsetz, nullptr, nullptr);
+        if (r_n < 2) {
+            printf("No receiver depth lies within the maximum offset\n");
+            return false;
+        }
+        R.ix.resize(r_n);
+        R.iz.resize(r_n);
+        swd_prep_wells(m.nx, m.nz, pmlc, m.dz, m.shotdep, m.offsetz, R.ix.data(), R.iz.data());
+        return true;
+    }
+    int r_n = 0;
+    bool ok = fscanf(fp, "%d", &r_n) == 1 && r_n >= 1;
+    for (int k = 0; ok && k < r_n; k++) {
+        int x, z;
+        if (fscanf(fp, "%d %d", &x, &z) != 2) {
+            printf("%s: %d receivers announced, %d read\n", name, r_n, k);
+            ok = false;
+            break;
+        }
+        if (x < 0 || x >= m.nx || z < 0 || z >= m.nz) {
+            printf("%s: receiver %d at (%d, %d) lies outside the %d x %d model\n", name, k, x, z, m.nx, m.nz);
+            ok = false;
+            break;
+        }
+        R.ix.push_back(pmlc + x);
+        R.iz.push_back(pmlc + z);
+    }
+    if (!ok && R.ix.empty() && r_n < 1) printf("%s: no receiver count\n", name);
+    fclose(fp);
+    return ok;
+}
+
 // Stencil coefficients, CPML profiles and stability print shared by AFor and AVSPRTM
 // (acoustic_HLVSPRTMC.cpp:106-118, 462-469).
 struct Operator {

@@ -54,7 +54,7 @@ struct DpStore {
 };
 
 // forward pressure-kernel modes
-constexpr int FP_PLAIN = 0, FP_BORN = 1, FP_STORE = 2;
+constexpr int FP_PLAIN = 0, FP_BORN = 1, FP_STORE = 2, FP_SCAT = 3;
 
 // One wavefield updated in place.
 struct Wave {
@@ -233,11 +233,19 @@ struct PTile {
 };
 
 // velocity half step (reference kernels _vx/_vz, acoustic_HLVSPRTMLc.cu:24-118; receiver
-// variants with the wider guards and -dx/-dz, :623-715), the pressure read through pl
-template <int LC, bool WIDE, class PL>
+// variants with the wider guards and -dx/-dz, :623-715), the pressure read through pl.
+// Scattered-field hooks (SC): 1 also returns the update sums d + phi of the four cells in
+// (*sx, *sz) (zero where a velocity is not updated); 2 adds dcb * (*sx, *sz) to the update, the
+// secondary source of an exact scattered field (coefficient difference dcbx, dcbz).
+template <int LC, bool WIDE, class PL, int SC = 0>
 __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
-                                            int x, int z0, const PL &pl)
+                                            int x, int z0, const PL &pl, float4 *sx = nullptr, float4 *sz = nullptr,
+                                            const float *dcbx = nullptr, const float *dcbz = nullptr)
 {
+    if constexpr (SC == 1) {
+        *sx = make_float4(0.f, 0.f, 0.f, 0.f);
+        *sz = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
     const Taps<LC> tx(g, odx), tz(g, odz);
@@ -277,6 +285,17 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
 #pragma unroll
             for (int k = 0; k < 4; k++)
                 if (gx[k]) el(v, k) = elc(cb, k) * (elc(d, k) + elc(phi, k)) + elc(v, k);
+            if constexpr (SC == 1) {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (gx[k]) el(*sx, k) = elc(d, k) + elc(phi, k);
+            }
+            if constexpr (SC == 2) {
+                const float4 db = ldg4(dcbx + ip);
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (gx[k]) el(v, k) = fmaf(elc(db, k), elc(*sx, k), elc(v, k));
+            }
             st4(w.vx + ip, v);
         }
     }
@@ -317,6 +336,17 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
 #pragma unroll
             for (int k = 0; k < 4; k++)
                 if (gz[k]) el(v, k) = elc(cb, k) * (elc(d, k) + elc(phi, k)) + elc(v, k);
+            if constexpr (SC == 1) {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (gz[k]) el(*sz, k) = elc(d, k) + elc(phi, k);
+            }
+            if constexpr (SC == 2) {
+                const float4 db = ldg4(dcbz + ip);
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (gz[k]) el(v, k) = fmaf(elc(db, k), elc(*sz, k), elc(v, k));
+            }
             st4(w.vz + ip, v);
         }
     }
@@ -484,6 +514,15 @@ struct FwdArgs {
     Ckpt ck;             // field-0 state checkpoints, taken by the CKPT instantiation of k_fwd_v
     Batch bt;            // the BATCH instantiations (NW == 1): shot = blockIdx.z
     DpStore ds;          // the FP_STORE instantiation (NW == 1): dp/dt of each step
+    // Exact scattered field (the SCAT instantiations, NW == 2): field 0 propagates in the
+    // background model (m), field 1 is the difference u(m1) - u(m) of the perturbed and the
+    // background wavefields, propagated in the perturbed model m1 with the secondary sources
+    // dcb * (d + phi) of field 0 in the velocity updates and dck * S0 in the pressure update
+    // (dcb, dck: coefficient differences m1 - m, formed in double).  The receivers record field
+    // 1; colcomp >= 0 writes field 1's column into that component of colbuf only.
+    Mat m1;
+    const float *dcbx, *dcbz, *dck;
+    int colcomp;
 };
 
 // The shot's view of a batched forward launch; false when the shot's record has ended.
@@ -581,7 +620,7 @@ __device__ __forceinline__ void cell4(int &x, int &z0)
     x = blockIdx.y * 8 + threadIdx.y;
 }
 
-template <int LC, int NW, bool CKPT, bool BATCH = false>
+template <int LC, int NW, bool CKPT, bool BATCH = false, bool SCAT = false>
 __global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
 {
     pdl_begin();
@@ -597,8 +636,17 @@ __global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
             ckpt_save(a.ck, a.w[0], it / a.ck.every, x < a.g.ntx && z0 < a.g.ntz, (size_t)x * a.g.ldz + z0);
     }
     if (x >= a.g.ntx || z0 >= a.g.ntz) return;
+    if constexpr (SCAT) {
+        static_assert(NW == 2, "the scattered field runs beside its background");
+        float4 sx, sz;
+        const PGlobal p0{a.w[0].p, a.g.ldz}, p1{a.w[1].p, a.g.ldz};
+        v_update4_l<LC, false, PGlobal, 1>(a.g, a.c, a.m, a.w[0], a.g.odx, a.g.odz, x, z0, p0, &sx, &sz);
+        v_update4_l<LC, false, PGlobal, 2>(a.g, a.c, a.m1, a.w[1], a.g.odx, a.g.odz, x, z0, p1, &sx, &sz, a.dcbx,
+                                           a.dcbz);
+    } else {
 #pragma unroll
-    for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.m, a.w[k], a.g.odx, a.g.odz, x, z0);
+        for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.m, a.w[k], a.g.odx, a.g.odz, x, z0);
+    }
 }
 
 // Blocks per SM of the batched pressure kernels (forward and backward), LC <= 4: the per-shot
@@ -617,7 +665,7 @@ constexpr int fwd_p_min_blocks()
     if (LC > 4) return 1;
     if (BATCH) return BATCH_P_MIN_BLOCKS;
     if (NW == 1) return MODE == FP_BORN ? 1 : 5;
-    return MODE == FP_PLAIN ? 5 : 4;
+    return MODE == FP_PLAIN ? 5 : 4;   // Born and scattered-field twins: 4
 }
 
 template <int LC, int NW, int MODE, bool BATCH = false>
@@ -625,7 +673,7 @@ __global__ void __launch_bounds__(256, (fwd_p_min_blocks<LC, NW, MODE, BATCH>())
     k_fwd_p(const FwdArgs a0)
 {
     pdl_begin();
-    constexpr bool BORN = MODE == FP_BORN;
+    constexpr bool BORN = MODE == FP_BORN, SCAT = MODE == FP_SCAT;
     FwdArgs a = a0;
     const int it = *a.itp + a.itoff;
     if constexpr (BATCH) {
@@ -644,9 +692,17 @@ __global__ void __launch_bounds__(256, (fwd_p_min_blocks<LC, NW, MODE, BATCH>())
 #pragma unroll
         for (int w = 0; w < NW; w++) {
             bool upd[4];
-            p_update4<LC>(g, a.c, a.m, a.w[w], g.odx, g.odz, x, z0, pn[w], upd,
+            p_update4<LC>(g, a.c, (SCAT && w == 1) ? a.m1 : a.m, a.w[w], g.odx, g.odz, x, z0, pn[w], upd,
                           (MODE != FP_PLAIN && w == 0) ? &s0 : nullptr);
             bool any = upd[0] || upd[1] || upd[2] || upd[3];
+            if constexpr (SCAT) {
+                if (w == 1) {
+                    const float4 dk = ldg4(a.dck + ip);
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (upd[k]) el(pn[w], k) = fmaf(elc(dk, k), elc(s0, k), elc(pn[w], k));
+                }
+            }
             if constexpr (BORN) {
                 if (w == 0 && a.s0_out) st4(a.s0_out + (size_t)(it % a.s0_mod) * a.s0_stride + ip, s0);
                 if (w == 1 && a.dkappa) {
@@ -656,7 +712,7 @@ __global__ void __launch_bounds__(256, (fwd_p_min_blocks<LC, NW, MODE, BATCH>())
                         if (upd[k]) el(pn[w], k) += g.dt * elc(dk, k) * elc(s0, k);
                 }
             }
-            if (x == a.sx) {
+            if (x == a.sx && !(SCAT && w == 1)) {   // the source is the same in both models
 #pragma unroll
                 for (int k = 0; k < 4; k++)
                     if (a.sz == z0 + k) { el(pn[w], k) += (w == 0 ? a.wav0[it] : a.wav1[it]); any = true; }
@@ -667,14 +723,19 @@ __global__ void __launch_bounds__(256, (fwd_p_min_blocks<LC, NW, MODE, BATCH>())
         if (wc >= 0) {
             const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * g.ldz + z0));
             const int t[4] = {tr.x, tr.y, tr.z, tr.w};
-            constexpr int rf = (BORN && NW == 2) ? 1 : 0;   // Born data: the scattered field
+            constexpr int rf = ((BORN || SCAT) && NW == 2) ? 1 : 0;   // Born / scattered data: field 1
 #pragma unroll
             for (int k = 0; k < 4; k++)
                 if (t[k] >= 0 && z0 + k < g.ntz) a.seis[(size_t)t[k] * a.nt + it] = elc(pn[rf], k);
             if (a.colmap) {
                 float2 *cb = a.colbuf + ((size_t)wc * a.nt + it) * g.ldz + z0;
+                if constexpr (SCAT) {
 #pragma unroll
-                for (int k = 0; k < 4; k++) cb[k] = make_float2(elc(pn[0], k), elc(pn[NW - 1], k));
+                    for (int k = 0; k < 4; k++) (&cb[k].x)[a.colcomp] = elc(pn[1], k);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) cb[k] = make_float2(elc(pn[0], k), elc(pn[NW - 1], k));
+                }
             }
         }
     }

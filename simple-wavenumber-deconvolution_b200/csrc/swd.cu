@@ -47,6 +47,10 @@ struct swd_ctx {
     std::vector<DevBuf *> bufs;
     // model / operator; mat = the update coefficients cbx, cbz, ck (struct Mat)
     DevBuf vp, rho, cpml[8], mat[4];
+    // perturbed model of the exact scattered field (swd_set_scatter_model): its coefficients
+    // and the coefficient differences dcbx, dcbz, dck against the background
+    DevBuf vp1, rho1, mat1[4], dmat[3];
+    bool have_scatter = false;
     // wavefields: w[0], w[1] (7 arrays each), dp/dt
     DevBuf wave[2][7], dpdt;
     // second copies of p, vx, vz, phi_p_x, phi_p_z for the fused (double-buffered) path
@@ -85,7 +89,7 @@ struct swd_ctx {
     DevBuf cig, cigring;
     // deconvolution scratch kept between swd_decon calls: inputs, taper, window slots,
     // outputs, staged workspaces
-    DevBuf dcn[5];
+    DevBuf dcn[6];
     DevBuf Ipart, Spart, Rpart;   // FP32 block sums of the imaging condition
     int batch_opt = 0;      // shots per batched launch; 0 = autotune on first use
     int batch_tuned = 0;    // the autotuner's choice (0 = not tuned yet)
@@ -124,6 +128,10 @@ struct swd_ctx {
             for (auto &b : w) bufs.push_back(&b);
         for (auto &b : cpml) bufs.push_back(&b);
         for (auto &b : mat) bufs.push_back(&b);
+        for (auto &b : mat1) bufs.push_back(&b);
+        for (auto &b : dmat) bufs.push_back(&b);
+        bufs.push_back(&vp1);
+        bufs.push_back(&rho1);
         for (auto &w : wave)
             for (auto &b : w) bufs.push_back(&b);
         for (auto &w : wave2)
@@ -279,6 +287,13 @@ static Mat make_mat(swd_ctx *c)
 {
     Mat m;
     m.cbx = F(c->mat[0]); m.cbz = F(c->mat[1]); m.ck = F(c->mat[2]); m.kap = F(c->mat[3]);
+    return m;
+}
+
+static Mat make_mat1(swd_ctx *c)
+{
+    Mat m;
+    m.cbx = F(c->mat1[0]); m.cbz = F(c->mat1[1]); m.ck = F(c->mat1[2]); m.kap = F(c->mat1[3]);
     return m;
 }
 
@@ -619,6 +634,32 @@ __global__ void k_material(const float *__restrict__ vp, const float *__restrict
     }
 }
 
+// Differences of the update coefficients of a perturbed model (vp1, rho1) and the background
+// (vp0, rho0), formed in double from the float models and rounded once, so the secondary
+// sources of the exact scattered field carry the FP64 coefficient differences rather than the
+// difference of two rounded coefficients (which would lose the digits the perturbation holds).
+__global__ void k_material_delta(const float *__restrict__ vp0, const float *__restrict__ rho0,
+                                 const float *__restrict__ vp1, const float *__restrict__ rho1, float dt, int ntx,
+                                 int ntz, int ldz, float *dcbx, float *dcbz, float *dck)
+{
+    const size_t n = (size_t)ntx * ldz;
+    const double t = (double)dt;
+    auto b = [&](double r0, double r1) { const double s = 0.5 * (r0 + r1); return s != 0.0 ? t / s : 0.0; };
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int z = (int)(i % ldz);
+        float bx = 0.f, bz = 0.f, kc = 0.f;
+        if (z < ntz) {
+            const double v0 = vp0[i], v1 = vp1[i], r0 = rho0[i], r1 = rho1[i];
+            bx = (float)(b(r1, rho1[i + ldz]) - b(r0, rho0[i + ldz]));
+            bz = (float)(b(r1, rho1[i + 1]) - b(r0, rho0[i + 1]));
+            kc = (float)(t * r1 * v1 * v1 - t * r0 * v0 * v0);
+        }
+        dcbx[i] = bx;
+        dcbz[i] = bz;
+        dck[i] = kc;
+    }
+}
+
 // model_in_pml (acoustic_HLVSPRTMC.cpp:1428-1468): x-edges for interior rows, then z-edges
 __global__ void k_pml_x(float *v, int ntx, int ntz, int pml)
 {
@@ -666,7 +707,9 @@ template <int LC>
 static void launch_fwd_v(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bool pdl = false)
 {
     const bool ck = a.ck.every > 0;
-    if (nw == 2) {
+    if (nw == 2 && a.dck) {
+        launch_step(k_fwd_v<LC, 2, false, false, true>, grid, s, pdl, a);
+    } else if (nw == 2) {
         if (ck) launch_step(k_fwd_v<LC, 2, true>, grid, s, pdl, a);
         else launch_step(k_fwd_v<LC, 2, false>, grid, s, pdl, a);
     } else {
@@ -679,7 +722,9 @@ template <int LC>
 static void launch_fwd_p(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bool pdl = false)
 {
     const bool born = a.s0_out || a.dkappa;
-    if (nw == 2) {
+    if (nw == 2 && a.dck) {
+        launch_step(k_fwd_p<LC, 2, FP_SCAT>, grid, s, pdl, a);
+    } else if (nw == 2) {
         if (born) launch_step(k_fwd_p<LC, 2, FP_BORN>, grid, s, pdl, a);
         else launch_step(k_fwd_p<LC, 2, FP_PLAIN>, grid, s, pdl, a);
     } else {
@@ -877,6 +922,10 @@ struct FwdJob {
     int s0_mod = 1;
     Ckpt ck{};               // background checkpoints (ck.every == 0: none)
     DpStore ds{};            // stored source dp/dt (ds.buf == nullptr: none)
+    // exact scattered field: field 1 = u(perturbed model) - u(background), no wavelet of its
+    // own; colcomp: the colbuf component it records (-1: the twin pair)
+    bool scat = false;
+    int colcomp = -1;
 };
 
 // device copies of the shot's wavelet(s): wav[0..nt) = rick, wav[nt..2nt) = Hilbert twin
@@ -884,7 +933,7 @@ static int upload_wavelets(swd_ctx *ctx, const FwdJob &J, int nt)
 {
     CKR(ensure(ctx, ctx->wav, sizeof(float) * 2 * (size_t)ctx->grid.nt_max));
     CK(cudaMemcpyAsync(F(ctx->wav), J.rick.data(), sizeof(float) * nt, cudaMemcpyHostToDevice, ctx->stream));
-    if (J.twin && J.dkappa) CK(cudaMemsetAsync(F(ctx->wav) + nt, 0, sizeof(float) * nt, ctx->stream));
+    if (J.twin && (J.dkappa || J.scat)) CK(cudaMemsetAsync(F(ctx->wav) + nt, 0, sizeof(float) * nt, ctx->stream));
     else if (J.twin) CK(cudaMemcpyAsync(F(ctx->wav) + nt, J.hrick.data(), sizeof(float) * nt, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));   // the host vectors may go away after this
     return SWD_OK;
@@ -992,7 +1041,7 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
 {
     ctx->kept.valid = false;   // wave[0], strips and the wavelet buffer are overwritten
     // Born fields, S0 output and checkpoints exist on the plain kernels only
-    if (fused(ctx) && !J.dkappa && !J.s0 && !J.ck.every && !J.ds.buf) return run_forward_fused(ctx, J, P);
+    if (fused(ctx) && !J.dkappa && !J.s0 && !J.ck.every && !J.ds.buf && !J.scat) return run_forward_fused(ctx, J, P);
     const swd_shot *s = J.shot;
     const int nt = s->nt;
     CKR(zero_wave(ctx, 0));
@@ -1020,6 +1069,13 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     a.dkappa = J.dkappa;
     a.ck = J.ck;
     a.ds = J.ds;
+    a.colcomp = J.colcomp;
+    if (J.scat) {
+        a.m1 = make_mat1(ctx);
+        a.dcbx = F(ctx->dmat[0]);
+        a.dcbz = F(ctx->dmat[1]);
+        a.dck = F(ctx->dmat[2]);
+    }
     const dim3 grid = grid_blocks(ctx);
     if (J.save_strips) {
         const int slen = strip_len(ctx);
@@ -1188,7 +1244,9 @@ static int decon_geo(const swd_decon_params *p, DeconGeo &g)
     if (p->filterwinx < g.outwinx || p->filterwinz < g.outwinz) return SWD_ERR_ARG;
     if (g.n0 > 512 || g.n1 > 512) return SWD_ERR_ARG;
     if (p->workspace != 0 && p->workspace != 1) return SWD_ERR_ARG;
-    g.staged = p->workspace == 1 || (size_t)g.FX * g.FZ * 8 + (g.n0 + g.n1) * 8 > 200 * 1024;
+    // the buffer and the transform tables in shared memory when they fit in 220 KB (of the
+    // 227 KB a CTA may have), else the buffer in a global workspace
+    g.staged = p->workspace == 1 || ((size_t)g.FX * g.FZ + decon_tab_len(g)) * 8 > 220 * 1024;
     if (p->iters < 0 || p->iters > 100000 || !(p->reg_l1 >= 0.0f) || !(p->reg_l2 >= 0.0f)) return SWD_ERR_ARG;
     g.iters = p->iters;
     g.reg_l1 = p->reg_l1;
@@ -1205,7 +1263,7 @@ static bool decon_persistent(const DeconGeo &g) { return g.staged || g.iters > 0
 static size_t decon_staged_cap(const DeconGeo &g) { return std::max<size_t>(12288, std::max(g.n0, g.n1)); }
 static size_t decon_ws_smem(const DeconGeo &g)
 {
-    return sizeof(float2) * (g.n0 + g.n1 + (g.staged ? decon_staged_cap(g) : (size_t)g.FX * g.FZ));
+    return sizeof(float2) * (decon_tab_len(g) + (g.staged ? decon_staged_cap(g) : (size_t)g.FX * g.FZ));
 }
 static const void *decon_ws_kernel(const DeconGeo &g)
 {
@@ -1225,22 +1283,25 @@ static int decon_ws_blocks(const DeconGeo &g, int dev)
     return std::max(1, std::min(g.totalnum, nsm * std::max(occ, 1)));
 }
 
-// Window kernel of g: one CTA per window in shared memory, or nblk persistent CTAs over the
-// workspace ws (staged transforms or iterations).
+// Window kernel of g: the transform tables are built into tabs (decon_tab_len(g) float2),
+// then one CTA per window in shared memory, or nblk persistent CTAs over the workspace ws
+// (staged transforms or iterations).  Two launches (three when n1 != n0).
 static cudaError_t launch_decon_windows(const DeconGeo &g, const float *mig, const float *psf, float *winout,
-                                        float *ws, int nblk, cudaStream_t st)
+                                        float *ws, int nblk, float2 *tabs, cudaStream_t st)
 {
+    k_wfft_tables<<<(int)((wfft_table_len(g.n0) + 63) / 64), 64, 0, st>>>(tabs, g.n0);
+    if (g.n1 != g.n0) k_wfft_tables<<<(int)((wfft_table_len(g.n1) + 63) / 64), 64, 0, st>>>(tabs + wfft_table_len(g.n0), g.n1);
     if (decon_persistent(g)) {
         const size_t sm = decon_ws_smem(g);
         cudaError_t e = cudaFuncSetAttribute(decon_ws_kernel(g), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        if (g.staged) k_decon_window_ws<true><<<nblk, 512, sm, st>>>(g, mig, psf, winout, ws, (int)decon_staged_cap(g));
-        else k_decon_window_ws<false><<<nblk, 512, sm, st>>>(g, mig, psf, winout, ws, 0);
+        if (g.staged) k_decon_window_ws<true><<<nblk, 512, sm, st>>>(g, mig, psf, winout, ws, (int)decon_staged_cap(g), tabs);
+        else k_decon_window_ws<false><<<nblk, 512, sm, st>>>(g, mig, psf, winout, ws, 0, tabs);
     } else {
-        const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + g.n0 + g.n1);
+        const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + decon_tab_len(g));
         cudaError_t e = cudaFuncSetAttribute(k_decon_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        k_decon_window<<<g.totalnum, 512, sm, st>>>(g, mig, psf, winout);
+        k_decon_window<<<g.totalnum, 512, sm, st>>>(g, mig, psf, winout, tabs);
     }
     return cudaGetLastError();
 }
@@ -1436,6 +1497,7 @@ int swd_set_model(swd_ctx *ctx, const float *vp, const float *rho)
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_model = true;
+    ctx->have_scatter = false;   // its coefficient differences were formed against the old model
     return SWD_OK;
 }
 
@@ -1535,6 +1597,93 @@ int swd_forward(swd_ctx *ctx, const swd_shot *shot, const float *rick, const flo
         CKR(copy_aliases(ctx, P, dn, nt));
         if (seis_up) CKR(from_dev(ctx, seis_up, up, sizeof(float) * (size_t)r_n * nt));
         if (seis_down) CKR(from_dev(ctx, seis_down, dn, sizeof(float) * (size_t)r_n * nt));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    prof_collect(ctx);
+    return SWD_OK;
+}
+
+int swd_set_scatter_model(swd_ctx *ctx, const float *vp1, const float *rho1)
+{
+    if (!ctx) return SWD_ERR_ARG;
+    if (!vp1 && !rho1) {
+        ctx->have_scatter = false;
+        return SWD_OK;
+    }
+    if (!vp1 || !rho1) return fail(ctx, SWD_ERR_ARG, "vp1 and rho1 are both required");
+    if (!ctx->have_model) return fail(ctx, SWD_ERR_STATE, "set the background model first");
+    CK(cudaSetDevice(ctx->dev));
+    CKR(ensure_grid(ctx, ctx->vp1, sizeof(float), 1));
+    CKR(ensure_grid(ctx, ctx->rho1, sizeof(float), 1));
+    CK(cudaMemsetAsync(ctx->vp1.p, 0, ctx->vp1.n, ctx->stream));
+    CK(cudaMemsetAsync(ctx->rho1.p, 0, ctx->rho1.n, ctx->stream));
+    CKR(grid_to_dev(ctx, F(ctx->vp1), vp1));
+    CKR(grid_to_dev(ctx, F(ctx->rho1), rho1));
+    for (auto &b : ctx->mat1) CKR(ensure_grid(ctx, b, sizeof(float)));
+    for (auto &b : ctx->dmat) CKR(ensure_grid(ctx, b, sizeof(float)));
+    k_material<<<592, 256, 0, ctx->stream>>>(F(ctx->vp1), F(ctx->rho1), ctx->grid.dt, ctx->ntx, ctx->ntz, ctx->ldz,
+                                             F(ctx->mat1[0]), F(ctx->mat1[1]), F(ctx->mat1[2]), F(ctx->mat1[3]));
+    k_material_delta<<<592, 256, 0, ctx->stream>>>(F(ctx->vp), F(ctx->rho), F(ctx->vp1), F(ctx->rho1), ctx->grid.dt,
+                                                   ctx->ntx, ctx->ntz, ctx->ldz, F(ctx->dmat[0]), F(ctx->dmat[1]),
+                                                   F(ctx->dmat[2]));
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->have_scatter = true;
+    return SWD_OK;
+}
+
+int swd_forward_scatter(swd_ctx *ctx, const swd_shot *shot, const float *rick, const float *hrick,
+                        const float *kz_coef, float *seis, float *seis_up, float *seis_down)
+{
+    CKR(check_ready(ctx));
+    if (!ctx->have_scatter) return fail(ctx, SWD_ERR_STATE, "no perturbed model (swd_set_scatter_model)");
+    if (!rick || !seis) return fail(ctx, SWD_ERR_ARG, "rick and seis are required");
+    const bool split = hrick != nullptr && kz_coef != nullptr;
+    if ((seis_up || seis_down) && !split) return fail(ctx, SWD_ERR_ARG, "seis_up/seis_down need hrick and kz_coef");
+    ShotPlan P;
+    CKR(plan_shot(ctx, shot, P));
+    const int nt = shot->nt, r_n = shot->r_n;
+    const size_t nrec = (size_t)r_n * nt;
+    CKR(ensure(ctx, ctx->seis, sizeof(float) * nrec));
+    CK(cudaMemsetAsync(ctx->seis.p, 0, sizeof(float) * nrec, ctx->stream));
+    if (split) {
+        CKR(ensure(ctx, ctx->colbuf, sizeof(float2) * (size_t)P.nwells * nt * ctx->ldz));
+        CKR(ensure(ctx, ctx->seis2, sizeof(float) * 2 * nrec));
+    }
+    // pass 0: the wavelet's background and scattered fields (scattered record; column .x);
+    // pass 1, for the up/down split: the Hilbert wavelet's (column .y; its record is dropped)
+    for (int pass = 0; pass < (split ? 2 : 1); pass++) {
+        FwdJob J;
+        J.shot = shot;
+        CKR(host_copy(ctx, J.rick, pass == 0 ? rick : hrick, nt));
+        J.twin = true;
+        J.scat = true;
+        J.colcomp = split ? pass : -1;
+        J.seis_dev = pass == 0 ? F(ctx->seis) : F(ctx->seis2);
+        J.colbuf = split ? (float2 *)ctx->colbuf.p : nullptr;
+        CKR(run_forward(ctx, J, P));
+    }
+    CKR(copy_aliases(ctx, P, F(ctx->seis), nt));
+    CKR(from_dev(ctx, seis, ctx->seis.p, sizeof(float) * nrec));
+    if (split) {
+        const int N = swd_prep_pow2(ctx->ntz);
+        CKR(ensure(ctx, ctx->kzcoef, sizeof(float) * N));
+        CKR(to_dev(ctx, ctx->kzcoef.p, kz_coef, sizeof(float) * N));
+        CKR(make_twiddles(ctx, ctx->tw, N));
+        float *up = F(ctx->seis2), *dn = up + nrec;
+        CK(cudaMemsetAsync(up, 0, sizeof(float) * 2 * nrec, ctx->stream));
+        const size_t sm = 2 * sizeof(float2) * N;
+        CK(cudaFuncSetAttribute(k_kzsep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_kzsep<<<dim3(nt, P.nwells), 256, sm, ctx->stream>>>((const float2 *)ctx->colbuf.p, F(ctx->kzcoef),
+                                                               (const float2 *)ctx->tw.p, I32(ctx->wmap), up, dn, nt,
+                                                               ctx->ntz, ctx->ldz, N, ilog2(N));
+        ctx->launches++;
+        CK(cudaGetLastError());
+        CKR(copy_aliases(ctx, P, up, nt));
+        CKR(copy_aliases(ctx, P, dn, nt));
+        if (seis_up) CKR(from_dev(ctx, seis_up, up, sizeof(float) * nrec));
+        if (seis_down) CKR(from_dev(ctx, seis_down, dn, sizeof(float) * nrec));
     }
     CK(cudaStreamSynchronize(ctx->stream));
     prof_collect(ctx);
@@ -2018,13 +2167,15 @@ int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, 
         // another GPU's memory) goes through the context's scratch with copies
         const bool din = is_device_ptr_on(migreal, ctx->dev) && is_device_ptr_on(migpsf, ctx->dev);
         const bool dout = is_device_ptr_on(mig_dec, ctx->dev) && is_device_ptr_on(mig_coef, ctx->dev);
-        DevBuf &bin = ctx->dcn[0], &bcoef = ctx->dcn[1], &bwin = ctx->dcn[2], &bout = ctx->dcn[3], &bws = ctx->dcn[4];
+        DevBuf &bin = ctx->dcn[0], &bcoef = ctx->dcn[1], &bwin = ctx->dcn[2], &bout = ctx->dcn[3], &bws = ctx->dcn[4],
+               &btab = ctx->dcn[5];
         const int nblk = decon_persistent(g) ? decon_ws_blocks(g, ctx->dev) : 0;
         if (decon_persistent(g) && nblk < 1) { rc = fail(ctx, SWD_ERR_CUDA, "decon: no launch shape for the window kernel"); break; }
         if (decon_persistent(g)) rc = ensure(ctx, bws, sizeof(float) * (size_t)nblk * decon_ws_floats(g));
         if (!rc && !din) rc = ensure(ctx, bin, sizeof(float) * 2 * np);
         if (!rc) rc = ensure(ctx, bcoef, sizeof(float) * nout);
         if (!rc) rc = ensure(ctx, bwin, sizeof(float) * nout * g.totalnum);
+        if (!rc) rc = ensure(ctx, btab, sizeof(float2) * decon_tab_len(g));
         if (!rc && !dout) rc = ensure(ctx, bout, sizeof(float) * 2 * np);
         const float *im = din ? migreal : F(bin), *ps = din ? migpsf : F(bin) + np;
         float *od = dout ? mig_dec : F(bout), *oc = dout ? mig_coef : F(bout) + np;
@@ -2033,13 +2184,13 @@ int swd_decon(swd_ctx *ctx_in, const swd_decon_params *p, const float *migreal, 
         if (!rc && cudaMemcpyAsync(bcoef.p, coefr.data(), sizeof(float) * nout, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
             rc = fail(ctx, SWD_ERR_CUDA, "decon: coefficient upload");
         if (!rc) {
-            cudaError_t e = launch_decon_windows(g, im, ps, F(bwin), F(bws), nblk, ctx->stream);
+            cudaError_t e = launch_decon_windows(g, im, ps, F(bwin), F(bws), nblk, (float2 *)btab.p, ctx->stream);
             if (e == cudaSuccess) {
                 k_decon_gather<<<592, 256, 0, ctx->stream>>>(g, F(bwin), F(bcoef), od, oc);
                 e = cudaGetLastError();
             }
             if (e != cudaSuccess) rc = fail(ctx, SWD_ERR_CUDA, "decon kernels: %s", cudaGetErrorString(e));
-            else ctx->launches += 2;
+            else ctx->launches += g.n1 != g.n0 ? 4 : 3;
         }
         if (!rc && !dout) rc = from_dev(ctx, mig_dec, od, sizeof(float) * np);
         if (!rc && !dout) rc = from_dev(ctx, mig_coef, oc, sizeof(float) * np);
@@ -2059,9 +2210,11 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
     DeconGeo g;
     if (!p || decon_geo(p, g) != SWD_OK) return SWD_ERR_ARG;
     const size_t nout = (size_t)g.outwinx * g.outwinz;
-    // scratch: taper, window slots, then (persistent kernel) the CTA workspaces from a 256-byte
-    // aligned offset; that kernel runs on as many CTAs as have a workspace that fits
-    const size_t used = (size_t)g.totalnum * nout + nout, wsoff = (used + 63) & ~(size_t)63;
+    // scratch: taper, window slots, the transform tables (from a 256-byte aligned offset), then
+    // (persistent kernel) the CTA workspaces from the next 256-byte aligned offset; that kernel
+    // runs on as many CTAs as have a workspace that fits
+    const size_t tabof = ((size_t)g.totalnum * nout + nout + 63) & ~(size_t)63;
+    const size_t used = tabof + 2 * decon_tab_len(g), wsoff = (used + 63) & ~(size_t)63;
     if (used > SWD_DECON_STATIC_SCRATCH_FLOATS) return SWD_ERR_CAPACITY;
     // a launch error left over from the caller's own work is not this call's: clear it, so the
     // checks below see only this call's launches
@@ -2099,7 +2252,8 @@ int swd_decon_noalloc(const swd_decon_params *p, const float *migreal, const flo
     cudaStream_t st = (cudaStream_t)cuda_stream;
     k_decon_taper<<<(int)((nout + 255) / 256), 256, 0, st>>>(coefr, g.outwinx, g.outwinz, p->snapwinx, p->snapwinz);
     if (cudaGetLastError() != cudaSuccess) return SWD_ERR_CUDA;
-    if (launch_decon_windows(g, migreal, migpsf, winout, coefr + wsoff, nblk, st) != cudaSuccess)
+    if (launch_decon_windows(g, migreal, migpsf, winout, coefr + wsoff, nblk, (float2 *)(coefr + tabof), st) !=
+        cudaSuccess)
         return SWD_ERR_CUDA;
     k_decon_gather<<<592, 256, 0, st>>>(g, winout, coefr, mig_dec, mig_coef);
     return cudaGetLastError() == cudaSuccess ? SWD_OK : SWD_ERR_CUDA;

@@ -54,6 +54,7 @@ def test_truncated_parameter_file_is_an_error():
     ("AVSPRTM", "swd.data = sideways", "swd.data = sideways: expected up|full|down"),
     ("AVSPRTM", "swd.strip_precision = fp16", "swd.strip_precision = fp16: expected f32|f16|bf16|i16"),
     ("AFor", "swd.perturb = pressure", "swd.perturb = pressure: expected density|velocity"),
+    ("AFor", "swd.scatter_field = born", "swd.scatter_field = born: expected difference|exact"),
 ])
 def test_unknown_extension_value_is_an_error(prog, line, msg):
     """An extension value the program does not know stops it before any device work, instead
@@ -68,6 +69,109 @@ def test_unknown_extension_value_is_an_error(prog, line, msg):
         r = subprocess.run([str(PKG_DIR / prog)], cwd=cwd, capture_output=True, text=True)
         assert r.returncode != 0
         assert msg in r.stdout
+
+
+def test_record_of_another_size_is_an_error():
+    """A record whose size is not r_n x itmax of its shot stops AVSPRTM before any device work,
+    with both shapes in the message (the reference would fread it without looking)."""
+    mk = _mkg("make_golden_ref_gpu")
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        mk.write_params(d / "parameter.txt", mk.CASE, 0)
+        mk.model().tofile(d / "input" / "acc_vp.bin")
+        np.zeros((41, mk.CASE["itmax"]), np.float32).tofile(d / "output" / "1source_seismogram_obsup.bin")
+        r = subprocess.run([str(PKG_DIR / "AVSPRTM")], cwd=d, capture_output=True, text=True)
+        assert r.returncode != 0
+        assert "holds 16400 floats; r_n x itmax = 42 x 400 = 16800 expected" in r.stdout
+        (d / "output" / "1source_seismogram_obsup.bin").unlink()
+        r = subprocess.run([str(PKG_DIR / "AVSPRTM")], cwd=d, capture_output=True, text=True)
+        assert r.returncode != 0 and "Cannot Open the File: ./output/1source_seismogram_obsup.bin" in r.stdout
+
+
+@pytest.mark.parametrize("prog", ["AFor", "AVSPRTM"])
+@pytest.mark.parametrize("text,msg", [
+    ("3\n10 5\n10 6\n", "3 receivers announced, 2 read"),
+    ("2\n10 5\n100 6\n", "receiver 1 at (100, 6) lies outside the 100 x 60 model"),
+    ("none\n", "no receiver count"),
+])
+def test_malformed_receivers_file_is_an_error(prog, text, msg):
+    """A shot's own receiver list (input/<shot>source_receivers.txt) that is short, outside the
+    model or without a count stops either program before any device work."""
+    mk = _mkg("make_golden_ref_gpu")
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        mk.write_params(d / "parameter.txt", mk.CASE, 0)
+        mk.model().tofile(d / "input" / "acc_vp.bin")
+        (d / "input" / "1source_receivers.txt").write_text(text)
+        cwd = d / "forward" if prog == "AFor" else d
+        r = subprocess.run([str(PKG_DIR / prog)], cwd=cwd, capture_output=True, text=True)
+        assert r.returncode != 0
+        assert msg in r.stdout
+
+
+@pytest.mark.gpu
+def test_per_shot_receivers_and_record_selection(swd):
+    """Two shots, the second with its own receiver list (30 receivers on one line, not the two
+    edge wells): AFor writes each shot's records with its own trace count, and AVSPRTM migrates
+    the full, down-going or up-going record (swd.data) of each shot with that shot's receivers,
+    giving the images of swd_rtm_shot on the same arrays."""
+    mk = _mkg("make_golden_ref_gpu")
+    c = dict(mk.CASE, ns=2, shotdx=150.0)
+    nx, nz, nt, pml, Lc = c["nx"], c["nz"], c["itmax"], c["pml"], c["Lc"]
+    p = pml + Lc
+    rx2, rz2 = np.full(30, 60), np.arange(5, 35)
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        v = mk.model()
+        v.tofile(d / "input" / "acc_vp.bin")
+        (d / "input" / "2source_receivers.txt").write_text("30\n" + "".join(f"{a} {b}\n" for a, b in zip(rx2, rz2)))
+        mk.write_params(d / "parameter.txt", c, 0)
+        subprocess.run([str(PKG_DIR / "AFor")], cwd=d / "forward", check=True, capture_output=True)
+        rd = lambda name: np.fromfile(d / "output" / name, np.float32)
+        r_n1 = rd("1source_seismogram_obs.bin").size // nt
+        assert r_n1 == 42 and rd("2source_seismogram_obs.bin").size == 30 * nt
+        E = swd.Engine(nx, nz, pml, Lc, c["dx"], c["dz"], c["dt"], nt)
+        vp = swd.pad_model(v, p)
+        rho = np.full_like(vp, 1000.0)
+        E.setup_default(vp, rho)
+        E.set_model(E.smooth(vp, p, c["window"]), rho)
+        rick = swd.ricker_wave(nt, c["f0"], c["dt"])
+        shot2 = swd.ShotSpec(p + int(c["sx0"] / c["dx"]) + int(c["shotdx"] / c["dx"]), p, rx2 + p, rz2 + p, nt)
+        for which, suffix in (("full", ""), ("down", "down"), ("up", "up")):
+            mk.write_params(d / "parameter.txt", c, 0)
+            with open(d / "parameter.txt", "a") as f:
+                f.write(f"swd.data = {which}\n")
+            subprocess.run([str(PKG_DIR / "AVSPRTM")], cwd=d, check=True, capture_output=True)
+            data2 = rd(f"2source_seismogram_obs{suffix}.bin").reshape(30, nt)
+            assert np.abs(data2).max() > 0
+            out = E.rtm_shot(shot2, rick, data2, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK,
+                             want=("image_pp", "fimage"))
+            assert rel_l2(rd("image_pp2.bin").reshape(nx, nz), out["image_pp"]) < 1e-6, which
+            assert rel_l2(rd("fimage_pp2.bin").reshape(nx, nz), out["fimage"]) < 1e-6, which
+        E.close()
+
+
+@pytest.mark.gpu
+def test_afor_exact_scatter_field_option(swd):
+    """`swd.scatter_field = exact` writes the scatter records of swd_forward_scatter; they agree
+    with the default difference of records to that difference's FP32 cancellation error."""
+    g = np.load(GOLDEN / "ref_gpu_small.npz")
+    mk = _mkg("make_golden_ref_gpu")
+    nt = int(g["case"][4])
+    with tempfile.TemporaryDirectory() as d:
+        d = _tree(Path(d))
+        g["acc_vp"].tofile(d / "input" / "acc_vp.bin")
+        rd = lambda name: np.fromfile(d / "output" / name, np.float32).reshape(-1, nt)
+        mk.write_params(d / "parameter.txt", mk.CASE, 1)
+        subprocess.run([str(PKG_DIR / "AFor")], cwd=d / "forward", check=True, capture_output=True)
+        diff = {k: rd(f"1source_seismogram_{k}.bin") for k in ("scatter", "scatterup", "scatterdown")}
+        with open(d / "parameter.txt", "a") as f:
+            f.write("swd.scatter_field = exact\n")
+        subprocess.run([str(PKG_DIR / "AFor")], cwd=d / "forward", check=True, capture_output=True)
+        for k, a in diff.items():
+            b = rd(f"1source_seismogram_{k}.bin")
+            assert b.shape == a.shape and np.abs(b).max() > 0
+            assert rel_l2(b, a) < 1e-2, k
 
 
 def test_decon_rejects_even_windows():
