@@ -274,6 +274,8 @@ def run_ours(args, rank, world, dist):
         E.set_option(swd.OPT_TMA, 1)
     if args.pdl:
         E.set_option(swd.OPT_PDL, 1)
+    if args.staged:
+        E.set_option(swd.OPT_STAGED, 1)
     if args.path is not None:
         E.set_kernel_path(args.path)
     strips = w.extra.get("strips", "f32")
@@ -406,7 +408,8 @@ def run_ours(args, rank, world, dist):
         "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP64 imaging)", "data": "synthetic (seeded random-field model, PSF data)",
         "config": {"workload": WORKLOADS[args.config], "parallelism": f"replicas x{world}",
-                   "l2": "flushed (256 MiB write) before every timed step", "strips": strips},
+                   "l2": "flushed (256 MiB write) before every timed step", "strips": strips,
+                   "options": {"staged_p": int(E.get_option(swd.OPT_STAGED)), "tma_v": int(E.get_option(swd.OPT_TMA))}},
         "gcell_updates_per_s": value * cells_per_shot / 1e9,
         "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(data.nbytes + rick.nbytes),
                 "d2h_bytes_per_step": int(2 * w.nx * w.nz * 4)},
@@ -1068,6 +1071,127 @@ def lsrtm_cpu_baseline(w, nsteps=100):
                       f"{dt:.2f} s measured"}
 
 
+C5FLOW_WORKLOAD = ("c5 imaging + PSF + deconvolution flow: 4001x1601 @4 m, nt=8000, dt=0.35 ms, 25 Hz, 24 surface shots, "
+                   "1201 well receivers, FP16-scaled strips; PSF data of a 40x16 lattice of +1% velocity points on the "
+                   "migration model (exact scattered field); both images stacked over the shots; windowed "
+                   "deconvolution with 127^2 output windows at the lattice's 99-cell PSF spacing")
+
+
+def run_c5flow(args, rank, world, dist):
+    """The large-survey flow of the reference's three programs on the 4001x1601 configuration: per
+    shot, the PSF data of the scatter lattice (AFor's scatter mode, as an exact scattered field),
+    the RTM of the observed data and the RTM of the PSF data (AVSPRTM, stacked), then the windowed
+    deconvolution of the stacked image by the stacked PSF image (decon2d_mine).  A step is the whole
+    flow; the observed data (the survey's input) are modelled once beforehand.  Per-image errors
+    against FP64 come from the oracle on the first shot over the first --parity-nt steps (1500 by
+    default; the full FP64 survey is days of host time) and from the oracle's window loop on the
+    engine's own stacked images."""
+    import ctypes as C
+    import torch
+    swd = load_pkg()
+    from swd_b200 import configs
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    w = configs.c5()
+    ns = args.c5_shots
+    p = w.pmlc
+    vtrue, vmig = swd.pad_model(w.vp, p), swd.pad_model(w.vp_mig, p)
+    rho = np.full_like(vmig, 1000.0)
+    vs = vmig.copy()
+    for ix in w.scatter_x:
+        for iz in w.scatter_z:
+            vs[ix + p, iz + p] *= np.float32(1.01)
+    E = swd.Engine(w.nx, w.nz, w.pml, w.Lc, w.dx, w.dz, w.dt, w.nt, device=dev)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    E.set_stream(stream.cuda_stream)
+    E.set_strip_precision(swd.STRIP_F16)
+    rick = swd.ricker_wave(w.nt, w.f0, w.dt)
+    rx, rz = w.receivers_padded()
+    shots = [swd.ShotSpec(w.sx[i] + p, p, rx, rz, w.nt) for i in range(ns)]
+    E.setup_default(vtrue, rho)
+    obs = [E.forward(s, rick) for s in shots]           # the survey's observed records (input)
+    E.set_model(vmig, rho)
+    E.set_scatter_model(vs, rho)
+    case = configs.decon_case("c5")
+    lay = configs.decon_layout(case)
+    dp = swd.DeconParams(w.nx, w.nz, case.psfwin[0], case.psfwin[1], case.filterwin[0], case.filterwin[1],
+                         case.snapwin[0], case.snapwin[1], case.epsilon, 0, 0, 0, 0, 0, 0.0, 0.0)
+    d_mig = torch.empty((w.nx, w.nz), dtype=torch.float32, device="cuda")
+    d_psf, d_dec, d_coef = torch.empty_like(d_mig), torch.empty_like(d_mig), torch.empty_like(d_mig)
+    L = swd.lib()
+
+    def flow():
+        psf_data = []
+        E.stack_reset()
+        for s, d in zip(shots, obs):
+            psf_data.append(E.forward_scatter(s, rick))
+            E.rtm_shot(s, rick, d, want=())
+        E._ck(L.swd_stack_get(E._h, 1, swd._ptr(d_mig)))
+        E.stack_reset()
+        for s, d in zip(shots, psf_data):
+            E.rtm_shot(s, rick, d, want=())
+        E._ck(L.swd_stack_get(E._h, 1, swd._ptr(d_psf)))
+        E._ck(L.swd_decon(E._h, C.byref(dp), swd._ptr(d_mig), swd._ptr(d_psf), swd._ptr(d_dec), swd._ptr(d_coef)))
+        return psf_data
+
+    for _ in range(args.warmup):
+        flow()
+    torch.cuda.synchronize()
+    n0 = E.launch_count()
+    with ClockSampler(dev) as clk:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        total = 0.0
+        for _ in range(args.steps):
+            a.record(stream)
+            psf_data = flow()
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+    launches = E.launch_count() - n0
+    t_ms, = max_over_ranks(dist, [total], "cuda")
+    if rank != 0:
+        return None
+    per = t_ms / args.steps
+    out = {"metric": "RTM shots/s", "value": 2 * ns * args.steps * world / (t_ms / 1e3), "unit": "shots/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 imaging, FP16 strips, FP64 spectral division)",
+           "data": "synthetic (seeded random-field model)",
+           "config": {"workload": C5FLOW_WORKLOAD, "shots": ns, "migrations_per_step": 2 * ns,
+                      "parallelism": f"replicas x{world}", "windows": lay["windows"]},
+           "flow_s": per / 1e3, "survey_images_per_s": 1e3 / per, "gpu_launches": launches, "clocks": clk.summary()}
+    if not args.no_parity:
+        orc = load_oracle()
+        pnt = args.parity_nt or 1500
+        mig, psf = d_mig.cpu().numpy(), d_psf.cpu().numpy()
+        dec = d_dec.cpu().numpy()
+        t = time.perf_counter()
+        odec, _ = orc.decon(w.nx, w.nz, mig, psf, case.psfwin, case.filterwin, case.snapwin, case.epsilon,
+                            nthreads=os.cpu_count() or 1)
+        e_dec = float(np.linalg.norm(dec - odec) / np.linalg.norm(odec))
+        # shot 1 over the first pnt steps: its RTM image (observed data) and PSF image (PSF data)
+        par = {"deconvolved_image_vs_oracle_decon_of_the_same_images": e_dec}
+        for name, rec in (("image", obs[0]), ("psf_image", psf_data[0])):
+            r = fp64_parity(swd, E, w, shots[0], rick, rec, nt=pnt)
+            par[name] = {k: r[k] for k in ("image_rel_l2", "illum_rel_l2", "fimage_rel_l2", "record", "pass")}
+        # the PSF data themselves: the exact scattered field against the FP64 difference of two records
+        M0, _ = oracle_model(orc, w, w.vp_mig, pnt)
+        M1 = orc.Model(vs, rho, orc.cpml(w.ntx, w.ntz, p, w.dx, w.dz, w.dt), orc.cal_xishu(w.Lc), p, w.Lc, pnt,
+                       w.dx, w.dz, w.dt)
+        G = orc.Geom(shots[0].s_ix, shots[0].s_iz, rx, rz)
+        rk = np.ascontiguousarray(rick[:pnt])
+        d64 = orc.forward(M1, G, rk, dtype=np.float64)["seis"] - orc.forward(M0, G, rk, dtype=np.float64)["seis"]
+        E.set_scatter_model(vs, rho)
+        sh = swd.ShotSpec(shots[0].s_ix, shots[0].s_iz, rx, rz, pnt)
+        par["psf_data_vs_fp64_difference"] = float(np.linalg.norm(E.forward_scatter(sh, rk) - d64) / np.linalg.norm(d64))
+        par["note"] = (f"shot 1, first {pnt} of {w.nt} steps, against the FP64 oracle; the deconvolution against the "
+                       "oracle's FP64 window loop on the engine's stacked images")
+        par["oracle_s"] = round(time.perf_counter() - t, 1)
+        out["parity"] = par
+    E.close()
+    return out
+
+
 def run_profile_kernels(args):
     """One RTM shot on the benchmark grid with a short record (--nt) and seeded random data,
     no warm-up shots and no data generation: the command the ncu captures run, so that few
@@ -1093,6 +1217,8 @@ def run_profile_kernels(args):
         E.set_option(swd.OPT_BWD_BY_KIND, 0)
     if args.stored:
         E.set_source_storage(1, swd.STRIP_I16)
+    if args.staged:
+        E.set_option(swd.OPT_STAGED, 1)
     if args.path is not None:
         E.set_kernel_path(args.path)
     E.set_strip_precision({"f32": swd.STRIP_F32, "f16": swd.STRIP_F16}[w.extra.get("strips", "f32")])
@@ -1237,6 +1363,10 @@ def run_reference(args):
         w = configs.c3()
         metric, workload = "RTM shots/s", BATCH_WORKLOAD
         sample = lambda: survey_cpu_baseline(w, max(8, args.cpu_steps))
+    elif args.workload == "c5flow":
+        w = configs.c5()
+        metric, workload = "RTM shots/s", C5FLOW_WORKLOAD
+        sample = lambda: cpu_baseline(w, samples=1, nsteps=rtm_cpu_steps(args, w))
     else:
         w = configs.CONFIGS[args.config]()
         metric, workload = "RTM shots/s", WORKLOADS[args.config]
@@ -1273,7 +1403,8 @@ def main():
     ap.add_argument("--stored", action="store_true", help="--profile-kernels: stored-source RTM (int16 dp/dt)")
     ap.add_argument("--ref-pairing", action="store_true",
                     help="--profile-kernels: the reference's pairing of the backward phases (k_bwd_1, k_bwd_2)")
-    ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch", "decon", "afor"], default="rtm")
+    ap.add_argument("--workload", choices=["rtm", "lsrtm", "batch", "decon", "afor", "c5flow"], default="rtm")
+    ap.add_argument("--c5-shots", type=int, default=24, help="--workload c5flow: shots of the survey")
     ap.add_argument("--config", choices=["c2", "c5", "shipped"], default="c2",
                     help="grid of --workload rtm (c2, c5) or decon (c2, c5, shipped: the reference's window geometry)")
     ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
@@ -1283,6 +1414,8 @@ def main():
                     help="record length of the FP64 check (0: the whole record on c2, 1500 steps on c5)")
     ap.add_argument("--tma", action="store_true", help="velocity kernels with TMA-staged pressure tiles (SWD_OPT_TMA)")
     ap.add_argument("--pdl", action="store_true", help="step kernels as programmatic dependent launches (SWD_OPT_PDL)")
+    ap.add_argument("--staged", action="store_true",
+                    help="forward pressure kernel with every stencil operand staged by TMA (SWD_OPT_STAGED)")
     ap.add_argument("--streams", type=int, default=3,
                     help="--workload lsrtm: engines (streams and host threads) the survey's shots are spread over")
     ap.add_argument("--decon-iters", type=int, default=0,
@@ -1309,7 +1442,8 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = td
-    runner = {"rtm": run_ours, "lsrtm": run_lsrtm, "batch": run_batch, "decon": run_decon, "afor": run_afor}[args.workload]
+    runner = {"rtm": run_ours, "lsrtm": run_lsrtm, "batch": run_batch, "decon": run_decon, "afor": run_afor,
+              "c5flow": run_c5flow}[args.workload]
     out = runner(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -214,6 +214,14 @@ int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *
  *                 predecessor before touching memory; the same images bit for bit); 0 (default):
  *                 plain stream order, which measures the same with CUDA graphs */
 #define SWD_OPT_PDL 7
+/* SWD_OPT_STAGED 1: the pressure launch of the single-wavefield forward pass (RTM forward and
+ *                 plain modelling, no Born, checkpoint or stored-source mode) stages every
+ *                 stencil operand of its tiles (vx and vz with their halos, p, the material
+ *                 coefficient) through the Tensor Memory Accelerator into a three-stage
+ *                 shared-memory ring walked by persistent CTAs, so the bytes in flight are bounded
+ *                 by shared memory rather than registers (the same images bit for bit);
+ *                 0 (default): per-thread loads */
+#define SWD_OPT_STAGED 8
 int swd_set_option(swd_ctx *ctx, int option, int value);
 int swd_get_option(swd_ctx *ctx, int option, int *value);
 

@@ -28,7 +28,7 @@ SWD_OK, SWD_ERR_ARG, SWD_ERR_CUDA, SWD_ERR_ALLOC, SWD_ERR_STATE, SWD_ERR_DEVICE,
 STRIP_F32, STRIP_F16, STRIP_BF16, STRIP_I16 = 0, 1, 2, 3
 PATH_PLAIN, PATH_FUSED = 0, 1
 RTM_PREPROCESS, RTM_ILLUM_RCV, RTM_NO_STACK, RTM_CIG = 1, 2, 4, 8
-OPT_GRAPHS, OPT_BATCH, OPT_BATCH_TUNED, OPT_IMAGE_BLOCKS, OPT_BWD_BY_KIND, OPT_TMA, OPT_PDL = 1, 2, 3, 4, 5, 6, 7
+OPT_GRAPHS, OPT_BATCH, OPT_BATCH_TUNED, OPT_IMAGE_BLOCKS, OPT_BWD_BY_KIND, OPT_TMA, OPT_PDL, OPT_STAGED = 1, 2, 3, 4, 5, 6, 7, 8
 
 
 class SwdError(RuntimeError):

@@ -325,6 +325,10 @@ int swd_set_option(swd_ctx *ctx, int option, int value)
             if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_PDL takes 0 or 1");
             ctx->use_pdl = value;
             return SWD_OK;
+        case SWD_OPT_STAGED:
+            if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_STAGED takes 0 or 1");
+            ctx->use_staged = value;
+            return SWD_OK;
         default:
             return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
@@ -341,6 +345,7 @@ int swd_get_option(swd_ctx *ctx, int option, int *value)
         case SWD_OPT_BWD_BY_KIND: *value = ctx->bwd_by_kind; return SWD_OK;
         case SWD_OPT_TMA: *value = ctx->use_tma; return SWD_OK;
         case SWD_OPT_PDL: *value = ctx->use_pdl; return SWD_OK;
+        case SWD_OPT_STAGED: *value = ctx->use_staged; return SWD_OK;
         default: return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
 }

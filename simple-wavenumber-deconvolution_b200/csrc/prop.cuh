@@ -234,6 +234,10 @@ struct PTile {
 
 // velocity half step (reference kernels _vx/_vz, acoustic_HLVSPRTMLc.cu:24-118; receiver
 // variants with the wider guards and -dx/-dz, :623-715), the pressure read through pl.
+// Within each half the coefficient and the old velocity are loaded with the pressure taps,
+// before the CPML branch and its store: a load after a store through a pointer the compiler
+// cannot prove distinct waits for the branch, which adds a memory latency per half.  The
+// arithmetic is the reference's, term by term.
 // Scattered-field hooks (SC): 1 also returns the update sums d + phi of the four cells in
 // (*sx, *sz) (zero where a velocity is not updated); 2 adds dcb * (*sx, *sz) to the update, the
 // secondary source of an exact scattered field (coefficient difference dcbx, dcbz).
@@ -261,6 +265,8 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
             any |= gx[k];
         }
         if (any) {
+            const float4 cb = ldg4(m.cbx + ip);
+            float4 v = ld4(w.vx + ip);
             float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int ic = 0; ic < LC; ic++) {
@@ -280,8 +286,6 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
                 }
                 st4(w.ppx + ip, po);
             }
-            const float4 cb = ldg4(m.cbx + ip);
-            float4 v = ld4(w.vx + ip);
 #pragma unroll
             for (int k = 0; k < 4; k++)
                 if (gx[k]) el(v, k) = elc(cb, k) * (elc(d, k) + elc(phi, k)) + elc(v, k);
@@ -311,6 +315,8 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
             any |= gz[k];
         }
         if (any) {
+            const float4 cb = ldg4(m.cbz + ip);
+            float4 v = ld4(w.vz + ip);
             ZWin<LC> pw;
             pl.zwin(pw, x, z0);
             float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -331,8 +337,6 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
                 }
                 st4(w.ppz + ip, po);
             }
-            const float4 cb = ldg4(m.cbz + ip);
-            float4 v = ld4(w.vz + ip);
 #pragma unroll
             for (int k = 0; k < 4; k++)
                 if (gz[k]) el(v, k) = elc(cb, k) * (elc(d, k) + elc(phi, k)) + elc(v, k);
@@ -360,7 +364,9 @@ __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat
 }
 
 // pressure step with CPML (reference kernel _p, :121-173) on the four cells; returns the
-// new values in pn (old values where not updated) and the per-cell update flags.
+// new values in pn (old values where not updated) and the per-cell update flags.  The
+// coefficient ck is loaded with the old pressure, before the CPML branches and their stores
+// (see v_update4_l).
 template <int LC>
 __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
                                           int x, int z0, float4 &pn, bool upd[4], float4 *ssum = nullptr)
@@ -376,6 +382,7 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat
         any |= upd[k];
     }
     if (!any) return;
+    const float4 kc = ldg4(m.ck + ip);
     float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
     const Taps<LC> tx(g, odx), tz(g, odz);
     ZWin<LC> vw;
@@ -413,7 +420,6 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat
         }
         st4(w.pvz + ip, po);
     }
-    const float4 kc = ldg4(m.ck + ip);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const float sk = elc(dvx, k) + elc(phx, k) + elc(dvz, k) + elc(phz, k);

@@ -164,3 +164,255 @@ __global__ void __launch_bounds__(256) k_bwd_v_tma(const BwdArgs a, const __grid
 }
 
 }  // namespace swd
+
+namespace swd {
+
+// ------------------------------------------------------------------------------------
+// Fully staged step kernels.  Every stencil operand of a tile (8 columns x 128 rows, the plain
+// kernels' block layout) is moved by cp.async.bulk.tensor into a shared-memory stage: the
+// neighbour columns and rows the taps read, the field updated in place and its material
+// coefficient.  The bytes in flight are then bounded by shared memory instead of by the
+// registers that per-thread loads must hold until they land, which is what limits the plain
+// kernels on grids larger than L2.  Persistent CTAs walk the tiles with STAGES stages in
+// flight; the CPML memories (frame tiles only), strips, sources and receivers are read per
+// thread as in the plain kernels, and the per-cell arithmetic is theirs term by term, so the
+// results are the same bits.
+// ------------------------------------------------------------------------------------
+constexpr int ST_TX = 8, ST_TZ = 128, ST_MAXBOX = 8;
+
+// Boxes of one stage: box b covers rows z0t + dz[b] .. + rows and columns x0 + dx[b] .. + cols
+// of its tensor map (box extents are fixed in the map) and lands at float offset off[b] of the
+// stage; off[] are multiples of 32 floats (128 bytes).
+struct StageBoxes {
+    int nbox;
+    int dz[ST_MAXBOX], dx[ST_MAXBOX], off[ST_MAXBOX];
+    int stage_floats;
+    unsigned bytes;
+};
+
+// Tile loop of the fully staged kernels; body(x0, z0t, stage) computes one tile.  A wait that
+// gives up is decided by the whole CTA (see vtile_loop): the error word is set, the copies in
+// flight are waited for (bounded), and every thread returns false together.
+template <int STAGES, class Body>
+__device__ __forceinline__ bool stage_loop(const Geo &g, const CUtensorMap *const *maps, const StageBoxes &sb,
+                                           int *err, Body body)
+{
+    extern __shared__ __align__(128) float st_sm[];
+    __shared__ __align__(8) unsigned long long sbar[STAGES];
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int ntz_t = (g.ntz + ST_TZ - 1) / ST_TZ, ntile = ntz_t * ((g.ntx + ST_TX - 1) / ST_TX);
+    auto issue = [&](int t, int s) {
+        const int x0 = (t / ntz_t) * ST_TX, z0 = (t % ntz_t) * ST_TZ;
+        float *st = st_sm + (size_t)s * sb.stage_floats;
+        mbar_expect_tx(&sbar[s], sb.bytes);
+        for (int b = 0; b < sb.nbox; b++) tma_load_2d(st + sb.off[b], maps[b], z0 + sb.dz[b], x0 + sb.dx[b], &sbar[s]);
+    };
+    auto wait_use = [&](int kk) {
+        long long tries = 0;
+        while (!mbar_try_wait(&sbar[kk % STAGES], (kk / STAGES) & 1))
+            if (++tries > VTile<4>::WAIT_TRIES) return false;
+        return true;
+    };
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; s++) mbar_init(&sbar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int s = 0; s < STAGES; s++) {
+            const int t = blockIdx.x + s * gridDim.x;
+            if (t < ntile) issue(t, s);
+        }
+    int k = 0;
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x, k++) {
+        const int s = k % STAGES;
+        if (__syncthreads_or(!wait_use(k))) {
+            if (tid == 0) {
+                atomicExch(err, 1);
+                for (int j = 0; j < STAGES; j++)
+                    if (t + j * gridDim.x < ntile) wait_use(k + j);
+            }
+            __syncthreads();
+            return false;
+        }
+        body((t / ntz_t) * ST_TX, (t % ntz_t) * ST_TZ, st_sm + (size_t)s * sb.stage_floats);
+        __syncthreads();   // every thread is done with stage s before it is refilled
+        if (tid == 0) {
+            const int tn = t + STAGES * gridDim.x;
+            if (tn < ntile) issue(tn, s);
+        }
+    }
+    return true;
+}
+
+// Stage layout of the forward pressure kernel: vx on columns x0-LC .. x0+TX+LC-2 (the x taps),
+// vz on rows z0t-4NB .. z0t+TZ+4NB-1 (the z taps), p and ck on the tile.
+template <int LC>
+struct FwdPStage {
+    static constexpr int NB = (LC + 3) / 4;
+    static constexpr int VXC = ST_TX + 2 * LC - 1, VZR = ST_TZ + 8 * NB;
+    static constexpr int OVX = 0, OVZ = OVX + (VXC * ST_TZ + 31) / 32 * 32, OP = OVZ + (ST_TX * VZR + 31) / 32 * 32,
+                         OCK = OP + ST_TX * ST_TZ, FLOATS = OCK + ST_TX * ST_TZ;
+    static constexpr unsigned BYTES = 4u * (VXC * ST_TZ + ST_TX * VZR + 2 * ST_TX * ST_TZ);
+    static constexpr int STAGES = 3;
+    __host__ __device__ static StageBoxes boxes()
+    {
+        StageBoxes b{};
+        b.nbox = 4;
+        b.dz[0] = 0;      b.dx[0] = -LC; b.off[0] = OVX;   // vx: TZ rows x VXC columns
+        b.dz[1] = -4 * NB; b.dx[1] = 0;  b.off[1] = OVZ;   // vz: VZR rows x TX columns
+        b.dz[2] = 0;      b.dx[2] = 0;   b.off[2] = OP;    // p
+        b.dz[3] = 0;      b.dx[3] = 0;   b.off[3] = OCK;   // ck
+        b.stage_floats = FLOATS;
+        b.bytes = BYTES;
+        return b;
+    }
+};
+
+template <int LC>
+constexpr size_t fwd_p_stage_smem() { return sizeof(float) * FwdPStage<LC>::STAGES * FwdPStage<LC>::FLOATS; }
+
+// Whether the tile (x0.., z0t..) holds a cell of the strip band (block_has_strips for a tile)
+__device__ __forceinline__ bool tile_has_strips(int x0, int z0t, int ntx, int ntz, int pmlc, int Lc)
+{
+    const int x1 = x0 + ST_TX - 1, z1 = z0t + ST_TZ - 1;
+    auto hit = [&](int xa, int xb, int za, int zb) { return x0 <= xb && x1 >= xa && z0t <= zb && z1 >= za; };
+    const int xl = pmlc, xr = ntx - pmlc - 1, zt = pmlc, zb = ntz - pmlc - 1;
+    return hit(xl, xr, zt, zt + Lc - 1) || hit(xl, xr, zb - Lc + 1, zb) || hit(xl, xl + Lc - 1, zt, zb) ||
+           hit(xr - Lc + 1, xr, zt, zb);
+}
+
+// Forward pressure step of one wavefield on a staged tile (k_fwd_p<LC, 1, FP_PLAIN> with every
+// stencil operand read from the stage): the same per-cell arithmetic as p_update4, then the
+// source, the receivers, the kz columns and the strips as k_fwd_p writes them.
+template <int LC>
+__global__ void __launch_bounds__(256) k_fwd_p_staged(const FwdArgs a, const __grid_constant__ CUtensorMap tvx,
+                                                      const __grid_constant__ CUtensorMap tvz,
+                                                      const __grid_constant__ CUtensorMap tp,
+                                                      const __grid_constant__ CUtensorMap tck, int *err)
+{
+    using S = FwdPStage<LC>;
+    const CUtensorMap *maps[4] = {&tvx, &tvz, &tp, &tck};
+    const StageBoxes sb = S::boxes();
+    const Geo &g = a.g;
+    const int it = *a.itp + a.itoff;
+    const Wave w = a.w[0];
+    stage_loop<S::STAGES>(g, maps, sb, err, [&](int x0, int z0t, const float *st) {
+        const int x = x0 + threadIdx.y, z0 = z0t + 4 * threadIdx.x;
+        const bool in = x < g.ntx && z0 < g.ntz;
+        const float *svx = st + S::OVX, *svz = st + S::OVZ + threadIdx.y * S::VZR, *sp = st + S::OP, *sck = st + S::OCK;
+        const int zr = z0 - z0t;   // row of z0 in the tile
+        float4 pn = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (in) {
+            const size_t ip = (size_t)x * g.ldz + z0;
+            const int ntx = g.ntx, ntz = g.ntz;
+            pn = ld4(sp + threadIdx.y * ST_TZ + zr);
+            bool upd[4], any = false;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int z = z0 + k;
+                upd[k] = z >= LC && z <= ntz - LC && x >= LC && x <= ntx - LC;
+                any |= upd[k];
+            }
+            if (any) {
+                float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
+                const Taps<LC> tx(g, g.odx), tz(g, g.odz);
+                ZWin<LC> vw;
+                vw.load(svz + 4 * S::NB, zr);   // row zr of the staged vz column, with its halo
+                // vx column x + c sits at stage column x + c - (x0 - LC)
+                const float *vxc = svx + (size_t)(threadIdx.y + LC) * ST_TZ + zr;
+#pragma unroll
+                for (int ic = 0; ic < LC; ic++) {
+                    const float4 va = ld4(vxc + ic * ST_TZ), vb = ld4(vxc - (ic + 1) * ST_TZ);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        el(dvx, k) += tx.c[ic] * (elc(va, k) - elc(vb, k));
+                        el(dvz, k) += tz.c[ic] * (vw.at(k + ic) - vw.at(k - ic - 1));
+                    }
+                }
+                float4 phx = make_float4(0.f, 0.f, 0.f, 0.f), phz = make_float4(0.f, 0.f, 0.f, 0.f);
+                const float ax = __ldg(a.c.ax + x);
+                if (ax != 0.f) {
+                    const float bx = __ldg(a.c.bx + x);
+                    float4 po = ld4(w.pvx + ip);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        el(phx, k) = bx * elc(po, k) + ax * elc(dvx, k);
+                        if (upd[k]) el(po, k) = elc(phx, k);
+                    }
+                    st4(w.pvx + ip, po);
+                }
+                const float4 az = ldg4(a.c.az + z0);
+                if (az.x != 0.f || az.y != 0.f || az.z != 0.f || az.w != 0.f) {
+                    const float4 bz = ldg4(a.c.bz + z0);
+                    float4 po = ld4(w.pvz + ip);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        el(phz, k) = elc(bz, k) * elc(po, k) + elc(az, k) * elc(dvz, k);
+                        if (upd[k] && elc(az, k) != 0.f) el(po, k) = elc(phz, k);
+                        else el(phz, k) = 0.f;
+                    }
+                    st4(w.pvz + ip, po);
+                }
+                const float4 kc = ld4(sck + threadIdx.y * ST_TZ + zr);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const float sk = elc(dvx, k) + elc(phx, k) + elc(dvz, k) + elc(phz, k);
+                    if (upd[k]) el(pn, k) = elc(kc, k) * sk + elc(pn, k);
+                }
+            }
+            if (x == a.sx) {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (a.sz == z0 + k) { el(pn, k) += a.wav0[it]; any = true; }
+            }
+            if (any) st4(w.p + ip, pn);
+            const int wc = a.seis ? __ldg(a.wells.wcol + x) : -1;
+            if (wc >= 0) {
+                const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * g.ldz + z0));
+                const int t4[4] = {tr.x, tr.y, tr.z, tr.w};
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (t4[k] >= 0 && z0 + k < g.ntz) a.seis[(size_t)t4[k] * a.nt + it] = elc(pn, k);
+                if (a.colmap) {
+                    float2 *cb = a.colbuf + ((size_t)wc * a.nt + it) * g.ldz + z0;
+#pragma unroll
+                    for (int k = 0; k < 4; k++) cb[k] = make_float2(elc(pn, k), elc(pn, k));
+                }
+            }
+        }
+        // strips: uncompressed store, or per-(step, tile) scaled 16-bit codes (tile = plain block)
+        if (a.strips.buf && tile_has_strips(x0, z0t, g.ntx, g.ntz, g.pmlc, LC)) {
+            int si[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) si[k] = (in && z0 + k < g.ntz) ? strip_index(x, z0 + k, g.ntx, g.ntz, g.pmlc, LC) : -1;
+            if (a.strips.prec == 0) {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (si[k] >= 0) ((float *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = elc(pn, k);
+            } else {
+                __shared__ float smax;
+                if (threadIdx.x == 0 && threadIdx.y == 0) smax = 0.f;
+                __syncthreads();
+                float v = 0.f;
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (si[k] >= 0) v = fmaxf(v, fabsf(elc(pn, k)));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+                if (threadIdx.x == 0 && v > 0.f) atomicMax((int *)&smax, __float_as_int(v));
+                __syncthreads();
+                const float mx = smax, inv = enc16_inv(mx);
+                const int slot = (x0 / ST_TX) * ((g.ntz + ST_TZ - 1) / ST_TZ) + z0t / ST_TZ;
+                if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)it * a.strips.nscale + slot] = mx;
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (si[k] >= 0)
+                        ((unsigned short *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = enc16(elc(pn, k), mx, inv, a.strips.prec);
+                __syncthreads();   // smax is read before the next tile resets it
+            }
+        }
+    });
+}
+
+}  // namespace swd

@@ -105,6 +105,7 @@ struct swd_ctx {
     int bwd_by_kind = 1;    // SWD_OPT_BWD_BY_KIND
     int use_tma = 0;        // SWD_OPT_TMA
     int use_pdl = 0;        // SWD_OPT_PDL
+    int use_staged = 0;     // SWD_OPT_STAGED
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -828,6 +829,39 @@ static void launch_bwd_v_tma(const BwdArgs &a, const CUtensorMap &mr, const CUte
     k_bwd_v_tma<LC><<<t.nblk, dim3(32, 8), t.smem, s>>>(a, mr, ms, err);
 }
 
+// launch shape of the fully staged forward pressure kernel (nblk = 0: unusable here)
+template <int LC>
+static void staged_p_prepare(int dev, TmaShape *t)
+{
+    t->nblk = 0;
+    t->smem = fwd_p_stage_smem<LC>();
+    const void *fn = (const void *)k_fwd_p_staged<LC>;
+    int nsm = 0, occ = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, t->smem) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        return;
+    }
+    t->nblk = nsm * occ;
+}
+
+// tensor maps of the staged forward pressure kernel: vx (TZ rows x VXC columns), vz (VZR x TX),
+// p and ck (TZ x TX)
+template <int LC>
+static void staged_p_maps(const swd_ctx *ctx, const FwdArgs &a, CUtensorMap *m, bool *ok)
+{
+    using S = FwdPStage<LC>;
+    *ok = make_pmap(ctx, &m[0], a.w[0].vx, ST_TZ, S::VXC) && make_pmap(ctx, &m[1], a.w[0].vz, S::VZR, ST_TX) &&
+          make_pmap(ctx, &m[2], a.w[0].p, ST_TZ, ST_TX) && make_pmap(ctx, &m[3], a.m.ck, ST_TZ, ST_TX);
+}
+
+template <int LC>
+static void launch_fwd_p_staged(const FwdArgs &a, const CUtensorMap *m, int *err, const TmaShape &t, cudaStream_t s)
+{
+    k_fwd_p_staged<LC><<<t.nblk, dim3(32, 8), t.smem, s>>>(a, m[0], m[1], m[2], m[3], err);
+}
+
 // error word of the TMA kernels (set when a wait on a copy gave up), after the step counter
 static int *tma_err(swd_ctx *ctx) { return I32(ctx->ctrl) + 8; }
 
@@ -836,7 +870,7 @@ static int tma_check(swd_ctx *ctx)
     int h = 0;
     CK(cudaMemcpyAsync(&h, tma_err(ctx), sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (h) return fail(ctx, SWD_ERR_CUDA, "a TMA-staged velocity kernel gave up waiting for its pressure tile");
+    if (h) return fail(ctx, SWD_ERR_CUDA, "a TMA-staged kernel gave up waiting for its tile");
     return SWD_OK;
 }
 
@@ -1108,6 +1142,17 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
         use_tma = tsh.nblk > 0 && make_pmap(ctx, &pmap, a.w[0].p, rows, cols);
         if (use_tma) CK(cudaMemsetAsync(tma_err(ctx), 0, sizeof(int), ctx->stream));
     }
+    // one plain wavefield: the pressure kernel with every stencil operand staged by TMA
+    int use_staged = ctx->use_staged && nw == 1 && !a.ck.every && !a.ds.buf && !a.s0_out && !a.dkappa && !a.dck;
+    CUtensorMap smap[4];
+    TmaShape ssh;
+    if (use_staged) {
+        bool ok = false;
+        LC_DISPATCH(ctx->Lc, staged_p_prepare, ctx->dev, &ssh);
+        if (ssh.nblk > 0) LC_DISPATCH(ctx->Lc, staged_p_maps, ctx, a, smap, &ok);
+        use_staged = ok;
+        if (use_staged) CK(cudaMemsetAsync(tma_err(ctx), 0, sizeof(int), ctx->stream));
+    }
     auto launch = [&](int k, cudaEvent_t *ev) {
         FwdArgs b = a;
         b.itoff = k;
@@ -1118,17 +1163,22 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
             LC_DISPATCH(ctx->Lc, launch_fwd_v, b, nw, grid, ctx->stream, ctx->use_pdl);
         }
         if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
-        LC_DISPATCH(ctx->Lc, launch_fwd_p, b, nw, grid, ctx->stream, ctx->use_pdl);
+        if (use_staged) {
+            LC_DISPATCH(ctx->Lc, launch_fwd_p_staged, b, smap, tma_err(ctx), ssh, ctx->stream);
+        } else {
+            LC_DISPATCH(ctx->Lc, launch_fwd_p, b, nw, grid, ctx->stream, ctx->use_pdl);
+        }
         if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
     };
     const int kid[2] = {0, 1};
     a.itoff = 0;
-    // the TMA choice is part of the captured graph's identity
+    // the TMA choices are part of the captured graph's identity
     std::vector<char> key((const char *)&a, (const char *)&a + sizeof a);
     key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
+    key.insert(key.end(), (const char *)&use_staged, (const char *)&use_staged + sizeof use_staged);
     key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
     CKR(run_steps(ctx, ctx->gfwd, key.data(), key.size(), 0, +1, nt, 2, kid, launch));
-    if (use_tma) CKR(tma_check(ctx));
+    if (use_tma || use_staged) CKR(tma_check(ctx));
     return SWD_OK;
 }
 
@@ -1301,7 +1351,11 @@ static cudaError_t launch_decon_windows(const DeconGeo &g, const float *mig, con
         const size_t sm = sizeof(float2) * ((size_t)g.FX * g.FZ + decon_tab_len(g));
         cudaError_t e = cudaFuncSetAttribute(k_decon_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        k_decon_window<<<g.totalnum, 512, sm, st>>>(g, mig, psf, winout, tabs);
+        // two CTAs of 256 threads per SM where two windows' buffers fit in shared memory (one CTA's
+        // barriers then overlap the other's transforms), else one CTA of 512; a window's result
+        // does not depend on the block size (one warp per transform, order-free maximum)
+        const int nthr = 2 * (sm + 1024) <= 227 * 1024 ? 256 : 512;
+        k_decon_window<<<g.totalnum, nthr, sm, st>>>(g, mig, psf, winout, tabs);
     }
     return cudaGetLastError();
 }

@@ -39,6 +39,7 @@ CASE = dict(nx=1612, nz=801, pml=30, Lc=4, dx=5.0, dz=5.0, itmax=6000, dt=4.0e-4
 def _load(name, path):
     spec = importlib.util.spec_from_file_location(name, path)
     mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod   # dataclasses look their module up while the class is built
     spec.loader.exec_module(mod)
     return mod
 

@@ -16,6 +16,7 @@ CASES = [
     (["--workload", "lsrtm"], "LSRTM gradient shots/s", "shots/s"),
     (["--workload", "batch"], "RTM shots/s", "shots/s"),
     (["--workload", "decon", "--config", "c2"], "decon windows/s", "windows/s"),
+    (["--workload", "c5flow"], "RTM shots/s", "shots/s"),
 ]
 
 

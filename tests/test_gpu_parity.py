@@ -507,6 +507,36 @@ def test_tma_velocity_kernels_same_bits(swd, orc, shape):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("shape", [(100, 60, 10, 4), (123, 97, 9, 4), (77, 141, 12, 1), (90, 75, 10, 7), (64, 48, 8, 8)],
+                         ids=["100x60_Lc4", "123x97_Lc4", "77x141_Lc1", "90x75_Lc7", "64x48_Lc8"])
+@pytest.mark.parametrize("strips", ["f32", "f16"])
+def test_staged_pressure_kernel_same_bits(swd, orc, shape, strips):
+    """The forward pressure kernel with every stencil operand staged by TMA (SWD_OPT_STAGED = 1)
+    against the per-thread loads: forward seismograms, the strips (so the reconstruction) and
+    the raw RTM images identical bit for bit, with FP32
+    and scaled FP16 strips, on grids that are not multiples of the tile and for stencil orders
+    1, 4, 7 and 8; also through the velocity kernel with TMA-staged pressure."""
+    nx, nz, pml, Lc = shape
+    c = Case(swd, orc, nx=nx, nz=nz, pml=pml, Lc=Lc, nt=240, path=0)
+    data = orc.forward(c.M, c.G, c.rick)["seis"]
+    flags = swd.RTM_PREPROCESS | swd.RTM_NO_STACK | swd.RTM_ILLUM_RCV
+    c.E.set_strip_precision({"f32": swd.STRIP_F32, "f16": swd.STRIP_F16}[strips])
+    out = {}
+    for staged, tma in ((0, 0), (1, 0), (1, 1)):
+        c.E.set_option(swd.OPT_STAGED, staged)
+        c.E.set_option(swd.OPT_TMA, tma)
+        seis = c.E.forward(c.shot, c.rick)
+        c.E.rtm_shot(c.shot, c.rick, data, flags=flags, want=())
+        out[(staged, tma)] = (seis,) + tuple(c.E.rtm_raw(rcv=True))
+    c.E.set_option(swd.OPT_STAGED, 0)
+    c.E.set_option(swd.OPT_TMA, 0)
+    ref = out[(0, 0)]
+    assert np.abs(ref[0]).max() > 0 and np.abs(ref[1]).max() > 0
+    for key, got in out.items():
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b), key
+
+
 def test_pdl_launches_same_bits(case, swd, orc):
     """RTM step kernels as programmatic dependent launches (SWD_OPT_PDL = 1) against plain
     stream order (the default), with CUDA graphs and with host launches, reconstructing and
