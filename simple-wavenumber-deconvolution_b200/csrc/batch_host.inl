@@ -329,6 +329,14 @@ int swd_set_option(swd_ctx *ctx, int option, int value)
             if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_STAGED takes 0 or 1");
             ctx->use_staged = value;
             return SWD_OK;
+        case SWD_OPT_AUTOTUNE:
+            if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_AUTOTUNE takes 0 or 1");
+            ctx->autotune = value;
+            // forward: bit 1 TMA-staged velocity launch, bit 2 fully staged pressure launch;
+            // backward: bit 1 TMA-staged velocity launch, bit 4 the reference's pairing
+            tune_reset(ctx->tfwd, {0, 1, 2, 3});
+            tune_reset(ctx->tbwd, {0, 1, 4});
+            return SWD_OK;
         default:
             return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
@@ -346,6 +354,9 @@ int swd_get_option(swd_ctx *ctx, int option, int *value)
         case SWD_OPT_TMA: *value = ctx->use_tma; return SWD_OK;
         case SWD_OPT_PDL: *value = ctx->use_pdl; return SWD_OK;
         case SWD_OPT_STAGED: *value = ctx->use_staged; return SWD_OK;
+        case SWD_OPT_AUTOTUNE: *value = ctx->autotune; return SWD_OK;
+        case SWD_OPT_TUNED_FWD: *value = ctx->autotune && ctx->tfwd.choice >= 0 ? ctx->tfwd.cand[ctx->tfwd.choice] : -1; return SWD_OK;
+        case SWD_OPT_TUNED_BWD: *value = ctx->autotune && ctx->tbwd.choice >= 0 ? ctx->tbwd.cand[ctx->tbwd.choice] : -1; return SWD_OK;
         default: return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
 }

@@ -10,6 +10,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <algorithm>
+#include <initializer_list>
 #include <cmath>
 #include <string>
 #include <utility>
@@ -106,6 +107,15 @@ struct swd_ctx {
     int use_tma = 0;        // SWD_OPT_TMA
     int use_pdl = 0;        // SWD_OPT_PDL
     int use_staged = 0;     // SWD_OPT_STAGED
+    // SWD_OPT_AUTOTUNE: the step-kernel variants of a pass (all give the same bits) are tried on
+    // successive passes, each timed over its graph replays, and the fastest is kept
+    struct PassTune {
+        int cand[8] = {0};
+        double ms[8] = {0};
+        int ncand = 0, next = 0, choice = -1;
+    };
+    int autotune = 0;
+    PassTune tfwd, tbwd;
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -996,6 +1006,26 @@ static void graph_free(swd_ctx::StepGraph &G)
     G = swd_ctx::StepGraph();
 }
 
+// variant of the next pass of a tuner: the chosen one, else the next one to try
+static int tune_pick(const swd_ctx::PassTune &T) { return T.choice >= 0 ? T.cand[T.choice] : T.cand[T.next]; }
+
+static void tune_record(swd_ctx::PassTune &T, double ms_per_step)
+{
+    if (T.choice >= 0) return;
+    T.ms[T.next++] = ms_per_step;
+    if (T.next < T.ncand) return;
+    int best = 0;
+    for (int i = 1; i < T.ncand; i++)
+        if (T.ms[i] < T.ms[best]) best = i;
+    T.choice = best;
+}
+
+static void tune_reset(swd_ctx::PassTune &T, std::initializer_list<int> cands)
+{
+    T = swd_ctx::PassTune();
+    for (int c : cands) T.cand[T.ncand++] = c;
+}
+
 template <class Launch>
 static int capture_chunk(swd_ctx *ctx, cudaGraphExec_t *out, int dir, int *counter, Launch launch, cudaEvent_t *ev,
                          int klen)
@@ -1015,9 +1045,12 @@ static int capture_chunk(swd_ctx *ctx, cudaGraphExec_t *out, int dir, int *count
 // Launch(k, ev): enqueue step k (itoff = dir*k) on ctx->stream; when ev != nullptr record
 // ev[2j] / ev[2j+1] around its j-th kernel.  nk kernels per step with profiling ids kid[].
 // Chunks hold klen steps (the key of the captured graph includes it).
+// pass_ms: when given, the pass's replays (captures excluded) are timed with events and the
+// milliseconds returned there (the stream is synchronised for it).
 template <class Launch>
 static int run_steps(swd_ctx *ctx, swd_ctx::StepGraph &G, const void *key, size_t keylen, int start, int dir,
-                     int nsteps, int nk, const int *kid, Launch launch, int klen = GRAPH_K, int pass_id = -1)
+                     int nsteps, int nk, const int *kid, Launch launch, int klen = GRAPH_K, int pass_id = -1,
+                     float *pass_ms = nullptr)
 {
     CKR(ensure(ctx, ctx->ctrl, 64));
     int *counter = I32(ctx->ctrl);
@@ -1042,6 +1075,13 @@ static int run_steps(swd_ctx *ctx, swd_ctx::StepGraph &G, const void *key, size_
         }
     }
     const int pc = prof && nchunks > 0 ? nchunks / 2 : -1;   // the chunk that carries the probe events
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (pass_ms) {
+        t0 = ev_get(ctx);
+        t1 = ev_get(ctx);
+        if (!t0 || !t1) return fail(ctx, SWD_ERR_CUDA, "no timing events");
+        CK(cudaEventRecord(t0, ctx->stream));
+    }
     {
         // whole-pass time per step (profiling ids 6 forward, 7 backward)
         ProfScope pass(ctx, pass_id >= 0 ? pass_id : (dir > 0 ? 6 : 7), prof, nsteps);
@@ -1055,6 +1095,11 @@ static int run_steps(swd_ctx *ctx, swd_ctx::StepGraph &G, const void *key, size_
         }
     }
     CK(cudaGetLastError());
+    if (pass_ms) {
+        CK(cudaEventRecord(t1, ctx->stream));
+        CK(cudaEventSynchronize(t1));
+        CK(cudaEventElapsedTime(pass_ms, t0, t1));
+    }
     if (pc >= 0) {
         // the probe step sits mid-chunk between busy neighbours; read it once the pass drained
         CK(cudaStreamSynchronize(ctx->stream));
@@ -1132,7 +1177,12 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     a.wav1 = J.twin ? F(ctx->wav) + nt : F(ctx->wav);
     const int nw = J.twin ? 2 : 1;
     // one wavefield without checkpoints: the velocity kernel with TMA-staged pressure
-    int use_tma = ctx->use_tma && nw == 1 && !a.ck.every;
+    // the plain single-wavefield forward (RTM forward, modelling without a twin): variants of the
+    // velocity and pressure launches, chosen by the tuner when SWD_OPT_AUTOTUNE is on
+    const bool plain1 = nw == 1 && !a.ck.every && !a.ds.buf && !a.s0_out && !a.dkappa && !a.dck;
+    const bool tune = ctx->autotune && plain1;
+    const int fv = tune ? tune_pick(ctx->tfwd) : ((ctx->use_tma ? 1 : 0) | (ctx->use_staged ? 2 : 0));
+    int use_tma = (fv & 1) && nw == 1 && !a.ck.every;
     CUtensorMap pmap;
     TmaShape tsh;
     if (use_tma) {
@@ -1143,7 +1193,7 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
         if (use_tma) CK(cudaMemsetAsync(tma_err(ctx), 0, sizeof(int), ctx->stream));
     }
     // one plain wavefield: the pressure kernel with every stencil operand staged by TMA
-    int use_staged = ctx->use_staged && nw == 1 && !a.ck.every && !a.ds.buf && !a.s0_out && !a.dkappa && !a.dck;
+    int use_staged = (fv & 2) && plain1;
     CUtensorMap smap[4];
     TmaShape ssh;
     if (use_staged) {
@@ -1177,8 +1227,12 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
     key.insert(key.end(), (const char *)&use_staged, (const char *)&use_staged + sizeof use_staged);
     key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
-    CKR(run_steps(ctx, ctx->gfwd, key.data(), key.size(), 0, +1, nt, 2, kid, launch));
+    float pass_ms = 0.f;
+    const bool timing = tune && ctx->tfwd.choice < 0;
+    CKR(run_steps(ctx, ctx->gfwd, key.data(), key.size(), 0, +1, nt, 2, kid, launch, GRAPH_K, -1,
+                  timing ? &pass_ms : nullptr));
     if (use_tma || use_staged) CKR(tma_check(ctx));
+    if (timing) tune_record(ctx->tfwd, pass_ms / nt);
     return SWD_OK;
 }
 
@@ -1948,9 +2002,13 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         }
         // phases paired by kind (k_bwd_v + k_bwd_p) unless the angle gathers need the source
         // velocities of every step (k_bwd_1 + k_bwd_2, the reference's pairing)
-        const int by_kind = ctx->bwd_by_kind && !want_cig;
+        // the variants (by-kind pairing with plain or TMA velocities, the reference's pairing)
+        // chosen by the tuner when SWD_OPT_AUTOTUNE is on
+        const bool tune = ctx->autotune && !want_cig;
+        const int bv = tune ? tune_pick(ctx->tbwd) : ((ctx->use_tma ? 1 : 0) | (ctx->bwd_by_kind ? 0 : 4));
+        const int by_kind = !(bv & 4) && !want_cig;
         // velocities of both wavefields with TMA-staged pressures
-        int use_tma = by_kind && ctx->use_tma;
+        int use_tma = by_kind && (bv & 1);
         CUtensorMap pmap_r, pmap_s;
         TmaShape tsh;
         if (use_tma) {
@@ -1992,8 +2050,12 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         key.insert(key.end(), (const char *)&by_kind, (const char *)&by_kind + sizeof by_kind);
         key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
         key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
-        CKR(run_steps(ctx, ctx->gbwd, key.data(), key.size(), nt - 2, -1, nt - 1, 2, kid, launch));
+        float pass_ms = 0.f;
+        const bool timing = tune && ctx->tbwd.choice < 0;
+        CKR(run_steps(ctx, ctx->gbwd, key.data(), key.size(), nt - 2, -1, nt - 1, 2, kid, launch, GRAPH_K, -1,
+                      timing ? &pass_ms : nullptr));
         if (use_tma) CKR(tma_check(ctx));
+        if (timing) tune_record(ctx->tbwd, pass_ms / (nt - 1));
         ctx->have_cig = want_cig;
     }
     CK(cudaGetLastError());
