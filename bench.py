@@ -276,6 +276,8 @@ def run_ours(args, rank, world, dist):
         E.set_option(swd.OPT_PDL, 1)
     if args.staged:
         E.set_option(swd.OPT_STAGED, 1)
+    if args.autotune:
+        E.set_option(swd.OPT_AUTOTUNE, 1)
     if args.path is not None:
         E.set_kernel_path(args.path)
     strips = w.extra.get("strips", "f32")
@@ -308,6 +310,11 @@ def run_ours(args, rank, world, dist):
 
     def timed(dd, rk, img, fim, K, W, profile=False):
         for _ in range(W):
+            step(dd, rk, img, fim)
+        # with the autotuner on, its tries all happen before the timed shots
+        for _ in range(8):
+            if not args.autotune or min(E.get_option(swd.OPT_TUNED_FWD), E.get_option(swd.OPT_TUNED_BWD)) >= 0:
+                break
             step(dd, rk, img, fim)
         if profile:
             E.profile(8)
@@ -409,7 +416,10 @@ def run_ours(args, rank, world, dist):
         "vs_baseline": None, "dtype": "f32 (FP64 imaging)", "data": "synthetic (seeded random-field model, PSF data)",
         "config": {"workload": WORKLOADS[args.config], "parallelism": f"replicas x{world}",
                    "l2": "flushed (256 MiB write) before every timed step", "strips": strips,
-                   "options": {"staged_p": int(E.get_option(swd.OPT_STAGED)), "tma_v": int(E.get_option(swd.OPT_TMA))}},
+                   "options": {"staged_p": int(E.get_option(swd.OPT_STAGED)), "tma_v": int(E.get_option(swd.OPT_TMA)),
+                               "autotune": int(E.get_option(swd.OPT_AUTOTUNE)),
+                               "tuned_fwd": int(E.get_option(swd.OPT_TUNED_FWD)),
+                               "tuned_bwd": int(E.get_option(swd.OPT_TUNED_BWD))}},
         "gcell_updates_per_s": value * cells_per_shot / 1e9,
         "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(data.nbytes + rick.nbytes),
                 "d2h_bytes_per_step": int(2 * w.nx * w.nz * 4)},
@@ -434,6 +444,38 @@ def run_ours(args, rank, world, dist):
 PARITY_TOL = 1e-3   # the metric's accuracy condition: image rel-L2 against FP64
 
 
+def oracle_rtm(w, shot, rick, data, nt):
+    """The FP64 oracle's RTM of a shot's first nt steps (the reference's strip reconstruction,
+    imaging, normalisation and -vp^2 Laplacian in double): raw image, illumination, filtered
+    image and the host seconds it took."""
+    orc = load_oracle()
+    t = time.perf_counter()
+    M, _ = oracle_model(orc, w, w.vp_mig, nt)
+    G = orc.Geom(shot.s_ix, shot.s_iz, shot.r_ix, shot.r_iz)
+    ref = orc.rtm_shot(M, G, np.ascontiguousarray(rick[:nt]), np.ascontiguousarray(data[:, :nt]), dtype=np.float64)
+    _, fim = orc.rtm_post(M, ref["img"], ref["illum"], np.float64)
+    return ref["img"], ref["illum"], fim, time.perf_counter() - t
+
+
+def engine_vs_oracle(swd, E, shot, rick, data, nt, ref):
+    """Relative L2 of the engine's raw image, illumination and filtered image of the same shot,
+    record and inputs against oracle_rtm's; None where the FP64 image is zero (no signal yet)."""
+    sh = swd.ShotSpec(shot.s_ix, shot.s_iz, shot.r_ix, shot.r_iz, nt)
+    out = E.rtm_shot(sh, np.ascontiguousarray(rick[:nt]), np.ascontiguousarray(data[:, :nt]),
+                     flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK, want=("fimage",))
+    I, S, _ = E.rtm_raw()
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / nb) if nb > 0 else None
+    res = {"image_rel_l2": rel(I, ref[0]), "illum_rel_l2": rel(S, ref[1]), "fimage_rel_l2": rel(out["fimage"], ref[2]),
+           "tolerance": PARITY_TOL}
+    errs = [res["image_rel_l2"], res["illum_rel_l2"], res["fimage_rel_l2"]]
+    # a record too short for the data to reach the receivers leaves the image zero: no verdict
+    res["pass"] = None if None in errs else max(errs) <= PARITY_TOL
+    return res
+
+
 def fp64_parity(swd, E, w, shot, rick, data, nt=None):
     """The metric's accuracy condition, checked outside every timed region: one more RTM shot of
     the benchmark (same engine, options and inputs; imaging without stacking) against the FP64
@@ -441,30 +483,14 @@ def fp64_parity(swd, E, w, shot, rick, data, nt=None):
     illumination normalisation and -vp^2 Laplacian, all in double) on the host cores.  Relative
     L2 errors of the raw image I, the source illumination S and the filtered image.  nt < the
     shot's record runs both on the first nt steps (stated in the result)."""
-    orc = load_oracle()
     nt = shot.nt if nt is None else min(nt, shot.nt)
-    sh = swd.ShotSpec(shot.s_ix, shot.s_iz, shot.r_ix, shot.r_iz, nt)
-    rk = np.ascontiguousarray(rick[:nt])
-    dd = np.ascontiguousarray(data[:, :nt])
-    out = E.rtm_shot(sh, rk, dd, flags=swd.RTM_PREPROCESS | swd.RTM_NO_STACK, want=("fimage",))
-    I, S, _ = E.rtm_raw()
-    t = time.perf_counter()
-    M, _ = oracle_model(orc, w, w.vp_mig, nt)
-    G = orc.Geom(sh.s_ix, sh.s_iz, sh.r_ix, sh.r_iz)
-    ref = orc.rtm_shot(M, G, rk, dd, dtype=np.float64)
-    _, fim = orc.rtm_post(M, ref["img"], ref["illum"], np.float64)
-    t = time.perf_counter() - t
-    def rel(a, b):
-        nb = float(np.linalg.norm(b))
-        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / nb) if nb > 0 else None
+    ref = oracle_rtm(w, shot, rick, data, nt)
     res = {"reference": "FP64 CPU oracle (oracle/), the reference's reconstruction and imaging in double",
            "nt": nt, "record": "full" if nt == shot.nt else f"first {nt} of {shot.nt} steps",
-           "receivers": len(sh.r_ix), "image_rel_l2": rel(I, ref["img"]), "illum_rel_l2": rel(S, ref["illum"]),
-           "fimage_rel_l2": rel(out["fimage"], fim), "tolerance": PARITY_TOL,
-           "oracle_s": round(t, 1), "oracle_threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))}
-    errs = [res["image_rel_l2"], res["illum_rel_l2"], res["fimage_rel_l2"]]
-    # a record too short for the data to reach the receivers leaves the image zero: no verdict
-    res["pass"] = None if None in errs else max(errs) <= PARITY_TOL
+           "receivers": len(shot.r_ix)}
+    res.update(engine_vs_oracle(swd, E, shot, rick, data, nt, ref))
+    res["oracle_s"] = round(ref[3], 1)
+    res["oracle_threads"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return res
 
 
@@ -1177,9 +1203,16 @@ def run_c5flow(args, rank, world, dist):
         e_dec = float(np.linalg.norm(dec - odec) / np.linalg.norm(odec))
         # shot 1 over the first pnt steps: its RTM image (observed data) and PSF image (PSF data)
         par = {"deconvolved_image_vs_oracle_decon_of_the_same_images": e_dec, "shot": i0 + 1}
+        # the shot's images with the flow's FP16 strips, and with int16 and FP32 strips for scale,
+        # against one FP64 oracle run per record
+        precs = {"f16": swd.STRIP_F16, "i16": swd.STRIP_I16, "f32": swd.STRIP_F32}
         for name, rec in (("image", obs[i0]), ("psf_image", psf_data[i0])):
-            r = fp64_parity(swd, E, w, shots[i0], rick, rec, nt=pnt)
-            par[name] = {k: r[k] for k in ("image_rel_l2", "illum_rel_l2", "fimage_rel_l2", "record", "pass")}
+            ref = oracle_rtm(w, shots[i0], rick, rec, pnt)
+            par[name] = {}
+            for pname, pv in precs.items():
+                E.set_strip_precision(pv)
+                par[name][pname + "_strips"] = engine_vs_oracle(swd, E, shots[i0], rick, rec, pnt, ref)
+            E.set_strip_precision(swd.STRIP_F16)
         # the PSF data themselves: the exact scattered field against the FP64 difference of two records
         M0, _ = oracle_model(orc, w, w.vp_mig, pnt)
         M1 = orc.Model(vs, rho, orc.cpml(w.ntx, w.ntz, p, w.dx, w.dz, w.dt), orc.cal_xishu(w.Lc), p, w.Lc, pnt,
@@ -1420,6 +1453,8 @@ def main():
                     help="record length of the FP64 check (0: the whole record; --workload c5flow: 2000 steps)")
     ap.add_argument("--tma", action="store_true", help="velocity kernels with TMA-staged pressure tiles (SWD_OPT_TMA)")
     ap.add_argument("--pdl", action="store_true", help="step kernels as programmatic dependent launches (SWD_OPT_PDL)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="the passes choose their step-kernel variants by timing (SWD_OPT_AUTOTUNE)")
     ap.add_argument("--staged", action="store_true",
                     help="forward pressure kernel with every stencil operand staged by TMA (SWD_OPT_STAGED)")
     ap.add_argument("--streams", type=int, default=3,

@@ -259,10 +259,11 @@ __global__ void __launch_bounds__(256) k_fwd_step(FStepArgs a)
         const int x = x0 + cc, z = z0 + rr;
         if (x >= g.ntx || z >= g.ntz) continue;
         const float p0 = sPn[0][cc * TZ + rr];
-        const int wc = __ldg(a.wells.wcol + x);
+        // seis == nullptr: no record wanted (the RTM forward pass when no synthetic is asked for)
+        const int wc = (a.seis || a.colmap) ? __ldg(a.wells.wcol + x) : -1;
         if (wc >= 0) {
             const int tr = __ldg(a.wells.wmap + (size_t)wc * g.ldz + z);
-            if (tr >= 0) a.seis[(size_t)tr * a.nt + it] = p0;
+            if (tr >= 0 && a.seis) a.seis[(size_t)tr * a.nt + it] = p0;
             if (a.colmap) a.colbuf[((size_t)wc * a.nt + it) * g.ldz + z] = make_float2(p0, sPn[NW - 1][cc * TZ + rr]);
         }
         if (a.strips.buf) {

@@ -190,59 +190,101 @@ struct StageBoxes {
     unsigned bytes;
 };
 
-// Tile loop of the fully staged kernels; body(x0, z0t, stage) computes one tile.  A wait that
-// gives up is decided by the whole CTA (see vtile_loop): the error word is set, the copies in
-// flight are waited for (bounded), and every thread returns false together.
+// Warp-specialised tile pipeline of the fully staged kernels.  The CTA is ST_CONS consumer
+// warps (threadIdx.y = 0 .. ST_CONS-1, the tile's columns) and one producer warp (threadIdx.y ==
+// ST_CONS).  Per stage s two mbarriers: full[s] completes when the stage's boxes have landed
+// (expect_tx by the producer), empty[s] when all consumer warps are done with it (one arrive per
+// warp).  The producer refills a stage as soon as it is empty, so no block-wide barrier stands
+// between a tile's compute and the next copy.  body(x0, z0t, stage) runs on the consumers; a
+// barrier it needs among them is cons_sync() (named barrier 1).
+// Bounded waits: a wait that gives up sets the error word and a shared abort flag, which every
+// other wait checks; the consumers take the decision to stop together (a vote on named barrier 1
+// after each wait, so none is left inside body's barriers), and the producer, once it stops
+// issuing, waits (bounded) for the copies it issued into stages not yet consumed, so the CTA does
+// not exit under its own bulk copies.
+constexpr int ST_CONS = 8;
+
+__device__ __forceinline__ void cons_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+// true when p holds on any consumer thread (all consumers call it)
+__device__ __forceinline__ bool cons_any(bool p)
+{
+    unsigned r;
+    asm volatile("{\n .reg .pred q, o;\n setp.ne.u32 q, %1, 0;\n barrier.red.or.pred o, 1, 256, q;\n selp.u32 %0, 1, 0, o;\n}"
+                 : "=r"(r) : "r"((unsigned)p) : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
 template <int STAGES, class Body>
-__device__ __forceinline__ bool stage_loop(const Geo &g, const CUtensorMap *const *maps, const StageBoxes &sb,
-                                           int *err, Body body)
+__device__ __forceinline__ void stage_loop_ws(const Geo &g, const CUtensorMap *const *maps, const StageBoxes &sb,
+                                              int *err, Body body)
 {
     extern __shared__ __align__(128) float st_sm[];
-    __shared__ __align__(8) unsigned long long sbar[STAGES];
-    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    __shared__ __align__(8) unsigned long long full[STAGES], empty[STAGES];
+    __shared__ int abort_flag;
+    const int warp = threadIdx.y, lane = threadIdx.x;
     const int ntz_t = (g.ntz + ST_TZ - 1) / ST_TZ, ntile = ntz_t * ((g.ntx + ST_TX - 1) / ST_TX);
-    auto issue = [&](int t, int s) {
-        const int x0 = (t / ntz_t) * ST_TX, z0 = (t % ntz_t) * ST_TZ;
-        float *st = st_sm + (size_t)s * sb.stage_floats;
-        mbar_expect_tx(&sbar[s], sb.bytes);
-        for (int b = 0; b < sb.nbox; b++) tma_load_2d(st + sb.off[b], maps[b], z0 + sb.dz[b], x0 + sb.dx[b], &sbar[s]);
+    volatile int *ab = &abort_flag;
+    auto give_up = [&]() {
+        atomicExch(err, 1);
+        *ab = 1;
     };
-    auto wait_use = [&](int kk) {
+    // bounded wait; stops early once another wait gave up (unless drain)
+    auto wait = [&](unsigned long long *b, unsigned parity, bool drain) {
         long long tries = 0;
-        while (!mbar_try_wait(&sbar[kk % STAGES], (kk / STAGES) & 1))
-            if (++tries > VTile<4>::WAIT_TRIES) return false;
+        while (!mbar_try_wait(b, parity)) {
+            if (!drain && *ab) return false;
+            if (++tries > VTile<4>::WAIT_TRIES) {
+                give_up();
+                return false;
+            }
+        }
         return true;
     };
-    if (tid == 0) {
-        for (int s = 0; s < STAGES; s++) mbar_init(&sbar[s], 1);
+    if (warp == 0 && lane == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], ST_CONS);
+        }
+        abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0)
-        for (int s = 0; s < STAGES; s++) {
-            const int t = blockIdx.x + s * gridDim.x;
-            if (t < ntile) issue(t, s);
+    if (warp == ST_CONS) {   // producer
+        if (lane != 0) return;
+        int k = 0;
+        for (int t = blockIdx.x; t < ntile; t += gridDim.x, k++) {
+            const int s = k % STAGES;
+            if (k >= STAGES && !wait(&empty[s], ((k / STAGES) - 1) & 1, false)) break;
+            const int x0 = (t / ntz_t) * ST_TX, z0 = (t % ntz_t) * ST_TZ;
+            float *st = st_sm + (size_t)s * sb.stage_floats;
+            mbar_expect_tx(&full[s], sb.bytes);
+            for (int b = 0; b < sb.nbox; b++)
+                tma_load_2d(st + sb.off[b], maps[b], z0 + sb.dz[b], x0 + sb.dx[b], &full[s]);
         }
+        if (*ab) {
+            // the last use j of each stage that was issued: wait for its copies to land
+            for (int j = k - 1; j >= 0 && j >= k - STAGES; j--) wait(&full[j % STAGES], (j / STAGES) & 1, true);
+        }
+        return;
+    }
     int k = 0;
     for (int t = blockIdx.x; t < ntile; t += gridDim.x, k++) {
         const int s = k % STAGES;
-        if (__syncthreads_or(!wait_use(k))) {
-            if (tid == 0) {
-                atomicExch(err, 1);
-                for (int j = 0; j < STAGES; j++)
-                    if (t + j * gridDim.x < ntile) wait_use(k + j);
-            }
-            __syncthreads();
-            return false;
+        const bool ok = wait(&full[s], (k / STAGES) & 1, false);
+        if (cons_any(!ok)) {
+            if (warp == 0 && lane == 0) give_up();
+            return;
         }
         body((t / ntz_t) * ST_TX, (t % ntz_t) * ST_TZ, st_sm + (size_t)s * sb.stage_floats);
-        __syncthreads();   // every thread is done with stage s before it is refilled
-        if (tid == 0) {
-            const int tn = t + STAGES * gridDim.x;
-            if (tn < ntile) issue(tn, s);
-        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
     }
-    return true;
 }
 
 // Stage layout of the forward pressure kernel: vx on columns x0-LC .. x0+TX+LC-2 (the x taps),
@@ -286,7 +328,7 @@ __device__ __forceinline__ bool tile_has_strips(int x0, int z0t, int ntx, int nt
 // stencil operand read from the stage): the same per-cell arithmetic as p_update4, then the
 // source, the receivers, the kz columns and the strips as k_fwd_p writes them.
 template <int LC>
-__global__ void __launch_bounds__(256) k_fwd_p_staged(const FwdArgs a, const __grid_constant__ CUtensorMap tvx,
+__global__ void __launch_bounds__(32 * (ST_CONS + 1)) k_fwd_p_staged(const FwdArgs a, const __grid_constant__ CUtensorMap tvx,
                                                       const __grid_constant__ CUtensorMap tvz,
                                                       const __grid_constant__ CUtensorMap tp,
                                                       const __grid_constant__ CUtensorMap tck, int *err)
@@ -297,11 +339,12 @@ __global__ void __launch_bounds__(256) k_fwd_p_staged(const FwdArgs a, const __g
     const Geo &g = a.g;
     const int it = *a.itp + a.itoff;
     const Wave w = a.w[0];
-    stage_loop<S::STAGES>(g, maps, sb, err, [&](int x0, int z0t, const float *st) {
+    stage_loop_ws<S::STAGES>(g, maps, sb, err, [&](int x0, int z0t, const float *st) {
         const int x = x0 + threadIdx.y, z0 = z0t + 4 * threadIdx.x;
         const bool in = x < g.ntx && z0 < g.ntz;
         const float *svx = st + S::OVX, *svz = st + S::OVZ + threadIdx.y * S::VZR, *sp = st + S::OP, *sck = st + S::OCK;
         const int zr = z0 - z0t;   // row of z0 in the tile
+        const int wc = (in && a.seis) ? __ldg(a.wells.wcol + x) : -1;
         float4 pn = make_float4(0.f, 0.f, 0.f, 0.f);
         if (in) {
             const size_t ip = (size_t)x * g.ldz + z0;
@@ -367,7 +410,6 @@ __global__ void __launch_bounds__(256) k_fwd_p_staged(const FwdArgs a, const __g
                     if (a.sz == z0 + k) { el(pn, k) += a.wav0[it]; any = true; }
             }
             if (any) st4(w.p + ip, pn);
-            const int wc = a.seis ? __ldg(a.wells.wcol + x) : -1;
             if (wc >= 0) {
                 const int4 tr = __ldg(reinterpret_cast<const int4 *>(a.wells.wmap + (size_t)wc * g.ldz + z0));
                 const int t4[4] = {tr.x, tr.y, tr.z, tr.w};
@@ -393,7 +435,7 @@ __global__ void __launch_bounds__(256) k_fwd_p_staged(const FwdArgs a, const __g
             } else {
                 __shared__ float smax;
                 if (threadIdx.x == 0 && threadIdx.y == 0) smax = 0.f;
-                __syncthreads();
+                cons_sync();
                 float v = 0.f;
 #pragma unroll
                 for (int k = 0; k < 4; k++)
@@ -401,7 +443,7 @@ __global__ void __launch_bounds__(256) k_fwd_p_staged(const FwdArgs a, const __g
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
                 if (threadIdx.x == 0 && v > 0.f) atomicMax((int *)&smax, __float_as_int(v));
-                __syncthreads();
+                cons_sync();
                 const float mx = smax, inv = enc16_inv(mx);
                 const int slot = (x0 / ST_TX) * ((g.ntz + ST_TZ - 1) / ST_TZ) + z0t / ST_TZ;
                 if (threadIdx.x == 0 && threadIdx.y == 0) a.strips.scale[(size_t)it * a.strips.nscale + slot] = mx;
@@ -409,7 +451,7 @@ __global__ void __launch_bounds__(256) k_fwd_p_staged(const FwdArgs a, const __g
                 for (int k = 0; k < 4; k++)
                     if (si[k] >= 0)
                         ((unsigned short *)a.strips.buf)[(size_t)it * a.strips.slen + si[k]] = enc16(elc(pn, k), mx, inv, a.strips.prec);
-                __syncthreads();   // smax is read before the next tile resets it
+                cons_sync();   // smax is read before a later strip tile resets it
             }
         }
     });

@@ -849,7 +849,8 @@ static void staged_p_prepare(int dev, TmaShape *t)
     int nsm = 0, occ = 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, t->smem) != cudaSuccess || occ < 1) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * (ST_CONS + 1), t->smem) != cudaSuccess ||
+        occ < 1) {
         cudaGetLastError();
         return;
     }
@@ -869,7 +870,7 @@ static void staged_p_maps(const swd_ctx *ctx, const FwdArgs &a, CUtensorMap *m, 
 template <int LC>
 static void launch_fwd_p_staged(const FwdArgs &a, const CUtensorMap *m, int *err, const TmaShape &t, cudaStream_t s)
 {
-    k_fwd_p_staged<LC><<<t.nblk, dim3(32, 8), t.smem, s>>>(a, m[0], m[1], m[2], m[3], err);
+    k_fwd_p_staged<LC><<<t.nblk, dim3(32, ST_CONS + 1), t.smem, s>>>(a, m[0], m[1], m[2], m[3], err);
 }
 
 // error word of the TMA kernels (set when a wait on a copy gave up), after the step counter
@@ -1834,9 +1835,13 @@ static int rtm_forward_part(swd_ctx *ctx, const swd_shot *shot, const float *ric
     const bool stored = ctx->src_store != 0;
     J.save_strips = !stored;
     if (stored) CKR(dp_store_layout(ctx, nt, &J.ds));
-    CKR(ensure(ctx, ctx->seis, sizeof(float) * ntr));
-    CK(cudaMemsetAsync(ctx->seis.p, 0, sizeof(float) * ntr, ctx->stream));
-    J.seis_dev = F(ctx->seis);
+    // the synthetic record is formed only when the caller asks for it (the backward pass uses
+    // the observed data)
+    if (syn) {
+        CKR(ensure(ctx, ctx->seis, sizeof(float) * ntr));
+        CK(cudaMemsetAsync(ctx->seis.p, 0, sizeof(float) * ntr, ctx->stream));
+        J.seis_dev = F(ctx->seis);
+    }
     CKR(run_forward(ctx, J, P));
     if (syn) {
         CKR(copy_aliases(ctx, P, F(ctx->seis), nt));
