@@ -193,8 +193,12 @@ __device__ void decon_iterate(const DeconGeo &g, float2 *Z, const DeconIter &it,
 }
 
 // Sum of |Z[(ox + ixx)*FZ + oz + izz]| (component x, or y when Y) over ixx < nxw, izz < nzw,
-// in that order, into a float through double additions (the reference's accumulation).  The
-// chain of additions is serial; loads are issued eight at a time ahead of it.
+// in that order, into a float: the reference's accumulation acc = (float)((double)acc + |v|).
+// That is computed here as one correctly rounded float addition, which gives the same bits: the
+// sum of two floats rounded to double and then to float equals the sum rounded to float once,
+// because double carries more than twice float's precision plus two bits (53 >= 2*24 + 2; double
+// rounding is innocuous for a single addition).  The chain of additions is serial; loads are
+// issued eight at a time ahead of it.
 template <bool Y>
 __device__ float l1_serial(const float2 *Z, int FZ, int ox, int oz, int nxw, int nzw)
 {
@@ -207,9 +211,9 @@ __device__ float l1_serial(const float2 *Z, int FZ, int ox, int oz, int nxw, int
 #pragma unroll
             for (int k = 0; k < 8; k++) v[k] = Y ? row[izz + k].y : row[izz + k].x;
 #pragma unroll
-            for (int k = 0; k < 8; k++) acc = (float)((double)acc + fabs((double)v[k]));
+            for (int k = 0; k < 8; k++) acc = __fadd_rn(acc, fabsf(v[k]));
         }
-        for (; izz < nzw; izz++) acc = (float)((double)acc + fabs((double)(Y ? row[izz].y : row[izz].x)));
+        for (; izz < nzw; izz++) acc = __fadd_rn(acc, fabsf(Y ? row[izz].y : row[izz].x));
     }
     return acc;
 }

@@ -242,6 +242,27 @@ def test_decon_workspace_variant_same_bits(swd):
     assert np.array_equal(a, b) and np.array_equal(ca, cb)
 
 
+@pytest.mark.parametrize("nx,nz,psf,flt,snap,fft_n", [
+    (300, 260, (31, 31), (71, 71), (11, 11), (128, 128)),   # padded to 128: the radix-2 path
+    (120, 100, (5, 5), (11, 11), (3, 3), (0, 0)),           # 15-point transforms: Bluestein through 32
+    (160, 150, (9, 7), (25, 19), (5, 4), (0, 0)),           # 33 x 25: 64- and 128-point, two lengths
+    (600, 500, (41, 41), (241, 241), (60, 60), (0, 0)),     # 281-point: 1024, the largest register width
+], ids=["pow2-128", "L15", "L33x25", "L281"])
+def test_decon_transform_lengths_match_oracle(swd, orc, nx, nz, psf, flt, snap, fft_n):
+    """The window transforms at the register widths the other decon tests do not reach (transform
+    buffers of 32, 64, 128 and 1024 points; radix 2 and Bluestein; equal and unequal lengths per
+    axis) against the oracle's FP64 FFTs."""
+    rng = np.random.default_rng(31)
+    mig = rng.standard_normal((nx, nz)).astype(np.float32)
+    img_psf = np.zeros((nx, nz), np.float32)
+    img_psf[psf[0] // 2::psf[0], psf[1] // 2::psf[1]] = 1.0
+    img_psf[psf[0] // 2 + 1::psf[0], psf[1] // 2::psf[1]] = -0.3
+    dec, coef = swd.decon(mig, img_psf, psf, flt, snap, 1e-3, fft_n=fft_n)
+    odec, ocoef = orc.decon(nx, nz, mig, img_psf, psf, flt, snap, 1e-3, fft_n=fft_n)
+    assert np.array_equal(coef, ocoef)
+    assert rel_l2(dec, odec) < TOL_DECON
+
+
 def test_decon_large_windows_match_oracle(swd, orc):
     """Windows whose 181 x 181 transform buffer (262 KB) exceeds shared memory take the
     workspace variant automatically; against the oracle."""
