@@ -225,16 +225,22 @@ int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *
 /* SWD_OPT_AUTOTUNE 1: the RTM passes choose their step-kernel variants themselves.  The forward
  *                 pass of one wavefield tries, on successive passes, the four combinations of
  *                 per-thread or TMA-staged velocity launch and per-thread or fully staged pressure
- *                 launch; the backward pass tries the by-kind pairing with per-thread or TMA-staged
- *                 velocities and the reference's pairing.  Each try is timed with CUDA events over
+ *                 launch, and (stencil order 4) the pressure kernel's register bound at 4 and 6
+ *                 blocks per SM instead of 5 and the velocity kernel's at 6; the backward pass
+ *                 tries the by-kind pairing with per-thread or TMA-staged velocities, the
+ *                 reference's pairing, and (order 4) the pressure-and-imaging kernel at 4 and 6
+ *                 blocks per SM and the velocity kernel at 6.  Without the tuning the velocity
+ *                 kernels take the 6-block bound when the pass's working set exceeds the L2.  Each try is timed with CUDA events over
  *                 its graph replays (captures excluded) and the fastest per step is kept for the
  *                 context.  Every variant gives the same images bit for bit, so only the speed of
  *                 the first few shots depends on the order.  Setting the option restarts the tuning;
  *                 while it is on it overrides SWD_OPT_TMA, SWD_OPT_STAGED and SWD_OPT_BWD_BY_KIND
  *                 for those passes.  0 (default): the options as set.
  * SWD_OPT_TUNED_FWD / SWD_OPT_TUNED_BWD (read only): the chosen variant (forward: 1 TMA velocity
- *                 + 2 staged pressure; backward: 1 TMA velocity, 4 reference pairing), -1 while
- *                 still trying or when the tuning is off. */
+ *                 + 2 staged pressure, 8 / 16 pressure kernel at 4 / 6 blocks per SM, 32 velocity
+ *                 kernel at 6; backward: 1 TMA velocity, 4 reference pairing, 8 / 16 at 4 / 6
+ *                 blocks per SM, 32 velocity kernel at 6), -1 while still trying or when the tuning
+ *                 is off. */
 #define SWD_OPT_AUTOTUNE 9
 #define SWD_OPT_TUNED_FWD 10
 #define SWD_OPT_TUNED_BWD 11

@@ -332,10 +332,18 @@ int swd_set_option(swd_ctx *ctx, int option, int value)
         case SWD_OPT_AUTOTUNE:
             if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_AUTOTUNE takes 0 or 1");
             ctx->autotune = value;
-            // forward: bit 1 TMA-staged velocity launch, bit 2 fully staged pressure launch;
-            // backward: bit 1 TMA-staged velocity launch, bit 4 the reference's pairing
-            tune_reset(ctx->tfwd, {0, 1, 2, 3});
-            tune_reset(ctx->tbwd, {0, 1, 4});
+            // forward: bit 1 TMA-staged velocity launch, bit 2 fully staged pressure launch,
+            // bits 8 / 16 the pressure kernel bounded to 4 / 6 blocks per SM, bit 32 the velocity
+            // kernel bounded to 6 (stencil order 4); backward: bit 1 TMA-staged velocity launch,
+            // bit 4 the reference's pairing, bits 8 / 16 the pressure-and-imaging kernel bounded to
+            // 4 / 6 blocks per SM, bit 32 the velocity kernel bounded to 6 (stencil order 4)
+            if (ctx->Lc == 4) {
+                tune_reset(ctx->tfwd, {0, 32, 1, 2, 3, 8, 16});
+                tune_reset(ctx->tbwd, {0, 32, 1, 4, 8, 16});
+            } else {
+                tune_reset(ctx->tfwd, {0, 1, 2, 3});
+                tune_reset(ctx->tbwd, {0, 1, 4});
+            }
             return SWD_OK;
         default:
             return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);

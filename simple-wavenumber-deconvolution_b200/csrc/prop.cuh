@@ -25,6 +25,9 @@ struct Geo {
     float odx, odz;     // (float)(1.0/(double)dx), (float)(1.0/(double)dz)
     float dt;
     float rc[MAXLC];
+    // stencil coefficients folded with the spacing, formed on the host in float:
+    // cx = rc * odx, cz = rc * odz, ncx = rc * (-odx), ncz = rc * (-odz)
+    float cx[MAXLC], cz[MAXLC], ncx[MAXLC], ncz[MAXLC];
 };
 
 struct Cpml {
@@ -185,15 +188,13 @@ __device__ __forceinline__ float elc(const float4 &v, int k) { return (&v.x)[k];
 
 // Stencil coefficients folded with the grid spacing: c[ic] = rc[ic] * (1/dx), so a tap costs
 // one subtraction and one fused multiply-add (the reference forms rc*(a-b)*odx per tap; the
-// folded form differs from it by rounding only).
+// folded form differs from it by rounding only).  The products are formed once on the host
+// (Geo::cx ...), so the taps read them from the kernel's parameter bank instead of holding them
+// in registers; the float product is the same on either side.
 template <int LC>
 struct Taps {
-    float c[LC];
-    __device__ __forceinline__ Taps(const Geo &g, float od)
-    {
-#pragma unroll
-        for (int ic = 0; ic < LC; ic++) c[ic] = g.rc[ic] * od;
-    }
+    const float (&c)[MAXLC];
+    __device__ __forceinline__ Taps(const float (&f)[MAXLC]) : c(f) {}
 };
 
 // z-window of a column around z0: w[NB*4 + k] holds z0 + k for k in [-NB*4, 4 + NB*4)
@@ -233,7 +234,7 @@ struct PTile {
 };
 
 // velocity half step (reference kernels _vx/_vz, acoustic_HLVSPRTMLc.cu:24-118; receiver
-// variants with the wider guards and -dx/-dz, :623-715), the pressure read through pl.
+// variants (WIDE) with the wider guards and -dx/-dz, :623-715), the pressure read through pl.
 // Within each half the coefficient and the old velocity are loaded with the pressure taps,
 // before the CPML branch and its store: a load after a store through a pointer the compiler
 // cannot prove distinct waits for the branch, which adds a memory latency per half.  The
@@ -242,8 +243,7 @@ struct PTile {
 // (*sx, *sz) (zero where a velocity is not updated); 2 adds dcb * (*sx, *sz) to the update, the
 // secondary source of an exact scattered field (coefficient difference dcbx, dcbz).
 template <int LC, bool WIDE, class PL, int SC = 0>
-__device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
-                                            int x, int z0, const PL &pl, float4 *sx = nullptr, float4 *sz = nullptr,
+__device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const Mat &m, Wave w, int x, int z0, const PL &pl, float4 *sx = nullptr, float4 *sz = nullptr,
                                             const float *dcbx = nullptr, const float *dcbz = nullptr)
 {
     if constexpr (SC == 1) {
@@ -252,7 +252,7 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
     }
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
-    const Taps<LC> tx(g, odx), tz(g, odz);
+    const Taps<LC> tx(WIDE ? g.ncx : g.cx), tz(WIDE ? g.ncz : g.cz);
     // ---- vx: x taps from the neighbouring columns
     const bool colx = x >= LC - 1 && x <= ntx - LC - 1;
     if (colx) {
@@ -357,19 +357,18 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
 }
 
 template <int LC, bool WIDE>
-__device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
-                                          int x, int z0)
+__device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, int x, int z0)
 {
-    v_update4_l<LC, WIDE>(g, c, m, w, odx, odz, x, z0, PGlobal{w.p, g.ldz});
+    v_update4_l<LC, WIDE>(g, c, m, w, x, z0, PGlobal{w.p, g.ldz});
 }
 
 // pressure step with CPML (reference kernel _p, :121-173) on the four cells; returns the
 // new values in pn (old values where not updated) and the per-cell update flags.  The
 // coefficient ck is loaded with the old pressure, before the CPML branches and their stores
-// (see v_update4_l).
-template <int LC>
-__device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, float odx, float odz,
-                                          int x, int z0, float4 &pn, bool upd[4], float4 *ssum = nullptr)
+// (see v_update4_l).  NEG: the receiver wavefield's -dx/-dz.
+template <int LC, bool NEG = false>
+__device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, int x, int z0,
+                                          float4 &pn, bool upd[4], float4 *ssum = nullptr)
 {
     const int ntx = g.ntx, ntz = g.ntz, ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
@@ -384,7 +383,7 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat
     if (!any) return;
     const float4 kc = ldg4(m.ck + ip);
     float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
-    const Taps<LC> tx(g, odx), tz(g, odz);
+    const Taps<LC> tx(NEG ? g.ncx : g.cx), tz(NEG ? g.ncz : g.cz);
     ZWin<LC> vw;
     vw.load(w.vz + (size_t)x * ldz, z0);
 #pragma unroll
@@ -626,8 +625,10 @@ __device__ __forceinline__ void cell4(int &x, int &z0)
     x = blockIdx.y * 8 + threadIdx.y;
 }
 
-template <int LC, int NW, bool CKPT, bool BATCH = false, bool SCAT = false>
-__global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
+// MB > 0 bounds the registers to MB blocks of 256 per SM (the variant for passes whose working
+// set streams from HBM, where more resident warps keep more bytes in flight; same bits)
+template <int LC, int NW, bool CKPT, bool BATCH = false, bool SCAT = false, int MB = 0>
+__global__ void __launch_bounds__(256, MB) k_fwd_v(const FwdArgs a0)
 {
     pdl_begin();
     FwdArgs a = a0;
@@ -646,12 +647,12 @@ __global__ void __launch_bounds__(256) k_fwd_v(const FwdArgs a0)
         static_assert(NW == 2, "the scattered field runs beside its background");
         float4 sx, sz;
         const PGlobal p0{a.w[0].p, a.g.ldz}, p1{a.w[1].p, a.g.ldz};
-        v_update4_l<LC, false, PGlobal, 1>(a.g, a.c, a.m, a.w[0], a.g.odx, a.g.odz, x, z0, p0, &sx, &sz);
-        v_update4_l<LC, false, PGlobal, 2>(a.g, a.c, a.m1, a.w[1], a.g.odx, a.g.odz, x, z0, p1, &sx, &sz, a.dcbx,
+        v_update4_l<LC, false, PGlobal, 1>(a.g, a.c, a.m, a.w[0], x, z0, p0, &sx, &sz);
+        v_update4_l<LC, false, PGlobal, 2>(a.g, a.c, a.m1, a.w[1], x, z0, p1, &sx, &sz, a.dcbx,
                                            a.dcbz);
     } else {
 #pragma unroll
-        for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.m, a.w[k], a.g.odx, a.g.odz, x, z0);
+        for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.m, a.w[k], x, z0);
     }
 }
 
@@ -674,8 +675,10 @@ constexpr int fwd_p_min_blocks()
     return MODE == FP_PLAIN ? 5 : 4;   // Born and scattered-field twins: 4
 }
 
-template <int LC, int NW, int MODE, bool BATCH = false>
-__global__ void __launch_bounds__(256, (fwd_p_min_blocks<LC, NW, MODE, BATCH>()))
+// MB > 0 asks the register allocator for MB blocks of 256 per SM instead of the default bound
+// (the autotuner's register-bound variants of the plain kernel; same code, same bits)
+template <int LC, int NW, int MODE, bool BATCH = false, int MB = 0>
+__global__ void __launch_bounds__(256, (MB > 0 ? MB : fwd_p_min_blocks<LC, NW, MODE, BATCH>()))
     k_fwd_p(const FwdArgs a0)
 {
     pdl_begin();
@@ -698,7 +701,7 @@ __global__ void __launch_bounds__(256, (fwd_p_min_blocks<LC, NW, MODE, BATCH>())
 #pragma unroll
         for (int w = 0; w < NW; w++) {
             bool upd[4];
-            p_update4<LC>(g, a.c, (SCAT && w == 1) ? a.m1 : a.m, a.w[w], g.odx, g.odz, x, z0, pn[w], upd,
+            p_update4<LC>(g, a.c, (SCAT && w == 1) ? a.m1 : a.m, a.w[w], x, z0, pn[w], upd,
                           (MODE != FP_PLAIN && w == 0) ? &s0 : nullptr);
             bool any = upd[0] || upd[1] || upd[2] || upd[3];
             if constexpr (SCAT) {
@@ -859,7 +862,7 @@ __device__ __forceinline__ void src_p_phase(const BwdArgs &a, int it, int x, int
     const bool src_here = x == a.sx && a.sz >= z0 && a.sz < z0 + 4;
     if (any) {
         float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
-        const Taps<LC> tx(g, g.odx), tz(g, g.odz);
+        const Taps<LC> tx(g.cx), tz(g.cz);
         ZWin<LC> vw;
         vw.load(a.s.vz + (size_t)x * ldz, z0);
 #pragma unroll
@@ -904,7 +907,7 @@ template <int LC, class PL>
 __device__ __forceinline__ void src_v_phase_l(const BwdArgs &a, int x, int z0, size_t ip, const bool in[4], const PL &pl)
 {
     const Geo &g = a.g;
-    const Taps<LC> tx(g, g.odx), tz(g, g.odz);
+    const Taps<LC> tx(g.cx), tz(g.cz);
     float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int ic = 0; ic < LC; ic++) {
@@ -947,7 +950,7 @@ __device__ __forceinline__ float4 rcv_p_phase(const BwdArgs &a, int it, int x, i
     const Geo &g = a.g;
     float4 pr;
     bool upd[4];
-    p_update4<LC>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0, pr, upd);
+    p_update4<LC, true>(g, a.c, a.m, a.r, x, z0, pr, upd);
     bool wr = upd[0] || upd[1] || upd[2] || upd[3];
     const int wc = __ldg(a.wells.wcol + x);
     if (wc >= 0) {
@@ -989,7 +992,7 @@ __global__ void __launch_bounds__(256) k_bwd_1(const BwdArgs a0)
     src_p_phase<LC>(a, it, x, z0, ip, in, any, dp);
     if (any) st4(a.dpdt + ip, dp);
     // receiver wavefield velocities (wide guards, negative spacing)
-    v_update4<LC, true>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0);
+    v_update4<LC, true>(g, a.c, a.m, a.r, x, z0);
 }
 
 // Imaging condition of one backward step on four cells (sum_image_GPU_kernel_image,
@@ -1111,8 +1114,9 @@ __global__ void __launch_bounds__(256, (LC <= 4 && !BATCH) ? 5 : 1) k_bwd_2(cons
 // velocities lag by one step (v of step 0 is never formed), so the angle gathers, which read
 // them after every step, use k_bwd_1 + k_bwd_2.
 // ------------------------------------------------------------------------------------
-template <int LC, bool BATCH = false>
-__global__ void __launch_bounds__(256) k_bwd_v(const BwdArgs a0)
+// MB as in k_fwd_v
+template <int LC, bool BATCH = false, int MB = 0>
+__global__ void __launch_bounds__(256, MB) k_bwd_v(const BwdArgs a0)
 {
     pdl_begin();
     BwdArgs a = a0;
@@ -1128,11 +1132,11 @@ __global__ void __launch_bounds__(256) k_bwd_v(const BwdArgs a0)
     bool in[4];
     const bool any = interior4(g, x, z0, in);
     if (any && it < a.nt - 2) src_v_phase<LC>(a, x, z0, ip, in);
-    v_update4<LC, true>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0);
+    v_update4<LC, true>(g, a.c, a.m, a.r, x, z0);
 }
 
-template <int LC, bool BATCH = false>
-__global__ void __launch_bounds__(256, LC > 4 ? 1 : BATCH ? BATCH_P_MIN_BLOCKS : 5) k_bwd_p(const BwdArgs a0)
+template <int LC, bool BATCH = false, int MB = 0>
+__global__ void __launch_bounds__(256, MB > 0 ? MB : (LC > 4 ? 1 : BATCH ? BATCH_P_MIN_BLOCKS : 5)) k_bwd_p(const BwdArgs a0)
 {
     pdl_begin();
     BwdArgs a = a0;
@@ -1168,7 +1172,7 @@ __global__ void __launch_bounds__(256) k_bwd_rcv_v(const BwdArgs a)
     int x, z0;
     cell4(x, z0);
     if (x >= a.g.ntx || z0 >= a.g.ntz) return;
-    v_update4<LC, true>(a.g, a.c, a.m, a.r, -a.g.odx, -a.g.odz, x, z0);
+    v_update4<LC, true>(a.g, a.c, a.m, a.r, x, z0);
 }
 
 template <int LC>
@@ -1189,7 +1193,7 @@ __global__ void __launch_bounds__(256, 5) k_bwd_rcv_p(const BwdArgs a)
     if (any) image_prefetch(a, ip, it);
     float4 pr;
     bool upd[4];
-    p_update4<LC>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0, pr, upd);
+    p_update4<LC, true>(g, a.c, a.m, a.r, x, z0, pr, upd);
     bool wr = upd[0] || upd[1] || upd[2] || upd[3];
     const int wc = __ldg(a.wells.wcol + x);
     if (wc >= 0) {

@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) k_fwd_v_tma(const FwdArgs a, const __grid
     vtile_loop<LC, 1>(g, maps, err, [&](int x0, int z0t, const float *st) {
         const int x = x0 + threadIdx.y, z0 = z0t + 4 * threadIdx.x;
         if (x < g.ntx && z0 < g.ntz)
-            v_update4_l<LC, false>(g, a.c, a.m, a.w[0], g.odx, g.odz, x, z0,
+            v_update4_l<LC, false>(g, a.c, a.m, a.w[0], x, z0,
                                    PTile{st, x0 - (LC - 1), z0t - 4 * T::NB, T::PR});
     });
 }
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(256) k_bwd_v_tma(const BwdArgs a, const __grid
         const bool any = interior4(g, x, z0, in);
         if (any && it < a.nt - 2)
             src_v_phase_l<LC>(a, x, z0, ip, in, PTile{st + T::SLOT, x0 - (LC - 1), z0t - 4 * T::NB, T::PR});
-        v_update4_l<LC, true>(g, a.c, a.m, a.r, -g.odx, -g.odz, x, z0, PTile{st, x0 - (LC - 1), z0t - 4 * T::NB, T::PR});
+        v_update4_l<LC, true>(g, a.c, a.m, a.r, x, z0, PTile{st, x0 - (LC - 1), z0t - 4 * T::NB, T::PR});
     });
 }
 
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(32 * (ST_CONS + 1)) k_fwd_p_staged(const FwdAr
             }
             if (any) {
                 float4 dvx = make_float4(0.f, 0.f, 0.f, 0.f), dvz = make_float4(0.f, 0.f, 0.f, 0.f);
-                const Taps<LC> tx(g, g.odx), tz(g, g.odz);
+                const Taps<LC> tx(g.cx), tz(g.cz);
                 ZWin<LC> vw;
                 vw.load(svz + 4 * S::NB, zr);   // row zr of the staged vz column, with its halo
                 // vx column x + c sits at stage column x + c - (x0 - LC)

@@ -116,6 +116,7 @@ struct swd_ctx {
     };
     int autotune = 0;
     PassTune tfwd, tbwd;
+    size_t l2_bytes = 0;    // the device's L2 size, for the default register bounds
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -282,7 +283,13 @@ static Geo make_geo(const swd_ctx *c)
     g.odx = (float)(1.0 / (double)c->grid.dx);
     g.odz = (float)(1.0 / (double)c->grid.dz);
     g.dt = c->grid.dt;
-    for (int i = 0; i < MAXLC; i++) g.rc[i] = c->rc[i];
+    for (int i = 0; i < MAXLC; i++) {
+        g.rc[i] = c->rc[i];
+        g.cx[i] = g.rc[i] * g.odx;
+        g.cz[i] = g.rc[i] * g.odz;
+        g.ncx[i] = g.rc[i] * -g.odx;
+        g.ncz[i] = g.rc[i] * -g.odz;
+    }
     return g;
 }
 
@@ -715,9 +722,13 @@ static void launch_step(void (*k)(P...), dim3 grid, cudaStream_t s, bool pdl, A 
 }
 
 template <int LC>
-static void launch_fwd_v(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bool pdl = false)
+static void launch_fwd_v(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bool pdl = false, int mb = 0)
 {
     const bool ck = a.ck.every > 0;
+    // register-bound variant of the plain single-wavefield kernel (stencil order 4)
+    if constexpr (LC == 4) {
+        if (nw == 1 && !ck && mb == 6) return launch_step(k_fwd_v<4, 1, false, false, false, 6>, grid, s, pdl, a);
+    }
     if (nw == 2 && a.dck) {
         launch_step(k_fwd_v<LC, 2, false, false, true>, grid, s, pdl, a);
     } else if (nw == 2) {
@@ -730,9 +741,14 @@ static void launch_fwd_v(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bo
 }
 
 template <int LC>
-static void launch_fwd_p(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bool pdl = false)
+static void launch_fwd_p(const FwdArgs &a, int nw, dim3 grid, cudaStream_t s, bool pdl = false, int mb = 0)
 {
     const bool born = a.s0_out || a.dkappa;
+    // register-bound variants of the plain single-wavefield kernel (stencil order 4 only)
+    if constexpr (LC == 4) {
+        if (nw == 1 && !a.ds.buf && !born && mb == 4) return launch_step(k_fwd_p<4, 1, FP_PLAIN, false, 4>, grid, s, pdl, a);
+        if (nw == 1 && !a.ds.buf && !born && mb == 6) return launch_step(k_fwd_p<4, 1, FP_PLAIN, false, 6>, grid, s, pdl, a);
+    }
     if (nw == 2 && a.dck) {
         launch_step(k_fwd_p<LC, 2, FP_SCAT>, grid, s, pdl, a);
     } else if (nw == 2) {
@@ -752,7 +768,13 @@ template <int LC>
 static void launch_bwd_2(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_2<LC>, grid, s, pdl, a); }
 
 template <int LC>
-static void launch_bwd_v(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_v<LC>, grid, s, pdl, a); }
+static void launch_bwd_v(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false, int mb = 0)
+{
+    if constexpr (LC == 4) {   // register-bound variant (stencil order 4)
+        if (mb == 6) return launch_step(k_bwd_v<4, false, 6>, grid, s, pdl, a);
+    }
+    launch_step(k_bwd_v<LC>, grid, s, pdl, a);
+}
 
 template <int LC>
 static void launch_bwd_2_cig(const BwdArgs &a, const CigArgs &c, dim3 grid, cudaStream_t s, bool pdl = false)
@@ -886,7 +908,15 @@ static int tma_check(swd_ctx *ctx)
 }
 
 template <int LC>
-static void launch_bwd_p(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_p<LC>, grid, s, pdl, a); }
+static void launch_bwd_p(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false, int mb = 0)
+{
+    // register-bound variants (stencil order 4 only)
+    if constexpr (LC == 4) {
+        if (mb == 4) return launch_step(k_bwd_p<4, false, 4>, grid, s, pdl, a);
+        if (mb == 6) return launch_step(k_bwd_p<4, false, 6>, grid, s, pdl, a);
+    }
+    launch_step(k_bwd_p<LC>, grid, s, pdl, a);
+}
 
 template <int LC>
 static void launch_bwd_rcv_v(const BwdArgs &a, dim3 grid, cudaStream_t s, bool pdl = false) { launch_step(k_bwd_rcv_v<LC>, grid, s, pdl, a); }
@@ -1008,6 +1038,15 @@ static void graph_free(swd_ctx::StepGraph &G)
 }
 
 // variant of the next pass of a tuner: the chosen one, else the next one to try
+// Whether a pass that touches `arrays` full-grid float arrays per step streams them from HBM
+// (its working set exceeds L2).  Such passes run the register-bound velocity kernels by default
+// (6 blocks of 256 per SM): with the data in HBM the extra resident warps keep more bytes in
+// flight, while an L2-resident pass is faster with the unbounded kernels.  Same bits either way.
+static bool streams_hbm(const swd_ctx *ctx, int arrays)
+{
+    return (size_t)ctx->ntx * ctx->ldz * sizeof(float) * arrays > ctx->l2_bytes;
+}
+
 static int tune_pick(const swd_ctx::PassTune &T) { return T.choice >= 0 ? T.cand[T.choice] : T.cand[T.next]; }
 
 static void tune_record(swd_ctx::PassTune &T, double ms_per_step)
@@ -1182,7 +1221,10 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     // velocity and pressure launches, chosen by the tuner when SWD_OPT_AUTOTUNE is on
     const bool plain1 = nw == 1 && !a.ck.every && !a.ds.buf && !a.s0_out && !a.dkappa && !a.dck;
     const bool tune = ctx->autotune && plain1;
-    const int fv = tune ? tune_pick(ctx->tfwd) : ((ctx->use_tma ? 1 : 0) | (ctx->use_staged ? 2 : 0));
+    // variant bits: 1 TMA velocity launch, 2 staged pressure launch, 8 / 16 pressure kernel at 4 / 6
+    // blocks per SM, 32 velocity kernel at 6 blocks per SM (p, vx, vz and three coefficients a step)
+    const int fv = tune ? tune_pick(ctx->tfwd)
+                        : ((ctx->use_tma ? 1 : 0) | (ctx->use_staged ? 2 : 0) | (streams_hbm(ctx, 6) ? 32 : 0));
     int use_tma = (fv & 1) && nw == 1 && !a.ck.every;
     CUtensorMap pmap;
     TmaShape tsh;
@@ -1195,6 +1237,8 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     }
     // one plain wavefield: the pressure kernel with every stencil operand staged by TMA
     int use_staged = (fv & 2) && plain1;
+    const int fmb = plain1 ? ((fv & 8) ? 4 : (fv & 16) ? 6 : 0) : 0;   // register-bound variants
+    const int vmb = plain1 && (fv & 32) ? 6 : 0;
     CUtensorMap smap[4];
     TmaShape ssh;
     if (use_staged) {
@@ -1211,13 +1255,13 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
         if (use_tma) {
             LC_DISPATCH(ctx->Lc, launch_fwd_v_tma, b, pmap, tma_err(ctx), tsh, ctx->stream);
         } else {
-            LC_DISPATCH(ctx->Lc, launch_fwd_v, b, nw, grid, ctx->stream, ctx->use_pdl);
+            LC_DISPATCH(ctx->Lc, launch_fwd_v, b, nw, grid, ctx->stream, ctx->use_pdl, vmb);
         }
         if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
         if (use_staged) {
             LC_DISPATCH(ctx->Lc, launch_fwd_p_staged, b, smap, tma_err(ctx), ssh, ctx->stream);
         } else {
-            LC_DISPATCH(ctx->Lc, launch_fwd_p, b, nw, grid, ctx->stream, ctx->use_pdl);
+            LC_DISPATCH(ctx->Lc, launch_fwd_p, b, nw, grid, ctx->stream, ctx->use_pdl, fmb);
         }
         if (ev) cudaEventRecordWithFlags(ev[3], ctx->stream, cudaEventRecordExternal);
     };
@@ -1227,6 +1271,8 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     std::vector<char> key((const char *)&a, (const char *)&a + sizeof a);
     key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
     key.insert(key.end(), (const char *)&use_staged, (const char *)&use_staged + sizeof use_staged);
+    key.insert(key.end(), (const char *)&fmb, (const char *)&fmb + sizeof fmb);
+    key.insert(key.end(), (const char *)&vmb, (const char *)&vmb + sizeof vmb);
     key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
     float pass_ms = 0.f;
     const bool timing = tune && ctx->tfwd.choice < 0;
@@ -1476,6 +1522,9 @@ int swd_create(swd_ctx **out, const swd_grid *g)
     ctx->ldz = (ctx->ntz + 31) / 32 * 32;
     cudaError_t e = cudaSetDevice(ctx->dev);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    int l2 = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->dev);
+    ctx->l2_bytes = (size_t)l2;
     if (e != cudaSuccess) {
         delete ctx;
         return SWD_ERR_CUDA;
@@ -2010,10 +2059,16 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         // the variants (by-kind pairing with plain or TMA velocities, the reference's pairing)
         // chosen by the tuner when SWD_OPT_AUTOTUNE is on
         const bool tune = ctx->autotune && !want_cig;
-        const int bv = tune ? tune_pick(ctx->tbwd) : ((ctx->use_tma ? 1 : 0) | (ctx->bwd_by_kind ? 0 : 4));
+        // variant bits: 1 TMA velocity launch, 4 the reference's pairing, 8 / 16 pressure kernel at
+        // 4 / 6 blocks per SM, 32 velocity kernel at 6 blocks per SM (two wavefields, four
+        // coefficients and the imaging sums: about twelve arrays a step)
+        const int bv = tune ? tune_pick(ctx->tbwd)
+                            : ((ctx->use_tma ? 1 : 0) | (ctx->bwd_by_kind ? 0 : 4) | (streams_hbm(ctx, 12) ? 32 : 0));
         const int by_kind = !(bv & 4) && !want_cig;
         // velocities of both wavefields with TMA-staged pressures
         int use_tma = by_kind && (bv & 1);
+        const int bmb = by_kind ? ((bv & 8) ? 4 : (bv & 16) ? 6 : 0) : 0;   // register-bound variants
+        const int bvmb = by_kind && (bv & 32) ? 6 : 0;
         CUtensorMap pmap_r, pmap_s;
         TmaShape tsh;
         if (use_tma) {
@@ -2030,13 +2085,13 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
             if (by_kind && use_tma) {
                 LC_DISPATCH(ctx->Lc, launch_bwd_v_tma, q, pmap_r, pmap_s, tma_err(ctx), tsh, ctx->stream);
             } else if (by_kind) {
-                LC_DISPATCH(ctx->Lc, launch_bwd_v, q, grid, ctx->stream, ctx->use_pdl);
+                LC_DISPATCH(ctx->Lc, launch_bwd_v, q, grid, ctx->stream, ctx->use_pdl, bvmb);
             } else {
                 LC_DISPATCH(ctx->Lc, launch_bwd_1, q, grid, ctx->stream, ctx->use_pdl);
             }
             if (ev) { cudaEventRecordWithFlags(ev[1], ctx->stream, cudaEventRecordExternal); cudaEventRecordWithFlags(ev[2], ctx->stream, cudaEventRecordExternal); }
             if (by_kind) {
-                LC_DISPATCH(ctx->Lc, launch_bwd_p, q, grid, ctx->stream, ctx->use_pdl);
+                LC_DISPATCH(ctx->Lc, launch_bwd_p, q, grid, ctx->stream, ctx->use_pdl, bmb);
             } else if (want_cig) {
                 // the gathers fused into the imaging launch
                 CigArgs cq = cg;
@@ -2054,6 +2109,8 @@ static int rtm_backward_part(swd_ctx *ctx, const swd_shot *shot, const float *da
         key.insert(key.end(), (const char *)&cg, (const char *)&cg + sizeof cg);
         key.insert(key.end(), (const char *)&by_kind, (const char *)&by_kind + sizeof by_kind);
         key.insert(key.end(), (const char *)&use_tma, (const char *)&use_tma + sizeof use_tma);
+        key.insert(key.end(), (const char *)&bmb, (const char *)&bmb + sizeof bmb);
+        key.insert(key.end(), (const char *)&bvmb, (const char *)&bvmb + sizeof bvmb);
         key.insert(key.end(), (const char *)&ctx->use_pdl, (const char *)&ctx->use_pdl + sizeof ctx->use_pdl);
         float pass_ms = 0.f;
         const bool timing = tune && ctx->tbwd.choice < 0;
