@@ -626,9 +626,12 @@ __device__ __forceinline__ void cell4(int &x, int &z0)
 }
 
 // MB > 0 bounds the registers to MB blocks of 256 per SM (the variant for passes whose working
-// set streams from HBM, where more resident warps keep more bytes in flight; same bits)
+// set streams from HBM, where more resident warps keep more bytes in flight; same bits).  The
+// plain twin is bounded to 5 blocks (48 registers instead of 52: AFor's velocity step 12.5 ->
+// 11.6 us on 1601x801).
 template <int LC, int NW, bool CKPT, bool BATCH = false, bool SCAT = false, int MB = 0>
-__global__ void __launch_bounds__(256, MB) k_fwd_v(const FwdArgs a0)
+__global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CKPT && !SCAT) ? 5 : 0))
+    k_fwd_v(const FwdArgs a0)
 {
     pdl_begin();
     FwdArgs a = a0;
