@@ -28,7 +28,20 @@ struct Geo {
     // stencil coefficients folded with the spacing, formed on the host in float:
     // cx = rc * odx, cz = rc * odz, ncx = rc * (-odx), ncz = rc * (-odz)
     float cx[MAXLC], cz[MAXLC], ncx[MAXLC], ncz[MAXLC];
+    // lean box [lx0, lx1) x [lz0, lz1): cells whose CPML coefficients a (both grids) are zero,
+    // inside the strip band, so every update guard holds (empty when lx0 >= lx1)
+    int lx0, lx1, lz0, lz1;
 };
+
+// Whether the calling (32, 8) block's 8 columns x 128 rows lie in the lean box: there every cell
+// is updated, no CPML memory term is formed (its coefficient is zero, so the general path adds
+// the same zero) and no strip cell is met, and the step kernels take a path without those
+// branches.  Block-uniform.
+__device__ __forceinline__ bool lean_block(const Geo &g)
+{
+    const int x0 = blockIdx.y * 8, z0 = blockIdx.x * 128;
+    return x0 >= g.lx0 && x0 + 8 <= g.lx1 && z0 >= g.lz0 && z0 + 128 <= g.lz1;
+}
 
 struct Cpml {
     const float *ax, *axh, *az, *azh, *bx, *bxh, *bz, *bzh;
@@ -242,7 +255,7 @@ struct PTile {
 // Scattered-field hooks (SC): 1 also returns the update sums d + phi of the four cells in
 // (*sx, *sz) (zero where a velocity is not updated); 2 adds dcb * (*sx, *sz) to the update, the
 // secondary source of an exact scattered field (coefficient difference dcbx, dcbz).
-template <int LC, bool WIDE, class PL, int SC = 0>
+template <int LC, bool WIDE, class PL, int SC = 0, bool LEAN = false>
 __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const Mat &m, Wave w, int x, int z0, const PL &pl, float4 *sx = nullptr, float4 *sz = nullptr,
                                             const float *dcbx = nullptr, const float *dcbz = nullptr)
 {
@@ -254,14 +267,14 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
     const size_t ip = (size_t)x * ldz + z0;
     const Taps<LC> tx(WIDE ? g.ncx : g.cx), tz(WIDE ? g.ncz : g.cz);
     // ---- vx: x taps from the neighbouring columns
-    const bool colx = x >= LC - 1 && x <= ntx - LC - 1;
+    const bool colx = LEAN || (x >= LC - 1 && x <= ntx - LC - 1);
     if (colx) {
         bool gx[4];
         bool any = false;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const int z = z0 + k;
-            gx[k] = WIDE ? (z <= ntz - 1) : (z >= LC && z <= ntz - LC);
+            gx[k] = LEAN || (WIDE ? (z <= ntz - 1) : (z >= LC && z <= ntz - LC));
             any |= gx[k];
         }
         if (any) {
@@ -274,9 +287,9 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
 #pragma unroll
                 for (int k = 0; k < 4; k++) el(d, k) += tx.c[ic] * (elc(a, k) - elc(b, k));
             }
-            const float ax = __ldg(c.axh + x);
             float4 phi = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (ax != 0.f) {
+            const float ax = LEAN ? 0.f : __ldg(c.axh + x);
+            if (!LEAN && ax != 0.f) {
                 const float bx = __ldg(c.bxh + x);
                 float4 po = ld4(w.ppx + ip);
 #pragma unroll
@@ -304,14 +317,14 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
         }
     }
     // ---- vz: z taps from the column's own window
-    const bool colz = WIDE ? (x >= 0 && x <= ntx - 1) : (x >= LC && x <= ntx - LC);
+    const bool colz = LEAN || (WIDE ? (x >= 0 && x <= ntx - 1) : (x >= LC && x <= ntx - LC));
     if (colz) {
         bool gz[4];
         bool any = false;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const int z = z0 + k;
-            gz[k] = z >= LC - 1 && z <= ntz - LC - 1;
+            gz[k] = LEAN || (z >= LC - 1 && z <= ntz - LC - 1);
             any |= gz[k];
         }
         if (any) {
@@ -325,8 +338,8 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
 #pragma unroll
                 for (int ic = 0; ic < LC; ic++) el(d, k) += tz.c[ic] * (pw.at(k + ic + 1) - pw.at(k - ic));
             float4 phi = make_float4(0.f, 0.f, 0.f, 0.f);
-            const float4 az = ldg4(c.azh + z0);
-            if (az.x != 0.f || az.y != 0.f || az.z != 0.f || az.w != 0.f) {
+            const float4 az = LEAN ? make_float4(0.f, 0.f, 0.f, 0.f) : ldg4(c.azh + z0);
+            if (!LEAN && (az.x != 0.f || az.y != 0.f || az.z != 0.f || az.w != 0.f)) {
                 const float4 bz = ldg4(c.bzh + z0);
                 float4 po = ld4(w.ppz + ip);
 #pragma unroll
@@ -356,17 +369,17 @@ __device__ __forceinline__ void v_update4_l(const Geo &g, const Cpml &c, const M
     }
 }
 
-template <int LC, bool WIDE>
+template <int LC, bool WIDE, bool LEAN = false>
 __device__ __forceinline__ void v_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, int x, int z0)
 {
-    v_update4_l<LC, WIDE>(g, c, m, w, x, z0, PGlobal{w.p, g.ldz});
+    v_update4_l<LC, WIDE, PGlobal, 0, LEAN>(g, c, m, w, x, z0, PGlobal{w.p, g.ldz});
 }
 
 // pressure step with CPML (reference kernel _p, :121-173) on the four cells; returns the
 // new values in pn (old values where not updated) and the per-cell update flags.  The
 // coefficient ck is loaded with the old pressure, before the CPML branches and their stores
-// (see v_update4_l).  NEG: the receiver wavefield's -dx/-dz.
-template <int LC, bool NEG = false>
+// (see v_update4_l).  NEG: the receiver wavefield's -dx/-dz; LEAN: a block of the lean box.
+template <int LC, bool NEG = false, bool LEAN = false>
 __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat &m, Wave w, int x, int z0,
                                           float4 &pn, bool upd[4], float4 *ssum = nullptr)
 {
@@ -377,7 +390,7 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const int z = z0 + k;
-        upd[k] = z >= LC && z <= ntz - LC && x >= LC && x <= ntx - LC;
+        upd[k] = LEAN || (z >= LC && z <= ntz - LC && x >= LC && x <= ntx - LC);
         any |= upd[k];
     }
     if (!any) return;
@@ -396,8 +409,8 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat
         }
     }
     float4 phx = make_float4(0.f, 0.f, 0.f, 0.f), phz = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float ax = __ldg(c.ax + x);
-    if (ax != 0.f) {
+    const float ax = LEAN ? 0.f : __ldg(c.ax + x);
+    if (!LEAN && ax != 0.f) {
         const float bx = __ldg(c.bx + x);
         float4 po = ld4(w.pvx + ip);
 #pragma unroll
@@ -407,8 +420,8 @@ __device__ __forceinline__ void p_update4(const Geo &g, const Cpml &c, const Mat
         }
         st4(w.pvx + ip, po);
     }
-    const float4 az = ldg4(c.az + z0);
-    if (az.x != 0.f || az.y != 0.f || az.z != 0.f || az.w != 0.f) {
+    const float4 az = LEAN ? make_float4(0.f, 0.f, 0.f, 0.f) : ldg4(c.az + z0);
+    if (!LEAN && (az.x != 0.f || az.y != 0.f || az.z != 0.f || az.w != 0.f)) {
         const float4 bz = ldg4(c.bz + z0);
         float4 po = ld4(w.pvz + ip);
 #pragma unroll
@@ -653,6 +666,9 @@ __global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CK
         v_update4_l<LC, false, PGlobal, 1>(a.g, a.c, a.m, a.w[0], x, z0, p0, &sx, &sz);
         v_update4_l<LC, false, PGlobal, 2>(a.g, a.c, a.m1, a.w[1], x, z0, p1, &sx, &sz, a.dcbx,
                                            a.dcbz);
+    } else if (lean_block(a.g)) {
+#pragma unroll
+        for (int k = 0; k < NW; k++) v_update4<LC, false, true>(a.g, a.c, a.m, a.w[k], x, z0);
     } else {
 #pragma unroll
         for (int k = 0; k < NW; k++) v_update4<LC, false>(a.g, a.c, a.m, a.w[k], x, z0);
@@ -695,6 +711,7 @@ __global__ void __launch_bounds__(256, (MB > 0 ? MB : fwd_p_min_blocks<LC, NW, M
     cell4(x, z0);
     const Geo &g = a.g;
     const bool in = x < g.ntx && z0 < g.ntz;
+    const bool lean = lean_block(g);
     float4 pn[NW];
 #pragma unroll
     for (int k = 0; k < NW; k++) pn[k] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -704,8 +721,10 @@ __global__ void __launch_bounds__(256, (MB > 0 ? MB : fwd_p_min_blocks<LC, NW, M
 #pragma unroll
         for (int w = 0; w < NW; w++) {
             bool upd[4];
-            p_update4<LC>(g, a.c, (SCAT && w == 1) ? a.m1 : a.m, a.w[w], x, z0, pn[w], upd,
-                          (MODE != FP_PLAIN && w == 0) ? &s0 : nullptr);
+            const Mat &mw = (SCAT && w == 1) ? a.m1 : a.m;
+            float4 *ss = (MODE != FP_PLAIN && w == 0) ? &s0 : nullptr;
+            if (lean) p_update4<LC, false, true>(g, a.c, mw, a.w[w], x, z0, pn[w], upd, ss);
+            else p_update4<LC>(g, a.c, mw, a.w[w], x, z0, pn[w], upd, ss);
             bool any = upd[0] || upd[1] || upd[2] || upd[3];
             if constexpr (SCAT) {
                 if (w == 1) {
@@ -754,7 +773,7 @@ __global__ void __launch_bounds__(256, (MB > 0 ? MB : fwd_p_min_blocks<LC, NW, M
     // dp/dt = kappa * S on the interior, for the backward pass of the stored-source mode
     if constexpr (MODE == FP_STORE) store_dpdt(a.ds, a.m, g, it, x, z0, in, s0);
     // strips (field 0): uncompressed store, or per-(step, block) scaled half/bf16
-    if (a.strips.buf && block_has_strips(g.ntx, g.ntz, g.pmlc, LC)) {
+    if (a.strips.buf && !lean && block_has_strips(g.ntx, g.ntz, g.pmlc, LC)) {
         int si[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) si[k] = (in && z0 + k < g.ntz) ? strip_index(x, z0 + k, g.ntx, g.ntz, g.pmlc, LC) : -1;
@@ -855,7 +874,7 @@ __device__ __forceinline__ float strip_restore(const Strips &st, int it, int si,
 // Source wavefield pressure of step it, interior only (fdtd_2d_GPU_kernel_p_backward
 // :434-485, -dt), source subtraction, boundary-strip overwrite (:575-620); returns
 // dp/dt = kap * div v in dp (0 outside the interior).
-template <int LC>
+template <int LC, bool LEAN = false>
 __device__ __forceinline__ void src_p_phase(const BwdArgs &a, int it, int x, int z0, size_t ip, const bool in[4],
                                             bool any, float4 &dp)
 {
@@ -882,7 +901,7 @@ __device__ __forceinline__ void src_p_phase(const BwdArgs &a, int it, int x, int
         const float4 ck = ldg4(a.m.ck + ip), kap = ldg4(a.m.kap + ip);
         float4 p = ld4(a.s.p + ip);
         const int nzb = (g.ntz + 127) / 128;
-        const bool band = block_has_strips(g.ntx, g.ntz, g.pmlc, LC);
+        const bool band = !LEAN && block_has_strips(g.ntx, g.ntz, g.pmlc, LC);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             if (!in[k]) continue;
@@ -947,13 +966,13 @@ __device__ __forceinline__ void src_v_phase(const BwdArgs &a, int x, int z0, siz
 }
 
 // Receiver wavefield pressure (CPML, -dx/-dz) and hard injection of the data (:717-782)
-template <int LC>
+template <int LC, bool LEAN = false>
 __device__ __forceinline__ float4 rcv_p_phase(const BwdArgs &a, int it, int x, int z0, size_t ip)
 {
     const Geo &g = a.g;
     float4 pr;
     bool upd[4];
-    p_update4<LC, true>(g, a.c, a.m, a.r, x, z0, pr, upd);
+    p_update4<LC, true, LEAN>(g, a.c, a.m, a.r, x, z0, pr, upd);
     bool wr = upd[0] || upd[1] || upd[2] || upd[3];
     const int wc = __ldg(a.wells.wcol + x);
     if (wc >= 0) {
@@ -1132,6 +1151,12 @@ __global__ void __launch_bounds__(256, MB) k_bwd_v(const BwdArgs a0)
     const Geo &g = a.g;
     if (x >= g.ntx || z0 >= g.ntz) return;
     const size_t ip = (size_t)x * g.ldz + z0;
+    if (lean_block(g)) {   // every cell interior, no CPML term, no strip
+        const bool in[4] = {true, true, true, true};
+        if (it < a.nt - 2) src_v_phase<LC>(a, x, z0, ip, in);
+        v_update4<LC, true, true>(g, a.c, a.m, a.r, x, z0);
+        return;
+    }
     bool in[4];
     const bool any = interior4(g, x, z0, in);
     if (any && it < a.nt - 2) src_v_phase<LC>(a, x, z0, ip, in);
@@ -1152,6 +1177,15 @@ __global__ void __launch_bounds__(256, MB > 0 ? MB : (LC > 4 ? 1 : BATCH ? BATCH
     const Geo &g = a.g;
     if (x >= g.ntx || z0 >= g.ntz) return;
     const size_t ip = (size_t)x * g.ldz + z0;
+    if (lean_block(g)) {   // every cell interior, no CPML term, no strip
+        const bool in[4] = {true, true, true, true};
+        image_prefetch(a, ip, it);
+        float4 dp;
+        src_p_phase<LC, true>(a, it, x, z0, ip, in, true, dp);
+        const float4 pr = rcv_p_phase<LC, true>(a, it, x, z0, ip);
+        image4(a, ip, in, dp, pr, it);
+        return;
+    }
     bool in[4];
     const bool any = interior4(g, x, z0, in);
     if (any) image_prefetch(a, ip, it);

@@ -117,6 +117,7 @@ struct swd_ctx {
     int autotune = 0;
     PassTune tfwd, tbwd;
     size_t l2_bytes = 0;    // the device's L2 size, for the default register bounds
+    int lean[4] = {0, 0, 0, 0};   // lean box of the step kernels (Geo::lx0 ...), from the CPML arrays
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -290,6 +291,7 @@ static Geo make_geo(const swd_ctx *c)
         g.ncx[i] = g.rc[i] * -g.odx;
         g.ncz[i] = g.rc[i] * -g.odz;
     }
+    g.lx0 = c->lean[0]; g.lx1 = c->lean[1]; g.lz0 = c->lean[2]; g.lz1 = c->lean[3];
     return g;
 }
 
@@ -1633,6 +1635,20 @@ int swd_set_cpml(swd_ctx *ctx, const float *a_x, const float *a_x_half, const fl
     }
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_cpml = true;
+    // lean box: inside the strip band's inner edge (pmlc + Lc from every side), shrunk to the
+    // columns / rows where both a coefficients (integer and half grid) are zero; empty when a
+    // nonzero coefficient remains inside
+    auto span = [&](const float *a, const float *ah, int n, int *s) {
+        int lo = ctx->pmlc + ctx->Lc, hi = n - ctx->pmlc - ctx->Lc;
+        while (lo < hi && (a[lo] != 0.f || ah[lo] != 0.f)) lo++;
+        while (hi > lo && (a[hi - 1] != 0.f || ah[hi - 1] != 0.f)) hi--;
+        bool clean = true;
+        for (int i = lo; i < hi; i++) clean = clean && a[i] == 0.f && ah[i] == 0.f;
+        s[0] = clean ? lo : 0;
+        s[1] = clean ? hi : 0;
+    };
+    span(a_x, a_x_half, ctx->ntx, ctx->lean);
+    span(a_z, a_z_half, ctx->ntz, ctx->lean + 2);
     return SWD_OK;
 }
 
