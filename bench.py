@@ -414,16 +414,17 @@ def run_ours(args, rank, world, dist):
     if not args.no_parity:
         pnt = args.parity_nt or None   # the whole record (c5: about 9 minutes of host time)
         parity = rank0_single(rank, world, lambda: fp64_parity(swd, E, w, shot, rick, data, nt=pnt))
+    options = {"staged_p": int(E.get_option(swd.OPT_STAGED)), "tma_v": int(E.get_option(swd.OPT_TMA)),
+               "autotune": int(E.get_option(swd.OPT_AUTOTUNE)), "tuned_fwd": int(E.get_option(swd.OPT_TUNED_FWD)),
+               "tuned_bwd": int(E.get_option(swd.OPT_TUNED_BWD))}
+    E.close()
     return {
         "metric": "RTM shots/s", "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_val / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP64 imaging)", "data": "synthetic (seeded random-field model, PSF data)",
         "config": {"workload": WORKLOADS[args.config], "parallelism": f"replicas x{world}",
                    "l2": "flushed (256 MiB write) before every timed step", "strips": strips,
-                   "options": {"staged_p": int(E.get_option(swd.OPT_STAGED)), "tma_v": int(E.get_option(swd.OPT_TMA)),
-                               "autotune": int(E.get_option(swd.OPT_AUTOTUNE)),
-                               "tuned_fwd": int(E.get_option(swd.OPT_TUNED_FWD)),
-                               "tuned_bwd": int(E.get_option(swd.OPT_TUNED_BWD))}},
+                   "options": options},
         "gcell_updates_per_s": value * cells_per_shot / 1e9,
         "e2e": {"value": e2e, "unit": "shots/s", "h2d_bytes_per_step": int(data.nbytes + rick.nbytes),
                 "d2h_bytes_per_step": int(2 * w.nx * w.nz * 4)},
@@ -1492,6 +1493,42 @@ def run_reference(args):
             "wall_s": time.perf_counter() - t0}
 
 
+def compact(rec):
+    """The figures of a workload's own line that its sub-record in the default line keeps."""
+    keep = ("metric", "value", "unit", "steps", "warmup", "ms_per_step", "dtype", "gpu_launches", "clocks", "parity")
+    out = {k: rec[k] for k in keep if k in rec}
+    out["workload"] = rec.get("config", {}).get("workload")
+    if rec.get("e2e"):
+        out["e2e"] = rec["e2e"].get("value")
+    r = rec.get("roofline") or {}
+    out["roofline"] = {k: r[k] for k in ("bound", "kernel", "achieved", "peak", "unit", "frac", "traffic",
+                                         "kernels_us", "kernels_frac", "fft_equivalent_gflops", "note") if k in r}
+    return out
+
+
+def extra_workloads(args):
+    """Sub-records of the default line (one-GPU runs, after its own timed regions): one shot of the
+    4001x1601 RTM (FP16 strips, per-kernel roofline), the AFor modelling shot and the 4001x1601
+    image's windowed deconvolution, each with its own warm-up and timed steps, L2 flush and clocks,
+    so that these workloads are measured by every default run too.  A failure is recorded in
+    place of the sub-record and leaves the headline line intact."""
+    import copy
+    subs = {}
+    jobs = (("rtm_c5", run_ours, dict(config="c5", steps=2, warmup=3, no_parity=True, no_batch=True, no_stored=True,
+                                      autotune=False, tma=False, staged=False, pdl=False, path=None)),
+            ("afor", run_afor, dict(steps=5, warmup=3)),
+            ("decon_c5", run_decon, dict(config="c5", steps=5, warmup=3)))
+    for name, fn, over in jobs:
+        a = copy.copy(args)
+        for k, v in over.items():
+            setattr(a, k, v)
+        try:
+            subs[name] = compact(fn(a, 0, 1, None))
+        except Exception as e:   # recorded, not hidden: the sub-record carries the error
+            subs[name] = {"error": f"{type(e).__name__}: {e}"}
+    return subs
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1511,6 +1548,8 @@ def main():
                     help="grid of --workload rtm (c2, c5) or decon (c2, c5, shipped: the reference's window geometry)")
     ap.add_argument("--no-stored", action="store_true", help="skip the stored-source measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-survey sub-record")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the sub-records of the other workloads (c5 shot, AFor modelling, c5 decon)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the image-error check against the FP64 oracle (a few minutes of host time)")
     ap.add_argument("--parity-nt", type=int, default=0,
@@ -1550,6 +1589,8 @@ def main():
     runner = {"rtm": run_ours, "lsrtm": run_lsrtm, "batch": run_batch, "decon": run_decon, "afor": run_afor,
               "c5flow": run_c5flow}[args.workload]
     out = runner(args, rank, world, dist)
+    if rank == 0 and world == 1 and args.workload == "rtm" and args.config == "c2" and not args.no_extra:
+        out["workloads"] = extra_workloads(args)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

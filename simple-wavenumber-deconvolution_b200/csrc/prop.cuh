@@ -1209,7 +1209,8 @@ __global__ void __launch_bounds__(256) k_bwd_rcv_v(const BwdArgs a)
     int x, z0;
     cell4(x, z0);
     if (x >= a.g.ntx || z0 >= a.g.ntz) return;
-    v_update4<LC, true>(a.g, a.c, a.m, a.r, x, z0);
+    if (lean_block(a.g)) v_update4<LC, true, true>(a.g, a.c, a.m, a.r, x, z0);
+    else v_update4<LC, true>(a.g, a.c, a.m, a.r, x, z0);
 }
 
 template <int LC>
@@ -1223,14 +1224,16 @@ __global__ void __launch_bounds__(256, 5) k_bwd_rcv_p(const BwdArgs a)
     if (x >= g.ntx || z0 >= g.ntz) return;
     const int ldz = g.ldz;
     const size_t ip = (size_t)x * ldz + z0;
+    const bool lean = lean_block(g);   // every cell interior and updated, no CPML term
     bool in[4];
     bool any = false;
 #pragma unroll
-    for (int k = 0; k < 4; k++) { in[k] = z0 + k < g.ntz && interior(x, z0 + k, g); any |= in[k]; }
+    for (int k = 0; k < 4; k++) { in[k] = lean || (z0 + k < g.ntz && interior(x, z0 + k, g)); any |= in[k]; }
     if (any) image_prefetch(a, ip, it);
     float4 pr;
     bool upd[4];
-    p_update4<LC, true>(g, a.c, a.m, a.r, x, z0, pr, upd);
+    if (lean) p_update4<LC, true, true>(g, a.c, a.m, a.r, x, z0, pr, upd);
+    else p_update4<LC, true>(g, a.c, a.m, a.r, x, z0, pr, upd);
     bool wr = upd[0] || upd[1] || upd[2] || upd[3];
     const int wc = __ldg(a.wells.wcol + x);
     if (wc >= 0) {

@@ -1224,9 +1224,11 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     const bool plain1 = nw == 1 && !a.ck.every && !a.ds.buf && !a.s0_out && !a.dkappa && !a.dck;
     const bool tune = ctx->autotune && plain1;
     // variant bits: 1 TMA velocity launch, 2 staged pressure launch, 8 / 16 pressure kernel at 4 / 6
-    // blocks per SM, 32 velocity kernel at 6 blocks per SM (p, vx, vz and three coefficients a step)
+    // blocks per SM, 32 velocity kernel at 6 blocks per SM (p, vx, vz and three coefficients a step;
+    // the stored-source forward also streams its dp/dt store out every step)
     const int fv = tune ? tune_pick(ctx->tfwd)
-                        : ((ctx->use_tma ? 1 : 0) | (ctx->use_staged ? 2 : 0) | (streams_hbm(ctx, 6) ? 32 : 0));
+                        : ((ctx->use_tma ? 1 : 0) | (ctx->use_staged ? 2 : 0) |
+                           (streams_hbm(ctx, 6) || a.ds.buf ? 32 : 0));
     int use_tma = (fv & 1) && nw == 1 && !a.ck.every;
     CUtensorMap pmap;
     TmaShape tsh;
@@ -1240,7 +1242,7 @@ static int run_forward(swd_ctx *ctx, FwdJob &J, ShotPlan &P)
     // one plain wavefield: the pressure kernel with every stencil operand staged by TMA
     int use_staged = (fv & 2) && plain1;
     const int fmb = plain1 ? ((fv & 8) ? 4 : (fv & 16) ? 6 : 0) : 0;   // register-bound variants
-    const int vmb = plain1 && (fv & 32) ? 6 : 0;
+    const int vmb = nw == 1 && !a.ck.every && (fv & 32) ? 6 : 0;
     CUtensorMap smap[4];
     TmaShape ssh;
     if (use_staged) {
