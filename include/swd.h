@@ -244,6 +244,11 @@ int swd_rtm_batch(swd_ctx *ctx, int nshots, const swd_shot *shots, const float *
 #define SWD_OPT_AUTOTUNE 9
 #define SWD_OPT_TUNED_FWD 10
 #define SWD_OPT_TUNED_BWD 11
+/* SWD_OPT_LEAN 1 (default): blocks of the step kernels that lie inside the CPML-free, strip-free
+ *                 box (found from the arrays of swd_set_cpml) take a path without the update
+ *                 guards, CPML branches and strip code; 0: every block takes the general path.  The
+ *                 same results bit for bit. */
+#define SWD_OPT_LEAN 12
 int swd_set_option(swd_ctx *ctx, int option, int value);
 int swd_get_option(swd_ctx *ctx, int option, int *value);
 

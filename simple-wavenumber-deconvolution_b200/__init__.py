@@ -29,7 +29,7 @@ STRIP_F32, STRIP_F16, STRIP_BF16, STRIP_I16 = 0, 1, 2, 3
 PATH_PLAIN, PATH_FUSED = 0, 1
 RTM_PREPROCESS, RTM_ILLUM_RCV, RTM_NO_STACK, RTM_CIG = 1, 2, 4, 8
 OPT_GRAPHS, OPT_BATCH, OPT_BATCH_TUNED, OPT_IMAGE_BLOCKS, OPT_BWD_BY_KIND, OPT_TMA, OPT_PDL, OPT_STAGED = 1, 2, 3, 4, 5, 6, 7, 8
-OPT_AUTOTUNE, OPT_TUNED_FWD, OPT_TUNED_BWD = 9, 10, 11
+OPT_AUTOTUNE, OPT_TUNED_FWD, OPT_TUNED_BWD, OPT_LEAN = 9, 10, 11, 12
 
 
 class SwdError(RuntimeError):

@@ -345,6 +345,10 @@ int swd_set_option(swd_ctx *ctx, int option, int value)
                 tune_reset(ctx->tbwd, {0, 1, 4});
             }
             return SWD_OK;
+        case SWD_OPT_LEAN:
+            if (value != 0 && value != 1) return fail(ctx, SWD_ERR_ARG, "SWD_OPT_LEAN takes 0 or 1");
+            ctx->use_lean = value;
+            return SWD_OK;
         default:
             return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);
     }
@@ -363,6 +367,7 @@ int swd_get_option(swd_ctx *ctx, int option, int *value)
         case SWD_OPT_PDL: *value = ctx->use_pdl; return SWD_OK;
         case SWD_OPT_STAGED: *value = ctx->use_staged; return SWD_OK;
         case SWD_OPT_AUTOTUNE: *value = ctx->autotune; return SWD_OK;
+        case SWD_OPT_LEAN: *value = ctx->use_lean; return SWD_OK;
         case SWD_OPT_TUNED_FWD: *value = ctx->autotune && ctx->tfwd.choice >= 0 ? ctx->tfwd.cand[ctx->tfwd.choice] : -1; return SWD_OK;
         case SWD_OPT_TUNED_BWD: *value = ctx->autotune && ctx->tbwd.choice >= 0 ? ctx->tbwd.cand[ctx->tbwd.choice] : -1; return SWD_OK;
         default: return fail(ctx, SWD_ERR_ARG, "unknown option %d", option);

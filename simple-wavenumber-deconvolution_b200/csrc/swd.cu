@@ -118,6 +118,7 @@ struct swd_ctx {
     PassTune tfwd, tbwd;
     size_t l2_bytes = 0;    // the device's L2 size, for the default register bounds
     int lean[4] = {0, 0, 0, 0};   // lean box of the step kernels (Geo::lx0 ...), from the CPML arrays
+    int use_lean = 1;             // SWD_OPT_LEAN
     // instrumentation
     int prof_every = 0;
     double prof_ms[SWD_NKERNELS] = {0};
@@ -291,7 +292,9 @@ static Geo make_geo(const swd_ctx *c)
         g.ncx[i] = g.rc[i] * -g.odx;
         g.ncz[i] = g.rc[i] * -g.odz;
     }
-    g.lx0 = c->lean[0]; g.lx1 = c->lean[1]; g.lz0 = c->lean[2]; g.lz1 = c->lean[3];
+    // an empty box (every block on the general path) when SWD_OPT_LEAN is 0
+    g.lx0 = c->use_lean ? c->lean[0] : 0; g.lx1 = c->use_lean ? c->lean[1] : 0;
+    g.lz0 = c->use_lean ? c->lean[2] : 0; g.lz1 = c->use_lean ? c->lean[3] : 0;
     return g;
 }
 

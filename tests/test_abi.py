@@ -36,6 +36,24 @@ def test_version_and_error_paths(swd):
     assert L.swd_last_error(None) == b"null context"
 
 
+def test_python_constants_match_the_header(swd):
+    """Every SWD_* integer constant of include/swd.h that the Python mirror names carries the
+    header's value (options, strip precisions, RTM flags, kernel paths, status codes)."""
+    src = (ROOT / "include" / "swd.h").read_text()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define SWD_([A-Z0-9_]+)\s+(-?\d+)\b", src)}
+    checked = 0
+    for name, value in defs.items():
+        for py in (name, name.replace("ERR_", "SWD_ERR_") if name.startswith("ERR_") else None,
+                   "SWD_" + name):
+            if py and hasattr(swd, py):
+                assert getattr(swd, py) == value, (name, getattr(swd, py), value)
+                checked += 1
+                break
+    opts = [n for n in defs if n.startswith("OPT_")]
+    assert len(opts) >= 12 and all(hasattr(swd, n) for n in opts), [n for n in opts if not hasattr(swd, n)]
+    assert checked >= 20
+
+
 def declared_arity():
     """{function: number of parameters} of every prototype in include/swd.h."""
     src = (ROOT / "include" / "swd.h").read_text()

@@ -656,3 +656,61 @@ def test_full_grid_images_vs_fp64_oracle(swd, orc, cfg):
     print(f"{cfg} grid, nt={nt}: I {eI:.2e}  S {eS:.2e}  filtered image {eF:.2e} vs FP64")
     assert np.abs(sh["img"]).max() > 0
     assert eI < TOL and eS < TOL and eF < TOL
+
+
+def _lean_blocks(c):
+    """Blocks (8 columns x 128 rows) of the step kernels inside the lean box, computed from the
+    case's CPML arrays the way the engine does; the lean-path test needs some."""
+    def span(a, ah, n):
+        lo, hi = c.pmlc + c.Lc, n - c.pmlc - c.Lc
+        zero = (np.asarray(a) == 0) & (np.asarray(ah) == 0)
+        while lo < hi and not zero[lo]:
+            lo += 1
+        while hi > lo and not zero[hi - 1]:
+            hi -= 1
+        return (lo, hi) if zero[lo:hi].all() else (0, 0)
+    lx0, lx1 = span(c.cp["a_x"], c.cp["a_x_half"], c.ntx)
+    lz0, lz1 = span(c.cp["a_z"], c.cp["a_z_half"], c.ntz)
+    bx = sum(1 for b in range(c.ntx // 8 + 1) if 8 * b >= lx0 and 8 * b + 8 <= lx1)
+    bz = sum(1 for b in range(c.ntz // 128 + 1) if 128 * b >= lz0 and 128 * b + 128 <= lz1)
+    return bx * bz
+
+
+@pytest.mark.parametrize("shape", [(101, 300, 10, 4), (77, 420, 12, 1), (90, 390, 10, 7), (64, 310, 8, 8)],
+                         ids=["101x300_Lc4", "77x420_Lc1", "90x390_Lc7", "64x310_Lc8"])
+@pytest.mark.parametrize("strips", ["f32", "f16"])
+def test_lean_blocks_same_bits(swd, orc, shape, strips):
+    """The step kernels' lean path (blocks inside the CPML-free, strip-free box: no update guards,
+    CPML branches or strip code) against the general path for every block (SWD_OPT_LEAN = 0): the
+    forward record, the raw RTM images (by-kind and reference pairing), the stored-source images and
+    the twin record with its up/down split are identical bit for bit, with FP32 and FP16 strips, on
+    grids that are not multiples of the block and for stencil orders 1, 4, 7 and 8."""
+    nx, nz, pml, Lc = shape
+    c = Case(swd, orc, nx=nx, nz=nz, pml=pml, Lc=Lc, nt=200, path=0)
+    assert _lean_blocks(c) > 0
+    data = orc.forward(c.M, c.G, c.rick)["seis"]
+    flags = swd.RTM_PREPROCESS | swd.RTM_NO_STACK | swd.RTM_ILLUM_RCV
+    c.E.set_strip_precision({"f32": swd.STRIP_F32, "f16": swd.STRIP_F16}[strips])
+    hr = c.E.hilbert(c.rick)
+    coef, _ = swd.kz_taper(swd.pow2(c.ntz), c.dz)
+    out = {}
+    for lean in (1, 0):
+        c.E.set_option(swd.OPT_LEAN, lean)
+        assert c.E.get_option(swd.OPT_LEAN) == lean
+        r = [c.E.forward(c.shot, c.rick)]
+        c.E.rtm_shot(c.shot, c.rick, data, flags=flags, want=())
+        r += list(c.E.rtm_raw(rcv=True))
+        c.E.set_option(swd.OPT_BWD_BY_KIND, 0)
+        c.E.rtm_shot(c.shot, c.rick, data, flags=flags, want=())
+        r += list(c.E.rtm_raw(rcv=True))
+        c.E.set_option(swd.OPT_BWD_BY_KIND, 1)
+        c.E.set_source_storage(1, swd.STRIP_I16)
+        c.E.rtm_shot(c.shot, c.rick, data, flags=flags, want=())
+        r += list(c.E.rtm_raw(rcv=True))
+        c.E.set_source_storage(0)
+        r += list(c.E.forward(c.shot, c.rick, hrick=hr, kz_coef=coef))
+        out[lean] = r
+    c.E.set_option(swd.OPT_LEAN, 1)
+    assert np.abs(out[1][0]).max() > 0 and np.abs(out[1][1]).max() > 0
+    for i, (a, b) in enumerate(zip(out[1], out[0])):
+        assert np.array_equal(a, b), i
