@@ -481,7 +481,7 @@ def engine_vs_oracle(swd, E, shot, rick, data, nt, ref):
     res = {"image_rel_l2": rel(I, ref[0]), "illum_rel_l2": rel(S, ref[1]), "fimage_rel_l2": rel(out["fimage"], ref[2]),
            "tolerance": PARITY_TOL}
     errs = [res["image_rel_l2"], res["illum_rel_l2"], res["fimage_rel_l2"]]
-    # a record too short for the data to reach the receivers leaves the image zero: no verdict
+    # a record too short for the data to reach the receivers leaves the image zero: no pass or fail
     res["pass"] = None if None in errs else max(errs) <= PARITY_TOL
     return res
 
