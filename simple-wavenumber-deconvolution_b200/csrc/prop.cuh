@@ -640,10 +640,11 @@ __device__ __forceinline__ void cell4(int &x, int &z0)
 
 // MB > 0 bounds the registers to MB blocks of 256 per SM (the variant for passes whose working
 // set streams from HBM, where more resident warps keep more bytes in flight; same bits).  The
-// plain twin is bounded to 5 blocks (48 registers instead of 52: AFor's velocity step 12.5 ->
-// 11.6 us on 1601x801).
+// twins without checkpoints are bounded to 5 blocks: the plain twin 48 registers instead of 52
+// (AFor's velocity step 12.5 -> 11.6 us on 1601x801), the scattered-field twin 48 instead of 54
+// (90.5 -> 80.6 us on 4001x1601).
 template <int LC, int NW, bool CKPT, bool BATCH = false, bool SCAT = false, int MB = 0>
-__global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CKPT && !SCAT) ? 5 : 0))
+__global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CKPT) ? 5 : 0))
     k_fwd_v(const FwdArgs a0)
 {
     pdl_begin();
@@ -682,8 +683,8 @@ __global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CK
 constexpr int BATCH_P_MIN_BLOCKS = 4;
 
 // Blocks per SM asked of the register allocator: 5 (48 registers) for one wavefield and for the
-// twin of the modelling forward (4 bytes of spill there), 4 (64 registers, no spill) for the Born
-// twin and the batched kernel; left free for LC > 4.  The twin at its free 80 registers ran 3
+// twins of the modelling forward and of the scattered field (small spills there), 4 (64
+// registers, no spill) for the Born twin and the batched kernel; left free for LC > 4.  The twin at its free 80 registers ran 3
 // blocks per SM and its launches took 8% longer.
 template <int LC, int NW, int MODE, bool BATCH>
 constexpr int fwd_p_min_blocks()
@@ -691,7 +692,9 @@ constexpr int fwd_p_min_blocks()
     if (LC > 4) return 1;
     if (BATCH) return BATCH_P_MIN_BLOCKS;
     if (NW == 1) return MODE == FP_BORN ? 1 : 5;
-    return MODE == FP_PLAIN ? 5 : 4;   // Born and scattered-field twins: 4
+    // Born twin: 4 (64 registers, no spill); the scattered-field twin at 5 (48 registers, a
+    // 108-byte spill) ran 72.5 -> 68.9 us per step on 4001x1601, ahead of 4 blocks
+    return (MODE == FP_PLAIN || MODE == FP_SCAT) ? 5 : 4;
 }
 
 // MB > 0 asks the register allocator for MB blocks of 256 per SM instead of the default bound
