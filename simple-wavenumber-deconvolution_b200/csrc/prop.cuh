@@ -664,9 +664,15 @@ __global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CK
         static_assert(NW == 2, "the scattered field runs beside its background");
         float4 sx, sz;
         const PGlobal p0{a.w[0].p, a.g.ldz}, p1{a.w[1].p, a.g.ldz};
-        v_update4_l<LC, false, PGlobal, 1>(a.g, a.c, a.m, a.w[0], x, z0, p0, &sx, &sz);
-        v_update4_l<LC, false, PGlobal, 2>(a.g, a.c, a.m1, a.w[1], x, z0, p1, &sx, &sz, a.dcbx,
-                                           a.dcbz);
+        if (lean_block(a.g)) {
+            v_update4_l<LC, false, PGlobal, 1, true>(a.g, a.c, a.m, a.w[0], x, z0, p0, &sx, &sz);
+            v_update4_l<LC, false, PGlobal, 2, true>(a.g, a.c, a.m1, a.w[1], x, z0, p1, &sx, &sz, a.dcbx,
+                                                     a.dcbz);
+        } else {
+            v_update4_l<LC, false, PGlobal, 1>(a.g, a.c, a.m, a.w[0], x, z0, p0, &sx, &sz);
+            v_update4_l<LC, false, PGlobal, 2>(a.g, a.c, a.m1, a.w[1], x, z0, p1, &sx, &sz, a.dcbx,
+                                               a.dcbz);
+        }
     } else if (lean_block(a.g)) {
 #pragma unroll
         for (int k = 0; k < NW; k++) v_update4<LC, false, true>(a.g, a.c, a.m, a.w[k], x, z0);
