@@ -642,9 +642,10 @@ __device__ __forceinline__ void cell4(int &x, int &z0)
 // set streams from HBM, where more resident warps keep more bytes in flight; same bits).  The
 // twins without checkpoints are bounded to 5 blocks: the plain twin 48 registers instead of 52
 // (AFor's velocity step 12.5 -> 11.6 us on 1601x801), the scattered-field twin 48 instead of 54
-// (90.5 -> 80.6 us on 4001x1601).
+// (90.5 -> 80.6 us on 4001x1601).  The batched kernel, whose batch streams from HBM, takes 6
+// (40 registers, no spill: 27.5 -> 24.3 us per step of four 1601x801 shots).
 template <int LC, int NW, bool CKPT, bool BATCH = false, bool SCAT = false, int MB = 0>
-__global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CKPT) ? 5 : 0))
+__global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CKPT) ? 5 : (BATCH && LC <= 4) ? 6 : 0))
     k_fwd_v(const FwdArgs a0)
 {
     pdl_begin();
@@ -682,11 +683,14 @@ __global__ void __launch_bounds__(256, MB > 0 ? MB : ((NW == 2 && LC <= 4 && !CK
     }
 }
 
-// Blocks per SM of the batched pressure kernels (forward and backward), LC <= 4: the per-shot
-// view of the arguments holds every shifted wave pointer in registers (96 and 120 unbounded, 2
-// blocks per SM); at 4 blocks (64 registers, no spill forward, 24 bytes backward) a batched survey
-// ran 21% faster than unbounded and 5% faster than at 3 blocks, with the same stack.
+// Blocks per SM of the batched pressure kernels, LC <= 4: the per-shot view of the arguments
+// holds every shifted wave pointer in registers (96 and 120 unbounded, 2 blocks per SM); at 4
+// blocks (64 registers) a batched survey ran 21% faster than unbounded and 5% faster than at 3
+// blocks, with the same stack.  With the lean path the backward one is faster still at 5 (48
+// registers, an 80-byte spill: 66.1 -> 62.4 us per step of four 1601x801 shots), the forward one
+// not (32.0 against 32.3 us).
 constexpr int BATCH_P_MIN_BLOCKS = 4;
+constexpr int BATCH_BWD_P_MIN_BLOCKS = 5;
 
 // Blocks per SM asked of the register allocator: 5 (48 registers) for one wavefield and for the
 // twins of the modelling forward and of the scattered field (small spills there), 4 (64
@@ -1173,7 +1177,7 @@ __global__ void __launch_bounds__(256, MB) k_bwd_v(const BwdArgs a0)
 }
 
 template <int LC, bool BATCH = false, int MB = 0>
-__global__ void __launch_bounds__(256, MB > 0 ? MB : (LC > 4 ? 1 : BATCH ? BATCH_P_MIN_BLOCKS : 5)) k_bwd_p(const BwdArgs a0)
+__global__ void __launch_bounds__(256, MB > 0 ? MB : (LC > 4 ? 1 : BATCH ? BATCH_BWD_P_MIN_BLOCKS : 5)) k_bwd_p(const BwdArgs a0)
 {
     pdl_begin();
     BwdArgs a = a0;
