@@ -84,3 +84,33 @@ def test_committed_traffic_has_no_rereads(acct):
     vals = [v["bytes_per_cell"] for v in t.values() if "bytes_per_cell" in v]
     vals += [c["bytes_per_cell"] for v in t.values() for c in v.get("by_config", {}).values()]
     assert vals and np.isfinite(vals).all()
+
+
+def test_workload_subrecords_keep_the_measured_figures(acct, monkeypatch):
+    # the default line's sub-records keep each workload's own value, e2e, clocks, parity and
+    # per-kernel roofline, and a workload that fails leaves its error in place of the figures
+    bench, _, _ = acct
+    rec = {"metric": "RTM shots/s", "value": 0.62, "unit": "shots/s", "steps": 2, "warmup": 3, "ms_per_step": 1600.0,
+           "gpu_launches": 64002, "clocks": {"sm_mhz": 1965.0}, "parity": None, "cpu_baseline": {"value": 1e-3},
+           "config": {"workload": "c5 PSF-RTM shot"}, "e2e": {"value": 0.61, "unit": "shots/s"},
+           "roofline": {"bound": "hbm", "kernel": "bwd_p", "frac": 0.77, "kernels_frac": {"bwd_p": 0.77},
+                        "timing": "events", "algorithmic_bytes_per_launch": 1}}
+    c = bench.compact(rec)
+    assert c["value"] == 0.62 and c["e2e"] == 0.61 and c["workload"] == "c5 PSF-RTM shot"
+    assert c["roofline"] == {"bound": "hbm", "kernel": "bwd_p", "frac": 0.77, "kernels_frac": {"bwd_p": 0.77}}
+    assert "cpu_baseline" not in c and c["warmup"] == 3 and c["clocks"] == {"sm_mhz": 1965.0}
+
+    def ok(args, rank, world, dist):
+        assert (rank, world, dist) == (0, 1, None) and args.warmup >= 3
+        return dict(rec, value=float(args.steps))
+
+    def bad(args, rank, world, dist):
+        raise RuntimeError("no device")
+
+    monkeypatch.setattr(bench, "run_ours", ok)
+    monkeypatch.setattr(bench, "run_afor", ok)
+    monkeypatch.setattr(bench, "run_decon", bad)
+    import argparse
+    subs = bench.extra_workloads(argparse.Namespace(config="c2", steps=20, warmup=5))
+    assert subs["rtm_c5"]["value"] == 2.0 and subs["afor"]["value"] == 5.0
+    assert subs["decon_c5"] == {"error": "RuntimeError: no device"}
