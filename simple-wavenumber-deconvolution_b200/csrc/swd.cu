@@ -1529,8 +1529,13 @@ int swd_create(swd_ctx **out, const swd_grid *g)
     ctx->ldz = (ctx->ntz + 31) / 32 * 32;
     cudaError_t e = cudaSetDevice(ctx->dev);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    // the L2 size only picks default register bounds (same bits either way): a failed query
+    // leaves 0, which counts every pass as streaming from HBM
     int l2 = 0;
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->dev);
+    if (e == cudaSuccess && cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->dev) != cudaSuccess) {
+        cudaGetLastError();
+        l2 = 0;
+    }
     ctx->l2_bytes = (size_t)l2;
     if (e != cudaSuccess) {
         delete ctx;
